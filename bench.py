@@ -1,0 +1,383 @@
+#!/usr/bin/env python3
+"""Benchmark: explosions/s of the B200 engine on the CH4 workload.
+
+Workload (one "step"): integrate S = 1e6 independent CH4 Coulomb explosions
+(C + 4 H, all q = +1, positions uniform in a 3.3-bohr ball, pairs >= 0.5 bohr,
+at rest) to their asymptotic momenta with adaptive DP5(4) at rtol 1e-6,
+atol 1e-7, pe_stop 1e-7 -- the operating point at which every sim is within
+1e-5 relative momentum error of FP64 (checked live on a subset below).
+
+  value   explosions/s with inputs resident in HBM, device-timed with CUDA
+          events on the launch stream (max over ranks), L2 flushed between steps
+  e2e     the same through the C ABI host-buffer call (ce_run): pinned host
+          positions in, momenta / KER / steps / status out, every step
+  roofline  FP32 CUDA-core bound of the integration kernel (the pair force is
+          not a dense contraction): algorithmic FLOPs per launch
+          over the event-timed launch, against a measured FP32 FMA peak
+  cpu_baseline  the reference scalar engine (built from its own sources,
+          oracle/_ref) on all host cores, bounded sample
+
+`--impl reference` runs only the reference CPU engine on the same workload.
+Multi-GPU: each rank integrates its own S sims (weak scaling, no collective on
+the data path); timing is max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "explosions/s on 1 B200 at <=1e-5 rel momentum err vs FP64; closure vs plain RK45"
+UNIT = "explosions/s"
+S_DEFAULT = 1_000_000
+SEED = 20261203
+TIGHT = (1e-6, 1e-7, 1e-7)
+
+
+def flops_per_sim(steps: np.ndarray, n: int) -> np.ndarray:
+    """Algorithmic FP32 FLOPs per sim: steps * (137 P + 438 N) + C_init with
+    C_init = 2 (21 P + 3 N) + 11 P + 60 N (counting rules in DESIGN.md)."""
+    p = n * (n - 1) // 2
+    return steps.astype(np.float64) * (137 * p + 438 * n) + (2 * (21 * p + 3 * n) + 11 * p + 60 * n)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([c.strip() for c in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_reference_rate(pos64, mol, budget_s: float, threads: int):
+    """Reference scalar engine (oracle/_ref, f32 build) on `threads` host threads
+    over growing samples until ~budget_s of wall time. Returns (rate, sims, threads)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_lib as ol
+
+    if not ol.ref_available():
+        return None
+    rtol, atol, pes = TIGHT
+    n = 2048 * max(1, threads)
+    done, spent = 0, 0.0
+    while spent < budget_s and n <= len(pos64):
+        t0 = time.perf_counter()
+        ol.ref_run_batch(pos64[:n], mol.masses_me, mol.charge_array, bits=32, rtol=rtol, atol=atol, pe_stop=pes,
+                         threads=threads)
+        dt = time.perf_counter() - t0
+        done, spent = n, dt
+        if dt > budget_s / 4:
+            break
+        n *= 4
+    return done / spent, done, threads
+
+
+def run_reference_arm(args):
+    world, rank, _ = dist_setup(args)
+    if rank != 0:
+        return 0
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_lib as ol
+    from __graft_entry__ import load_package
+
+    load_package()
+    import importlib
+
+    wl = importlib.import_module("coulomb_explosion_b200.workloads")
+    if not ol.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference engine not built (oracle/_ref missing)"}))
+        return 0
+    mol = wl.CH4
+    threads = os.cpu_count() or 1
+    sample = min(S_DEFAULT, max(20_000, 16_000 * threads))
+    pos = wl.sample_molecule(mol, sample, seed=SEED).astype(np.float32).astype(np.float64)
+    rtol, atol, pes = TIGHT
+    for _ in range(args.warmup):
+        ol.ref_run_batch(pos[: min(sample, 4096)], mol.masses_me, mol.charge_array, bits=32, rtol=rtol, atol=atol,
+                         pe_stop=pes, threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ol.ref_run_batch(pos, mol.masses_me, mol.charge_array, bits=32, rtol=rtol, atol=atol, pe_stop=pes,
+                         threads=threads)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = sample * len(times) / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"CH4 explosions (bounded sample of {sample} of the 1e6-sim step)",
+                   "sims_per_step": sample, "atoms": 5, "rtol": rtol, "atol": atol, "pe_stop": pes},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{sample} CH4 sims per step, reference scalar f32 engine, {threads} threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--sims", type=int, default=S_DEFAULT)
+    ap.add_argument("--mode", type=int, default=3, help="CE_PREC_* bits")
+    ap.add_argument("--cpu-budget", type=float, default=8.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+
+    world, rank, local = dist_setup(args)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local if world > 1 else 0)
+    torch.cuda.set_device(dev)
+
+    from __graft_entry__ import load_package
+
+    ce = load_package()
+    import importlib
+
+    wl = importlib.import_module("coulomb_explosion_b200.workloads")
+    mol = wl.CH4
+    S, n = args.sims, mol.n
+    rtol, atol, pes = TIGHT
+    cfg = ce.RunConfig(rtol=rtol, atol=atol, pe_stop_fraction=pes, precision_mode=args.mode)
+
+    pos_host = wl.sample_molecule(mol, S, seed=SEED + rank).astype(np.float32)
+    eng = ce.Engine(dev.index)
+    eng.set_molecule(mol.masses_me, mol.charge_array)
+
+    stream = torch.cuda.Stream(device=dev)
+    pos_d = torch.from_numpy(pos_host).to(dev)
+    mom_d = torch.empty((S, n, 3), dtype=torch.float32, device=dev)
+    ker_d = torch.empty(S, dtype=torch.float64, device=dev)
+    steps_d = torch.empty(S, dtype=torch.int32, device=dev)
+    status_d = torch.empty(S, dtype=torch.uint8, device=dev)
+    out = ce.CeOutputs(mom_d.data_ptr(), ker_d.data_ptr(), steps_d.data_ptr(), status_d.data_ptr(), None, None,
+                       None, None)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > 126 MB L2
+    torch.cuda.synchronize(dev)
+
+    def launch():
+        eng.run_device(S, pos_d.data_ptr(), cfg, out, stream.cuda_stream)
+        return eng.last_launch_count()
+
+    for _ in range(args.warmup):
+        launch()
+    torch.cuda.synchronize(dev)
+
+    # ---- device-timed region ----
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    launches = 0
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(dev.index) as clk:
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(i & 0xFF)
+                ev[i][0].record(stream)
+            launches += launch()
+            ev[i][1].record(stream)
+        torch.cuda.synchronize(dev)
+    if world > 1:
+        torch.distributed.barrier()
+    per = [a.elapsed_time(b) for a, b in ev]  # ms per launch (flush excluded)
+    total_ms = float(sum(per))
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * S * args.steps / (total_ms / 1e3)
+
+    # ---- results of the last step: accuracy and FLOP accounting ----
+    mom = mom_d.cpu().numpy()
+    steps = steps_d.cpu().numpy().astype(np.uint32)
+    status = status_d.cpu().numpy()
+    ker = ker_d.cpu().numpy()
+
+    # ---- end-to-end through the C ABI host-buffer call ----
+    pin_pos = torch.from_numpy(pos_host).pin_memory()
+    pin_mom = torch.empty((S, n, 3), dtype=torch.float32).pin_memory()
+    pin_ker = torch.empty(S, dtype=torch.float64).pin_memory()
+    pin_steps = torch.empty(S, dtype=torch.int32).pin_memory()
+    pin_status = torch.empty(S, dtype=torch.uint8).pin_memory()
+    hout = ce.CeOutputs(pin_mom.data_ptr(), pin_ker.data_ptr(), pin_steps.data_ptr(), pin_status.data_ptr(),
+                        None, None, None, None)
+    import ctypes
+
+    cc = cfg.to_c()
+    e2e_steps = max(3, args.steps // 2)
+    eng.lib.ce_run(eng.h, S, ctypes.c_void_p(pin_pos.data_ptr()), ctypes.byref(cc), ctypes.byref(hout))
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        rc = eng.lib.ce_run(eng.h, S, ctypes.c_void_p(pin_pos.data_ptr()), ctypes.byref(cc), ctypes.byref(hout))
+        assert rc == 0, eng.lib.ce_last_error(eng.h)
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * S * e2e_steps / e2e_s
+    h2d = S * n * 3 * 4
+    d2h = S * (n * 3 * 4 + 8 + 4 + 1)
+
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return 0
+
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_lib as ol  # checker / CPU baseline only
+
+    sub = np.arange(0, S, max(1, S // 500))[:500]
+    ref = ol.run_batch(pos_host[sub].astype(np.float64), mol.masses_me, mol.charge_array, bits=64, rtol=1e-10,
+                       atol=1e-16, pe_stop=1e-11)
+    err = ol.config_norm_error(mom[sub], ref["momenta"])
+
+    fl = flops_per_sim(steps, n).sum()
+    per_launch_ms = total_ms / args.steps if world == 1 else float(np.mean(per))
+    achieved_tflops = fl / (per_launch_ms / 1e3) / 1e12
+    peak = measure_fp32_peak(torch, dev)
+
+    cpu = None
+    if not args.no_cpu and world == 1:
+        pos64 = pos_host.astype(np.float64)
+        threads = os.cpu_count() or 1
+        r_all = cpu_reference_rate(pos64, mol, args.cpu_budget, threads)
+        r_one = cpu_reference_rate(pos64, mol, args.cpu_budget / 4, 1)
+        if r_all:
+            cpu = {"value": r_all[0], "unit": UNIT, "cores": r_all[2], "kind": "reference",
+                   "sample": f"{r_all[1]} CH4 sims of the step on {r_all[2]} threads (reference scalar f32 engine)",
+                   "single_core_value": r_one[0] if r_one else None}
+
+    traffic = None
+    tp = ROOT / "profiles" / "traffic_rk45_fixed_ch4.json"
+    if tp.exists():
+        try:
+            traffic = json.loads(tp.read_text()).get("bytes_per_launch_full")
+        except Exception:
+            traffic = None
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {
+            "workload": f"CH4 Coulomb explosions, {S} sims per step per GPU (C+4H, q=+1, r 3.3, min pair 0.5)",
+            "sims_per_step": S, "atoms": n, "rtol": rtol, "atol": atol, "pe_stop": pes,
+            "precision_mode": args.mode, "parallelism": f"replicas x{world} (independent shards)",
+            "l2": "flushed between timed steps (256 MiB write, outside the events)",
+            "inputs": "seeded uniform-ball geometries (numpy PCG64), resident in HBM",
+        },
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "path": "ce_run (C ABI, pinned host buffers, synchronous)"},
+        "gpu_launches": launches,
+        "roofline": {"bound": "fp32", "achieved": achieved_tflops, "peak": peak["tflops"], "unit": "TFLOP/s",
+                     "frac": achieved_tflops / peak["tflops"], "traffic": traffic,
+                     "peak_source": peak["source"],
+                     "flops_per_launch": fl, "mean_steps": float(steps.mean())},
+        "accuracy": {"vs": "fp64 oracle (rtol 1e-10, pe_stop 1e-11)", "subset": int(len(sub)),
+                     "max_rel_err": float(err.max()), "median_rel_err": float(np.median(err)),
+                     "p99_rel_err": float(np.percentile(err, 99)),
+                     "status_ok_frac": float((status == 0).mean()),
+                     "ker_vs_pe0_max_rel": float(np.max(np.abs(ker[sub] - ref["ker"]) / ref["ker"]))},
+        "clocks": clk.summary(),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    eng.close()
+    return 0
+
+
+def measure_fp32_peak(torch, dev):
+    """FP32 FMA throughput of this GPU, measured with the engine's probe kernel;
+    falls back to the nominal 148 SMs x 128 lanes x 2 x 1.965 GHz."""
+    from __graft_entry__ import load_package
+
+    ce = load_package()
+    lib = ce.load_library()
+    import ctypes
+
+    if hasattr(lib, "ce_probe_fp32_peak"):
+        v = ctypes.c_double(0.0)
+        rc = lib.ce_probe_fp32_peak(int(dev.index), ctypes.byref(v))
+        if rc == 0 and v.value > 0:
+            return {"tflops": v.value, "source": "measured (FFMA probe kernel, best of 5)"}
+    return {"tflops": 148 * 128 * 2 * 1.965e9 / 1e12, "source": "nominal (148 SMs x 128 FP32 lanes x 1.965 GHz)"}
+
+
+if __name__ == "__main__":
+    sys.exit(main())

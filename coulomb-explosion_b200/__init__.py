@@ -1,0 +1,254 @@
+"""B200-native Coulomb-explosion engine: Python plumbing over the C ABI.
+
+The product is ``libce_gpu.so`` (CUDA, sm_100a) behind ``include/ce_gpu.h`` and
+the C++ host mirror of the reference's ``coulomb::engine`` API under ``host/``.
+This module binds the same C ABI with ctypes for tests and the benchmark; it
+holds no numerics of its own and fails loudly when the CUDA library is absent.
+
+Reference interfaces this mirrors (paths inside the reference project):
+  BatchedRK45<T>(mol, k, lanes, rtol, atol)   include/coulomb/batched_integrator.hpp:71
+  set_lane_geometry(lane, pos)                 include/coulomb/batched_integrator.hpp:112
+  run(RunConfig) -> Result                     include/coulomb/batched_integrator.hpp:123
+  RunConfig / IntegratorOptions                include/coulomb/driver.hpp:141, integrator.hpp:230
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+PKG_DIR = Path(__file__).resolve().parent
+LIB_PATH = PKG_DIR / "libce_gpu.so"
+
+AMU_TO_ME = 1822.888486209  # include/coulomb/units.hpp:13
+
+CE_OK = 0
+CE_ERR_INVALID = -1
+CE_ERR_CUDA = -2
+CE_ERR_NO_DEVICE = -3
+CE_ERR_STATE = -4
+
+CE_SIM_OK = 0
+CE_SIM_REJECT_LIMIT = 1
+CE_SIM_MAX_STEPS = 2
+CE_SIM_NONFINITE = 3
+
+CE_PREC_FP32 = 0
+CE_PREC_KAHAN = 1
+CE_PREC_FP64 = 2
+
+
+class CeRunConfig(C.Structure):
+    _fields_ = [
+        ("rtol", C.c_double),
+        ("atol", C.c_double),
+        ("pe_stop_fraction", C.c_double),
+        ("max_dt", C.c_double),
+        ("max_steps", C.c_uint64),
+        ("redistribute_energy", C.c_int32),
+        ("precision_mode", C.c_int32),
+    ]
+
+
+class CeOutputs(C.Structure):
+    _fields_ = [
+        ("momenta", C.c_void_p),
+        ("ker", C.c_void_p),
+        ("steps", C.c_void_p),
+        ("status", C.c_void_p),
+        ("rejects", C.c_void_p),
+        ("t_final", C.c_void_p),
+        ("pe_final", C.c_void_p),
+        ("ke_before", C.c_void_p),
+    ]
+
+
+class CeTuning(C.Structure):
+    _fields_ = [
+        ("block_threads", C.c_int32),
+        ("blocks_per_sm", C.c_int32),
+        ("refill_threshold", C.c_int32),
+        ("lanes_per_sim", C.c_int32),
+    ]
+
+
+# Every entry point include/ce_gpu.h declares, with its ctypes signature.
+_SIGNATURES = {
+    "ce_version": ([], C.c_char_p),
+    "ce_default_config": ([C.POINTER(CeRunConfig)], None),
+    "ce_create": ([C.POINTER(C.c_void_p), C.c_int], C.c_int),
+    "ce_destroy": ([C.c_void_p], None),
+    "ce_last_error": ([C.c_void_p], C.c_char_p),
+    "ce_set_molecule": ([C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_double], C.c_int),
+    "ce_set_tuning": ([C.c_void_p, C.POINTER(CeTuning)], C.c_int),
+    "ce_get_tuning": ([C.c_void_p, C.POINTER(CeTuning)], C.c_int),
+    "ce_run": ([C.c_void_p, C.c_uint64, C.c_void_p, C.POINTER(CeRunConfig), C.POINTER(CeOutputs)], C.c_int),
+    "ce_run_device": (
+        [C.c_void_p, C.c_uint64, C.c_void_p, C.POINTER(CeRunConfig), C.POINTER(CeOutputs), C.c_void_p],
+        C.c_int,
+    ),
+    "ce_last_launch_count": ([C.c_void_p], C.c_int),
+    "ce_probe_fp32_peak": ([C.c_int, C.POINTER(C.c_double)], C.c_int),
+}
+
+_lib = None
+
+
+def load_library(path: os.PathLike | None = None) -> C.CDLL:
+    """Load libce_gpu.so (built in-tree by ``build.py``). Raises if missing."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise RuntimeError(f"CUDA engine library not built: {p} (run __graft_entry__.build())")
+    lib = C.CDLL(str(p))
+    for name, (args, res) in _SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    if path is None:
+        _lib = lib
+    return lib
+
+
+class EngineError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"ce_gpu error {code}: {msg}")
+        self.code = code
+
+
+@dataclass
+class RunConfig:
+    """RunConfig + IntegratorOptions (driver.hpp:141-163, integrator.hpp:230-233).
+
+    Defaults are the reference's: rtol 1e-8, atol 1e-16, pe_stop 1e-9,
+    max_dt 1e12, max_steps 1e6, redistribution on."""
+
+    rtol: float = 1e-8
+    atol: float = 1e-16
+    pe_stop_fraction: float = 1e-9
+    max_dt: float = 1e12
+    max_steps: int = 1_000_000
+    redistribute_energy: bool = True
+    precision_mode: int = CE_PREC_FP32
+
+    def to_c(self) -> CeRunConfig:
+        return CeRunConfig(
+            float(self.rtol), float(self.atol), float(self.pe_stop_fraction), float(self.max_dt),
+            int(self.max_steps), 1 if self.redistribute_energy else 0, int(self.precision_mode),
+        )
+
+
+@dataclass
+class Result:
+    """Per-sim outputs (BatchedRK45<T>::Result, batched_integrator.hpp:64-69, plus
+    KER, status and diagnostics)."""
+
+    momenta: np.ndarray  # [S, N, 3] float32
+    ker: np.ndarray  # [S] float64
+    steps: np.ndarray  # [S] uint32
+    status: np.ndarray  # [S] uint8
+    rejects: np.ndarray | None = None
+    t_final: np.ndarray | None = None
+    pe_final: np.ndarray | None = None
+    ke_before: np.ndarray | None = None
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def converged(self) -> np.ndarray:
+        return self.status == CE_SIM_OK
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+class Engine:
+    """One engine per host thread and device (include/ce_gpu.h)."""
+
+    def __init__(self, device: int = 0, lib_path: os.PathLike | None = None):
+        self.lib = load_library(lib_path)
+        h = C.c_void_p()
+        rc = self.lib.ce_create(C.byref(h), int(device))
+        if rc != CE_OK:
+            raise EngineError(rc, f"ce_create(device={device}) failed")
+        self.h = h
+        self.n = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ce_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int):
+        if rc != CE_OK:
+            raise EngineError(rc, self.lib.ce_last_error(self.h).decode())
+
+    def set_molecule(self, masses_me, charges, coulomb_k: float = 1.0):
+        m = np.ascontiguousarray(masses_me, dtype=np.float64)
+        q = np.ascontiguousarray(charges, dtype=np.float64)
+        if m.shape != q.shape or m.ndim != 1:
+            raise ValueError("masses and charges must be 1-D of equal length")
+        self._check(self.lib.ce_set_molecule(self.h, int(m.size), _ptr(m), _ptr(q), float(coulomb_k)))
+        self.n = int(m.size)
+        self.masses = m
+        self.charges = q
+
+    def set_tuning(self, block_threads=0, blocks_per_sm=0, refill_threshold=0, lanes_per_sim=0):
+        t = CeTuning(int(block_threads), int(blocks_per_sm), int(refill_threshold), int(lanes_per_sim))
+        self._check(self.lib.ce_set_tuning(self.h, C.byref(t)))
+
+    def get_tuning(self) -> dict:
+        t = CeTuning()
+        self._check(self.lib.ce_get_tuning(self.h, C.byref(t)))
+        return {f: getattr(t, f) for f, _ in CeTuning._fields_}
+
+    def run(self, pos, cfg: RunConfig | None = None, diagnostics: bool = False) -> Result:
+        """Host-buffer path (ce_run): positions [S, N, 3] -> Result."""
+        if self.n is None:
+            raise EngineError(CE_ERR_STATE, "no molecule set")
+        cfg = cfg or RunConfig()
+        x = np.ascontiguousarray(pos, dtype=np.float32)
+        if x.ndim != 3 or x.shape[1] != self.n or x.shape[2] != 3:
+            raise ValueError(f"pos must be [S, {self.n}, 3]")
+        S = x.shape[0]
+        r = Result(
+            momenta=np.zeros((S, self.n, 3), np.float32), ker=np.zeros(S, np.float64),
+            steps=np.zeros(S, np.uint32), status=np.zeros(S, np.uint8),
+        )
+        if diagnostics:
+            r.rejects = np.zeros(S, np.uint32)
+            r.t_final = np.zeros(S, np.float64)
+            r.pe_final = np.zeros(S, np.float64)
+            r.ke_before = np.zeros(S, np.float64)
+        out = CeOutputs(_ptr(r.momenta), _ptr(r.ker), _ptr(r.steps), _ptr(r.status), _ptr(r.rejects),
+                        _ptr(r.t_final), _ptr(r.pe_final), _ptr(r.ke_before))
+        c = cfg.to_c()
+        self._check(self.lib.ce_run(self.h, S, _ptr(x), C.byref(c), C.byref(out)))
+        return r
+
+    def run_device(self, S: int, pos_ptr: int, cfg: RunConfig, out: CeOutputs, stream: int = 0):
+        """Device-buffer path (ce_run_device): raw device pointers, async on `stream`."""
+        c = cfg.to_c()
+        self._check(self.lib.ce_run_device(self.h, int(S), C.c_void_p(pos_ptr), C.byref(c), C.byref(out),
+                                           C.c_void_p(stream)))
+
+    def last_launch_count(self) -> int:
+        return int(self.lib.ce_last_launch_count(self.h))
+
+
+def methane(charge_c: float = 1.0, charge_h: float = 1.0):
+    """CH4 as examples/generate_dataset.cpp:56-66: C then 4 H, singly ionized."""
+    amu = np.array([12.011, 1.008, 1.008, 1.008, 1.008])
+    q = np.array([charge_c] + [charge_h] * 4, dtype=np.float64)
+    return amu * AMU_TO_ME, q

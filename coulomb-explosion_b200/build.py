@@ -1,0 +1,96 @@
+"""Build recipe for libce_gpu.so (sm_100a) and the C++ host mirror.
+
+Compiles every CUDA translation unit with
+``nvcc -gencode arch=compute_100a,code=sm_100a -lineinfo -O3`` in parallel
+into ``_build/`` and links the shared library in-tree (next to this file), so
+it travels with the repository snapshot. Incremental: a unit is rebuilt only
+when a source or header is newer than its object.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from concurrent.futures import ThreadPoolExecutor
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+BUILD = PKG / "_build"
+INCLUDE = ROOT / "include"
+LIB = PKG / "libce_gpu.so"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-ftz=true", "-Xcompiler", "-fPIC",
+                  "-I", str(INCLUDE), "-I", str(CSRC)]
+
+# (object name, source, extra flags)
+UNITS = [("ce_gpu.o", "ce_gpu.cu", []), ("probe.o", "probe.cu", [])] + [
+    (f"kernels_fixed_m{m}.o", "kernels_fixed.cu", [f"-DCE_MODE={m}"]) for m in range(4)
+]
+
+
+def _nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _headers() -> list[Path]:
+    return list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
+
+
+def _stale(obj: Path, src: Path) -> bool:
+    if not obj.exists():
+        return True
+    t = obj.stat().st_mtime
+    return any(p.stat().st_mtime > t for p in [src, *_headers(), Path(__file__)])
+
+
+def build_cuda(verbose: bool = False, ptxas_info: bool = False) -> Path:
+    nvcc = _nvcc()
+    BUILD.mkdir(exist_ok=True)
+    jobs = []
+    for obj, src, extra in UNITS:
+        o, s = BUILD / obj, CSRC / src
+        if _stale(o, s) or ptxas_info:
+            cmd = [nvcc, *NVFLAGS, *extra, "-c", str(s), "-o", str(o)]
+            if ptxas_info:
+                cmd += ["-Xptxas", "-v"]
+            jobs.append((obj, cmd))
+
+    def run(job):
+        obj, cmd = job
+        p = subprocess.run(cmd, capture_output=True, text=True)
+        return obj, p
+
+    failed = []
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 4))) as ex:
+        for obj, p in ex.map(run, jobs):
+            if verbose or ptxas_info:
+                sys.stderr.write(p.stdout + p.stderr)
+            if p.returncode != 0:
+                failed.append((obj, p.stderr))
+    if failed:
+        msg = "\n".join(f"--- {o}\n{e}" for o, e in failed)
+        raise RuntimeError(f"nvcc failed:\n{msg}")
+    objs = [str(BUILD / o) for o, _, _ in UNITS]
+    newest = max(Path(o).stat().st_mtime for o in objs)
+    if not LIB.exists() or LIB.stat().st_mtime < newest:
+        cmd = [nvcc, *ARCH, "-shared", "-o", str(LIB), *objs, "-lcudart"]
+        p = subprocess.run(cmd, capture_output=True, text=True)
+        if p.returncode != 0:
+            raise RuntimeError(f"link failed:\n{p.stderr}")
+    return LIB
+
+
+def build_all(verbose: bool = False) -> None:
+    build_cuda(verbose=verbose)
+
+
+if __name__ == "__main__":
+    build_cuda(verbose=True, ptxas_info="--ptxas" in sys.argv)
+    print(LIB)

@@ -1,0 +1,314 @@
+// ce_gpu.cu -- C ABI of the B200 Coulomb-explosion engine (include/ce_gpu.h).
+//
+// Host side of the drop-in boundary: engine lifetime, molecule constants
+// (BatchedRK45 ctor, include/coulomb/batched_integrator.hpp:71-106), argument
+// checks (the reference throws std::invalid_argument; here CE_ERR_INVALID), the
+// persistent launch, and the host-buffer convenience path.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "ce_gpu.h"
+#include "rk45_sim.cuh"
+
+namespace {
+
+using KernelFn = ce::FixedKernelFn;
+
+KernelFn select_fixed_kernel(int n, int mode) {
+  switch (mode & 3) {
+    case 0: return ce::fixed_kernel_m0(n);
+    case 1: return ce::fixed_kernel_m1(n);
+    case 2: return ce::fixed_kernel_m2(n);
+    default: return ce::fixed_kernel_m3(n);
+  }
+}
+
+}  // namespace
+
+struct ce_engine {
+  int device = 0;
+  int sms = 0;
+  bool has_mol = false;
+  int n = 0;
+  ce::FixedMol mol{};
+  ce_tuning tuning{128, 0, 1, 1};
+  unsigned long long* d_cursor = nullptr;  // work-queue head (engine scratch)
+  cudaStream_t stream = nullptr;           // stream of the host-buffer path
+  void* d_arena = nullptr;                 // device buffers of the host-buffer path
+  size_t arena_bytes = 0;
+  int last_launches = 0;
+  std::string err;
+};
+
+namespace {
+
+int fail(ce_engine* e, int code, const std::string& msg) {
+  if (e) e->err = msg;
+  return code;
+}
+
+int cuda_fail(ce_engine* e, cudaError_t st, const char* what) {
+  return fail(e, CE_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(st));
+}
+
+bool finite_pos(double x) { return std::isfinite(x); }
+
+int check_config(ce_engine* e, const ce_run_config* cfg) {
+  if (!cfg) return fail(e, CE_ERR_INVALID, "ce_run: cfg is NULL");
+  if (!(cfg->rtol >= 0.0) || !(cfg->atol >= 0.0) || !finite_pos(cfg->rtol) || !finite_pos(cfg->atol))
+    return fail(e, CE_ERR_INVALID, "ce_run: rtol and atol must be finite and >= 0");
+  if (!(cfg->rtol > 0.0 || cfg->atol > 0.0))
+    return fail(e, CE_ERR_INVALID, "ce_run: rtol and atol cannot both be 0");
+  if (!(cfg->max_dt > 0.0)) return fail(e, CE_ERR_INVALID, "ce_run: max_dt must be > 0");
+  if (!finite_pos(cfg->pe_stop_fraction))
+    return fail(e, CE_ERR_INVALID, "ce_run: pe_stop_fraction must be finite");
+  if (cfg->precision_mode < 0 || cfg->precision_mode > 3)
+    return fail(e, CE_ERR_INVALID, "ce_run: precision_mode must be a combination of CE_PREC_* bits");
+  return CE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ce_version(void) { return "ce_gpu 0.1 (sm_100a)"; }
+
+void ce_default_config(ce_run_config* cfg) {
+  if (!cfg) return;
+  cfg->rtol = 1e-8;
+  cfg->atol = 1e-16;
+  cfg->pe_stop_fraction = 1e-9;
+  cfg->max_dt = 1e12;
+  cfg->max_steps = 1000000ull;
+  cfg->redistribute_energy = 1;
+  cfg->precision_mode = CE_PREC_FP32;
+}
+
+int ce_create(ce_engine** out, int device) {
+  if (!out) return CE_ERR_INVALID;
+  *out = nullptr;
+  int count = 0;
+  cudaError_t st = cudaGetDeviceCount(&count);
+  if (st != cudaSuccess || count <= 0) return CE_ERR_NO_DEVICE;
+  if (device < 0 || device >= count) return CE_ERR_INVALID;
+  cudaDeviceProp prop{};
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return CE_ERR_CUDA;
+  if (prop.major < 10) return CE_ERR_NO_DEVICE;  // built for sm_100a only
+  if (cudaSetDevice(device) != cudaSuccess) return CE_ERR_CUDA;
+  ce_engine* e = new ce_engine();
+  e->device = device;
+  e->sms = prop.multiProcessorCount;
+  if ((st = cudaMalloc(&e->d_cursor, sizeof(unsigned long long))) != cudaSuccess) {
+    delete e;
+    return CE_ERR_CUDA;
+  }
+  if ((st = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+    cudaFree(e->d_cursor);
+    delete e;
+    return CE_ERR_CUDA;
+  }
+  *out = e;
+  return CE_OK;
+}
+
+void ce_destroy(ce_engine* e) {
+  if (!e) return;
+  cudaSetDevice(e->device);
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  if (e->d_arena) cudaFree(e->d_arena);
+  if (e->d_cursor) cudaFree(e->d_cursor);
+  if (e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+}
+
+const char* ce_last_error(const ce_engine* e) { return e ? e->err.c_str() : "null engine"; }
+
+int ce_last_launch_count(const ce_engine* e) { return e ? e->last_launches : 0; }
+
+int ce_set_molecule(ce_engine* e, int n, const double* mass_me, const double* charge,
+                    double coulomb_k) {
+  if (!e) return CE_ERR_INVALID;
+  if (n < 1 || n > CE_MAX_ATOMS)
+    return fail(e, CE_ERR_INVALID, "ce_set_molecule: n must be in 1..10");
+  if (!mass_me || !charge) return fail(e, CE_ERR_INVALID, "ce_set_molecule: NULL mass or charge");
+  if (!std::isfinite(coulomb_k)) return fail(e, CE_ERR_INVALID, "ce_set_molecule: non-finite k");
+  ce::FixedMol m{};
+  for (int i = 0; i < n; ++i) {
+    if (!(mass_me[i] > 0.0) || !std::isfinite(mass_me[i]))
+      return fail(e, CE_ERR_INVALID, "ce_set_molecule: masses must be finite and > 0");
+    if (!std::isfinite(charge[i]))
+      return fail(e, CE_ERR_INVALID, "ce_set_molecule: charges must be finite");
+    m.mass[i] = mass_me[i];
+    m.inv_m[i] = static_cast<float>(1.0 / mass_me[i]);
+    for (int j = 0; j < n; ++j)
+      m.pc[i * n + j] = static_cast<float>(coulomb_k * charge[i] * charge[j]);
+  }
+  e->mol = m;
+  e->n = n;
+  e->has_mol = true;
+  return CE_OK;
+}
+
+int ce_set_tuning(ce_engine* e, const ce_tuning* t) {
+  if (!e || !t) return CE_ERR_INVALID;
+  ce_tuning v = *t;
+  if (v.block_threads == 0) v.block_threads = 128;
+  if (v.block_threads < 32 || v.block_threads > 256 || (v.block_threads % 32) != 0)
+    return fail(e, CE_ERR_INVALID, "ce_set_tuning: block_threads must be a multiple of 32 in 32..256");
+  if (v.blocks_per_sm < 0 || v.blocks_per_sm > 64)
+    return fail(e, CE_ERR_INVALID, "ce_set_tuning: blocks_per_sm must be in 0..64");
+  if (v.refill_threshold == 0) v.refill_threshold = 1;
+  if (v.refill_threshold < 1 || v.refill_threshold > 32)
+    return fail(e, CE_ERR_INVALID, "ce_set_tuning: refill_threshold must be in 1..32");
+  if (v.lanes_per_sim == 0) v.lanes_per_sim = 1;
+  if (v.lanes_per_sim != 1)
+    return fail(e, CE_ERR_INVALID, "ce_set_tuning: lanes_per_sim must be 1 for the fixed-molecule path");
+  e->tuning = v;
+  return CE_OK;
+}
+
+int ce_get_tuning(const ce_engine* e, ce_tuning* t) {
+  if (!e || !t) return CE_ERR_INVALID;
+  *t = e->tuning;
+  return CE_OK;
+}
+
+int ce_run_device(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
+                  const ce_outputs* out, void* stream) {
+  if (!e) return CE_ERR_INVALID;
+  e->last_launches = 0;
+  int rc = check_config(e, cfg);
+  if (rc != CE_OK) return rc;
+  if (!e->has_mol) return fail(e, CE_ERR_STATE, "ce_run: no molecule set (ce_set_molecule)");
+  if (S == 0) return CE_OK;
+  if (!pos || !out || !out->momenta)
+    return fail(e, CE_ERR_INVALID, "ce_run: pos and out->momenta are required");
+  if (S > (1ull << 40)) return fail(e, CE_ERR_INVALID, "ce_run: S too large");
+  cudaError_t st = cudaSetDevice(e->device);
+  if (st != cudaSuccess) return cuda_fail(e, st, "cudaSetDevice");
+
+  const KernelFn fn = select_fixed_kernel(e->n, cfg->precision_mode);
+  if (!fn) return fail(e, CE_ERR_INVALID, "ce_run: no kernel for this atom count");
+  const int block = e->tuning.block_threads;
+  int per_sm = e->tuning.blocks_per_sm;
+  if (per_sm == 0) {
+    st = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, 0);
+    if (st != cudaSuccess) return cuda_fail(e, st, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (per_sm < 1) per_sm = 1;
+  }
+  const uint64_t need_blocks = (S + static_cast<uint64_t>(block) - 1) / static_cast<uint64_t>(block);
+  const uint64_t grid = std::min<uint64_t>(static_cast<uint64_t>(e->sms) * per_sm, need_blocks);
+
+  ce::RunParams P{};
+  P.pos = pos;
+  P.momenta = out->momenta;
+  P.ker = out->ker;
+  P.steps = out->steps;
+  P.status = out->status;
+  P.rejects = out->rejects;
+  P.t_final = out->t_final;
+  P.pe_final = out->pe_final;
+  P.ke_before = out->ke_before;
+  P.cursor = e->d_cursor;
+  P.S = S;
+  P.rtol = static_cast<float>(cfg->rtol);
+  P.atol = static_cast<float>(cfg->atol);
+  P.max_dt = static_cast<float>(cfg->max_dt);
+  P.pe_stop_f = static_cast<float>(cfg->pe_stop_fraction);
+  P.pe_stop_d = cfg->pe_stop_fraction;
+  P.max_steps = cfg->max_steps > 0xffffffffull ? 0xffffffffu : static_cast<uint32_t>(cfg->max_steps);
+  P.redistribute = cfg->redistribute_energy ? 1 : 0;
+  P.refill_threshold = e->tuning.refill_threshold;
+
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  st = cudaMemsetAsync(e->d_cursor, 0, sizeof(unsigned long long), s);
+  if (st != cudaSuccess) return cuda_fail(e, st, "cudaMemsetAsync(cursor)");
+  fn<<<static_cast<unsigned>(grid), block, 0, s>>>(P, e->mol);
+  st = cudaGetLastError();
+  if (st != cudaSuccess) return cuda_fail(e, st, "rk45 kernel launch");
+  e->last_launches = 1;
+  return CE_OK;
+}
+
+int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
+           const ce_outputs* out) {
+  if (!e) return CE_ERR_INVALID;
+  int rc = check_config(e, cfg);
+  if (rc != CE_OK) return rc;
+  if (!e->has_mol) return fail(e, CE_ERR_STATE, "ce_run: no molecule set (ce_set_molecule)");
+  if (S == 0) return CE_OK;
+  if (!pos || !out || !out->momenta)
+    return fail(e, CE_ERR_INVALID, "ce_run: pos and out->momenta are required");
+  cudaError_t st = cudaSetDevice(e->device);
+  if (st != cudaSuccess) return cuda_fail(e, st, "cudaSetDevice");
+
+  const size_t n3 = static_cast<size_t>(e->n) * 3;
+  auto al = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
+  const size_t b_pos = al(S * n3 * sizeof(float));
+  const size_t b_mom = al(S * n3 * sizeof(float));
+  const size_t b_d = al(S * sizeof(double));
+  const size_t b_u = al(S * sizeof(uint32_t));
+  const size_t b_s = al(S);
+  const size_t total = b_pos + b_mom + 4 * b_d + 2 * b_u + b_s;
+  if (total > e->arena_bytes) {
+    if (e->d_arena) cudaFree(e->d_arena);
+    e->d_arena = nullptr;
+    e->arena_bytes = 0;
+    st = cudaMalloc(&e->d_arena, total);
+    if (st != cudaSuccess) return cuda_fail(e, st, "cudaMalloc(arena)");
+    e->arena_bytes = total;
+  }
+  char* base = static_cast<char*>(e->d_arena);
+  float* d_pos = reinterpret_cast<float*>(base);
+  base += b_pos;
+  ce_outputs d{};
+  d.momenta = reinterpret_cast<float*>(base);
+  base += b_mom;
+  double* dd[4];
+  for (int i = 0; i < 4; ++i) {
+    dd[i] = reinterpret_cast<double*>(base);
+    base += b_d;
+  }
+  uint32_t* du[2];
+  for (int i = 0; i < 2; ++i) {
+    du[i] = reinterpret_cast<uint32_t*>(base);
+    base += b_u;
+  }
+  uint8_t* d_status = reinterpret_cast<uint8_t*>(base);
+  d.ker = out->ker ? dd[0] : nullptr;
+  d.t_final = out->t_final ? dd[1] : nullptr;
+  d.pe_final = out->pe_final ? dd[2] : nullptr;
+  d.ke_before = out->ke_before ? dd[3] : nullptr;
+  d.steps = out->steps ? du[0] : nullptr;
+  d.rejects = out->rejects ? du[1] : nullptr;
+  d.status = out->status ? d_status : nullptr;
+
+  st = cudaMemcpyAsync(d_pos, pos, S * n3 * sizeof(float), cudaMemcpyHostToDevice, e->stream);
+  if (st != cudaSuccess) return cuda_fail(e, st, "cudaMemcpyAsync(pos H2D)");
+  rc = ce_run_device(e, S, d_pos, cfg, &d, e->stream);
+  if (rc != CE_OK) return rc;
+  struct Copy {
+    void* dst;
+    const void* src;
+    size_t bytes;
+  } copies[] = {
+      {out->momenta, d.momenta, S * n3 * sizeof(float)}, {out->ker, d.ker, S * sizeof(double)},
+      {out->t_final, d.t_final, S * sizeof(double)},    {out->pe_final, d.pe_final, S * sizeof(double)},
+      {out->ke_before, d.ke_before, S * sizeof(double)}, {out->steps, d.steps, S * sizeof(uint32_t)},
+      {out->rejects, d.rejects, S * sizeof(uint32_t)},  {out->status, d.status, S}};
+  for (const Copy& c : copies) {
+    if (!c.dst) continue;
+    st = cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, e->stream);
+    if (st != cudaSuccess) return cuda_fail(e, st, "cudaMemcpyAsync(D2H)");
+  }
+  st = cudaStreamSynchronize(e->stream);
+  if (st != cudaSuccess) return cuda_fail(e, st, "cudaStreamSynchronize");
+  return CE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,31 @@
+// kernels_fixed.cu -- instantiates the fixed-molecule persistent kernel for
+// N = 1..10 atoms at one precision mode. Compiled once per mode
+// (-DCE_MODE=0..3) so the 40 instantiations build in parallel.
+#include "rk45_sim.cuh"
+
+#ifndef CE_MODE
+#error "compile with -DCE_MODE=<0..3>"
+#endif
+
+#define CE_CAT2(a, b) a##b
+#define CE_CAT(a, b) CE_CAT2(a, b)
+
+namespace ce {
+
+FixedKernelFn CE_CAT(fixed_kernel_m, CE_MODE)(int n) {
+  switch (n) {
+    case 1: return &rk45_fixed_kernel<1, CE_MODE>;
+    case 2: return &rk45_fixed_kernel<2, CE_MODE>;
+    case 3: return &rk45_fixed_kernel<3, CE_MODE>;
+    case 4: return &rk45_fixed_kernel<4, CE_MODE>;
+    case 5: return &rk45_fixed_kernel<5, CE_MODE>;
+    case 6: return &rk45_fixed_kernel<6, CE_MODE>;
+    case 7: return &rk45_fixed_kernel<7, CE_MODE>;
+    case 8: return &rk45_fixed_kernel<8, CE_MODE>;
+    case 9: return &rk45_fixed_kernel<9, CE_MODE>;
+    case 10: return &rk45_fixed_kernel<10, CE_MODE>;
+    default: return nullptr;
+  }
+}
+
+}  // namespace ce

@@ -1,0 +1,63 @@
+// probe.cu -- FP32 FMA throughput probe (include/ce_probe.h).
+#include <cuda_runtime.h>
+
+#include "ce_gpu.h"
+#include "ce_probe.h"
+
+namespace {
+
+constexpr int kChains = 8;
+constexpr int kIters = 2048;
+
+__global__ void __launch_bounds__(256) ffma_probe(float* out, float b, float c) {
+  float a[kChains];
+#pragma unroll
+  for (int i = 0; i < kChains; ++i) a[i] = static_cast<float>(threadIdx.x + i);
+  for (int it = 0; it < kIters; ++it) {
+#pragma unroll
+    for (int i = 0; i < kChains; ++i) a[i] = fmaf(a[i], b, c);
+  }
+  float s = 0.0f;
+#pragma unroll
+  for (int i = 0; i < kChains; ++i) s += a[i];
+  if (s == 1234.5f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;  // keeps the chains live
+}
+
+}  // namespace
+
+extern "C" int ce_probe_fp32_peak(int device, double* tflops_out) {
+  if (!tflops_out) return CE_ERR_INVALID;
+  *tflops_out = 0.0;
+  if (cudaSetDevice(device) != cudaSuccess) return CE_ERR_NO_DEVICE;
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return CE_ERR_CUDA;
+  const int block = 256, per_sm = 8;
+  const int grid = sms * per_sm;
+  float* out = nullptr;
+  if (cudaMalloc(&out, sizeof(float) * grid * block) != cudaSuccess) return CE_ERR_CUDA;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best_ms = 1e30f;
+  int rc = CE_OK;
+  for (int rep = 0; rep < 6; ++rep) {
+    cudaEventRecord(e0);
+    ffma_probe<<<grid, block>>>(out, 0.999999f, 1e-7f);
+    cudaEventRecord(e1);
+    if (cudaEventSynchronize(e1) != cudaSuccess) {
+      rc = CE_ERR_CUDA;
+      break;
+    }
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (rep > 0 && ms < best_ms) best_ms = ms;  // rep 0 is warm-up
+  }
+  if (cudaGetLastError() != cudaSuccess) rc = CE_ERR_CUDA;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  if (rc != CE_OK) return rc;
+  const double flops = 2.0 * kChains * static_cast<double>(kIters) * grid * block;
+  *tflops_out = flops / (best_ms * 1e-3) / 1e12;
+  return CE_OK;
+}

@@ -1,0 +1,143 @@
+/*
+ * ce_gpu.h -- C ABI of the B200 Coulomb-explosion engine (libce_gpu.so).
+ *
+ * The drop-in boundary for the reference's batched explosion path. The reference
+ * exposes that path as a C++ class template (include/coulomb/batched_integrator.hpp);
+ * a C++ host (coulomb::gpu::BatchedRK45, host/include/coulomb/gpu/batched_rk45.hpp)
+ * or any FFI binds these plain entry points instead:
+ *
+ *   reference                                                  replaced by
+ *   BatchedRK45<T>(mol, coulomb_k, lanes, rtol, atol)          ce_create + ce_set_molecule
+ *     include/coulomb/batched_integrator.hpp:71-106
+ *   BatchedRK45<T>::set_lane_geometry(lane, pos)               the pos[S][N][3] argument
+ *     include/coulomb/batched_integrator.hpp:112-121
+ *   BatchedRK45<T>::run(RunConfig) -> Result                   ce_run / ce_run_device
+ *     include/coulomb/batched_integrator.hpp:123-191
+ *   run_to_convergence(mol, force, integrator, state, cfg)     ce_run (per sim, batched)
+ *     src/driver.cpp:7-46
+ *
+ * Conventions: plain pointers and sizes, no exceptions across the ABI. Every
+ * function returns CE_OK (0) or a negative CE_ERR_* code; ce_last_error() gives
+ * the message. Per-sim failures are NOT call failures: they are reported in
+ * the per-sim status array (CE_SIM_*), mirroring the reference precision
+ * sweep's FailureCode (bench/bench_precision_sweep.cpp:80-85).
+ *
+ * Units: atomic units throughout (Coulomb constant passed explicitly, 1.0 in
+ * atomic units); masses in electron masses (amu * 1822.888486209,
+ * include/coulomb/units.hpp:11-14). Every simulation starts at rest.
+ *
+ * Threading: one engine per host thread; calls on one engine are stream-ordered
+ * and not thread-safe (the reference's BatchedRK45 likewise holds mutable state).
+ */
+#ifndef CE_GPU_H
+#define CE_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- call status ---- */
+#define CE_OK 0
+#define CE_ERR_INVALID (-1)   /* bad argument: the reference's std::invalid_argument */
+#define CE_ERR_CUDA (-2)      /* a CUDA runtime call failed                        */
+#define CE_ERR_NO_DEVICE (-3) /* no usable sm_100 device                            */
+#define CE_ERR_STATE (-4)     /* engine not ready (no molecule set, ...)            */
+
+/* ---- per-sim status (uint8), bench/bench_precision_sweep.cpp:80-85 ---- */
+#define CE_SIM_OK 0           /* reached PE <= pe_stop_fraction * PE_0               */
+#define CE_SIM_REJECT_LIMIT 1 /* > 100 rejections in one step (reference throws,
+                                 src/integrators.cpp:78-82); state kept as is       */
+#define CE_SIM_MAX_STEPS 2    /* max_steps reached first (converged = false,
+                                 src/driver.cpp:20-23)                                */
+#define CE_SIM_NONFINITE 3    /* non-finite initial potential energy (NaN input)    */
+
+/* ---- precision mode bits (ce_run_config.precision_mode) ---- */
+#define CE_PREC_FP32 0  /* FP32 state, FP32 time and stop test (reference f32 engine)   */
+#define CE_PREC_KAHAN 1 /* + compensated (Kahan) accumulation of the x / v updates      */
+#define CE_PREC_FP64 2  /* + FP64 time accumulator and FP64-summed stop-test energy     */
+
+#define CE_MAX_ATOMS 10
+
+typedef struct ce_engine ce_engine;
+
+/* RunConfig (include/coulomb/driver.hpp:141-163) + IntegratorOptions
+ * (include/coulomb/integrator.hpp:230-233) in one struct. */
+typedef struct ce_run_config {
+  double rtol;             /* relative tolerance (reference default 1e-8)            */
+  double atol;             /* absolute tolerance (reference default 1e-16)           */
+  double pe_stop_fraction; /* stop at PE <= f * PE_0 (reference default 1e-9)        */
+  double max_dt;           /* step cap (reference default 1e12)                      */
+  uint64_t max_steps;      /* accepted-step cap (reference default 1e6)              */
+  int32_t redistribute_energy; /* rescale v so KE = E_0 (reference default true)     */
+  int32_t precision_mode;  /* CE_PREC_* bits                                         */
+} ce_run_config;
+
+/* Fill `cfg` with the reference defaults (driver.hpp:147-162, integrator.hpp:231-232). */
+void ce_default_config(ce_run_config* cfg);
+
+/* Per-sim outputs. For ce_run these are host pointers, for ce_run_device device
+ * pointers; same layouts. momenta is required, every other field may be NULL.
+ *   momenta   [S][N][3] float  m_i v_i after redistribution (Result::momenta,
+ *                              batched_integrator.hpp:65, (lane*n+i)*3+c order)
+ *   ker       [S] double       sum |p_i|^2 / (2 m_i)  (demo/sanity_check.py:82-83)
+ *   steps     [S] uint32       accepted steps (Result::steps)
+ *   status    [S] uint8        CE_SIM_*  (Result::converged == (status == 0))
+ *   rejects   [S] uint32       rejected attempts over the run
+ *   t_final   [S] double       simulated time at termination (RunResult::t_final)
+ *   pe_final  [S] double       potential energy at termination (RunResult::pe_final)
+ *   ke_before [S] double       kinetic energy before redistribution
+ *                              (RunResult::ke_before_redist)                         */
+typedef struct ce_outputs {
+  float* momenta;
+  double* ker;
+  uint32_t* steps;
+  uint8_t* status;
+  uint32_t* rejects;
+  double* t_final;
+  double* pe_final;
+  double* ke_before;
+} ce_outputs;
+
+/* Launch-shape knobs picked by the autotuner (0 = engine default). */
+typedef struct ce_tuning {
+  int32_t block_threads;    /* threads per block (thread-per-sim: sims per block)   */
+  int32_t blocks_per_sm;    /* persistent grid = SMs * this (0: occupancy limit)    */
+  int32_t refill_threshold; /* refill a warp once this many lanes are idle (1..32)  */
+  int32_t lanes_per_sim;    /* 1 = one thread per sim; 0 = engine picks by N        */
+} ce_tuning;
+
+/* Engine lifetime. ce_create selects `device` and allocates the engine's small
+ * device scratch (work-queue cursor). */
+int ce_create(ce_engine** out, int device);
+void ce_destroy(ce_engine* e);
+const char* ce_last_error(const ce_engine* e);
+const char* ce_version(void);
+
+/* Fixed molecule for ce_run / ce_run_device: n in 1..10 atoms, masses (electron
+ * masses, > 0) and charges; pair constants k q_i q_j are formed in double and
+ * narrowed to float like batched_integrator.hpp:79-87. */
+int ce_set_molecule(ce_engine* e, int n, const double* mass_me, const double* charge,
+                    double coulomb_k);
+int ce_set_tuning(ce_engine* e, const ce_tuning* t);
+int ce_get_tuning(const ce_engine* e, ce_tuning* t);
+
+/* Integrate S explosions of the fixed molecule from rest.
+ * pos: [S][N][3] float initial positions (host for ce_run, device for
+ * ce_run_device). ce_run copies in, runs and copies out synchronously;
+ * ce_run_device enqueues on `stream` (cudaStream_t, NULL = legacy default) and
+ * returns without synchronizing. S == 0 is a no-op. */
+int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
+           const ce_outputs* out);
+int ce_run_device(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
+                  const ce_outputs* out, void* stream);
+
+/* Number of kernel launches the last ce_run / ce_run_device issued. */
+int ce_last_launch_count(const ce_engine* e);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CE_GPU_H */

@@ -1,0 +1,24 @@
+/*
+ * ce_probe.h -- measurement helper exported by libce_gpu.so.
+ *
+ * No counterpart in the reference (its benchmarks are CPU-only). The explosion
+ * kernel is bound by the FP32 CUDA-core pipe, not by tensor cores or HBM, so its
+ * roofline denominator is the chip's FP32 FMA throughput, measured here with a
+ * dependent-chain-free FFMA kernel (8 independent chains per thread, every SM
+ * fully occupied), timed with CUDA events, best of 5.
+ */
+#ifndef CE_PROBE_H
+#define CE_PROBE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* FP32 FMA throughput of `device` in TFLOP/s (an FMA counts 2). Returns 0 or a
+ * negative CE_ERR_* code. */
+int ce_probe_fp32_peak(int device, double* tflops_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CE_PROBE_H */

@@ -1,0 +1,179 @@
+"""ctypes bindings to the CPU oracle (test infrastructure only).
+
+  oracle/libce_oracle.so   the C restatement of the reference scalar engine
+  oracle/_ref/libref_*.so  the reference scalar engine built from its own sources
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[1]
+ORACLE_SO = ROOT / "oracle" / "libce_oracle.so"
+REF_F32_SO = ROOT / "oracle" / "_ref" / "libref_f32.so"
+REF_F64_SO = ROOT / "oracle" / "_ref" / "libref_f64.so"
+
+KAHAN = 1
+FP64 = 2
+
+
+class OracleCfg(C.Structure):
+    _fields_ = [
+        ("rtol", C.c_double),
+        ("atol", C.c_double),
+        ("pe_stop_fraction", C.c_double),
+        ("max_dt", C.c_double),
+        ("max_steps", C.c_uint64),
+        ("redistribute_energy", C.c_int),
+        ("mode", C.c_int),
+    ]
+
+
+class OracleStats(C.Structure):
+    _fields_ = [
+        ("steps", C.c_uint32),
+        ("rejects", C.c_uint32),
+        ("status", C.c_uint8),
+        ("t_final", C.c_double),
+        ("e0", C.c_double),
+        ("pe_final", C.c_double),
+        ("ke_before", C.c_double),
+        ("ke_after", C.c_double),
+        ("scale", C.c_double),
+    ]
+
+
+def _p(a):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+_oracle = None
+_refs: dict = {}
+
+
+def oracle() -> C.CDLL:
+    global _oracle
+    if _oracle is None:
+        if not ORACLE_SO.exists():
+            raise RuntimeError(f"oracle not built: {ORACLE_SO} (make -C oracle)")
+        lib = C.CDLL(str(ORACLE_SO))
+        vp = C.c_void_p
+        lib.ce_oracle_run_batch.argtypes = [C.c_int, C.c_int, vp, vp, C.c_double, C.c_uint64, vp,
+                                            C.POINTER(OracleCfg)] + [vp] * 8 + [C.c_int]
+        lib.ce_oracle_run_batch_mixed.argtypes = [C.c_int, C.c_uint64, vp, vp, vp, C.c_double, vp,
+                                                  C.POINTER(OracleCfg), vp, vp, vp, vp, C.c_int]
+        for s in ("f32", "f64"):
+            f = getattr(lib, f"ce_oracle_accel_{s}")
+            f.argtypes = [C.c_int, vp, vp, vp, C.c_double, vp]
+            f = getattr(lib, f"ce_oracle_pe_{s}")
+            f.argtypes = [C.c_int, vp, vp, C.c_double]
+            f.restype = C.c_double
+            f = getattr(lib, f"ce_oracle_run_{s}")
+            f.argtypes = [C.c_int, vp, vp, C.c_double, vp, C.POINTER(OracleCfg), vp, C.POINTER(OracleStats)]
+        lib.ce_oracle_run_state_f32.argtypes = [C.c_int, vp, vp, C.c_double, vp, C.POINTER(OracleCfg), vp, vp,
+                                                C.POINTER(OracleStats)]
+        _oracle = lib
+    return _oracle
+
+
+def ref_available() -> bool:
+    return REF_F32_SO.exists() and REF_F64_SO.exists()
+
+
+def ref(bits: int) -> C.CDLL:
+    if bits not in _refs:
+        path = REF_F32_SO if bits == 32 else REF_F64_SO
+        if not path.exists():
+            raise RuntimeError(f"reference engine not built: {path}")
+        lib = C.CDLL(str(path))
+        vp = C.c_void_p
+        lib.ref_run_batch.argtypes = [C.c_int, vp, vp, C.c_double, C.c_uint64, vp, C.c_double, C.c_double,
+                                      C.c_double, C.c_double, C.c_uint64, C.c_int, vp, vp, vp, vp, C.c_int]
+        lib.ref_accel.argtypes = [C.c_int, vp, vp, vp, C.c_double, vp]
+        lib.ref_pe.argtypes = [C.c_int, vp, vp, C.c_double]
+        lib.ref_pe.restype = C.c_double
+        lib.ref_sample.argtypes = [C.c_double, C.c_double, C.c_uint64, C.c_uint64, C.c_int, C.c_uint64, vp]
+        lib.ref_sample.restype = C.c_int
+        lib.ref_real_bytes.restype = C.c_int
+        _refs[bits] = lib
+    return _refs[bits]
+
+
+def cfg(rtol=1e-8, atol=1e-16, pe_stop=1e-9, max_dt=1e12, max_steps=1_000_000, redistribute=True, mode=0):
+    return OracleCfg(rtol, atol, pe_stop, max_dt, max_steps, 1 if redistribute else 0, mode)
+
+
+def run_batch(pos, mass, charge, *, bits=32, k=1.0, threads=0, **kw):
+    """Oracle over pos [S, N, 3] (float64) for one molecule. Returns a dict."""
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    mass = np.ascontiguousarray(mass, dtype=np.float64)
+    charge = np.ascontiguousarray(charge, dtype=np.float64)
+    S, n, _ = pos.shape
+    out = dict(
+        momenta=np.zeros((S, n, 3)), steps=np.zeros(S, np.uint32), status=np.zeros(S, np.uint8),
+        rejects=np.zeros(S, np.uint32), ker=np.zeros(S), t_final=np.zeros(S), pe_final=np.zeros(S),
+        ke_before=np.zeros(S),
+    )
+    c = cfg(**kw)
+    oracle().ce_oracle_run_batch(bits, n, _p(mass), _p(charge), k, S, _p(pos), C.byref(c), _p(out["momenta"]),
+                                 _p(out["steps"]), _p(out["status"]), _p(out["rejects"]), _p(out["ker"]),
+                                 _p(out["t_final"]), _p(out["pe_final"]), _p(out["ke_before"]), int(threads))
+    return out
+
+
+def run_batch_mixed(n_per, mass, charge, pos, *, bits=32, k=1.0, threads=0, **kw):
+    """Oracle over mixed molecules: n_per [S], mass/charge [S,10], pos [S,10,3]."""
+    n_per = np.ascontiguousarray(n_per, dtype=np.uint8)
+    mass = np.ascontiguousarray(mass, dtype=np.float64)
+    charge = np.ascontiguousarray(charge, dtype=np.float64)
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    S = n_per.size
+    out = dict(momenta=np.zeros((S, 10, 3)), steps=np.zeros(S, np.uint32), status=np.zeros(S, np.uint8),
+               ker=np.zeros(S))
+    c = cfg(**kw)
+    oracle().ce_oracle_run_batch_mixed(bits, S, _p(n_per), _p(mass), _p(charge), k, _p(pos), C.byref(c),
+                                       _p(out["momenta"]), _p(out["steps"]), _p(out["status"]),
+                                       _p(out["ker"]), int(threads))
+    return out
+
+
+def ref_run_batch(pos, mass, charge, *, bits=32, k=1.0, rtol=1e-8, atol=1e-16, pe_stop=1e-9, max_dt=1e12,
+                  max_steps=1_000_000, redistribute=True, threads=0):
+    """The reference scalar engine (run_to_convergence per sim) over pos [S, N, 3]."""
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    mass = np.ascontiguousarray(mass, dtype=np.float64)
+    charge = np.ascontiguousarray(charge, dtype=np.float64)
+    S, n, _ = pos.shape
+    out = dict(momenta=np.zeros((S, n, 3)), steps=np.zeros(S, np.uint32), status=np.zeros(S, np.uint8),
+               t_final=np.zeros(S))
+    ref(bits).ref_run_batch(n, _p(mass), _p(charge), k, S, _p(pos), rtol, atol, pe_stop, max_dt, max_steps,
+                            1 if redistribute else 0, _p(out["momenta"]), _p(out["steps"]), _p(out["status"]),
+                            _p(out["t_final"]), int(threads))
+    return out
+
+
+def accel(x, mass, charge, *, bits=64, k=1.0):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    mass = np.ascontiguousarray(mass, dtype=np.float64)
+    charge = np.ascontiguousarray(charge, dtype=np.float64)
+    a = np.zeros_like(x)
+    getattr(oracle(), f"ce_oracle_accel_f{bits}")(x.shape[0], _p(x), _p(mass), _p(charge), k, _p(a))
+    return a
+
+
+def potential(x, charge, *, bits=64, k=1.0):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    charge = np.ascontiguousarray(charge, dtype=np.float64)
+    return getattr(oracle(), f"ce_oracle_pe_f{bits}")(x.shape[0], _p(x), _p(charge), k)
+
+
+def config_norm_error(p, p_ref):
+    """Per-sim ||p - p_ref||_2 / ||p_ref||_2 over all 3N components
+    (python/analysis/plot_precision.py:52-56; examples/verify_subset.py:77-79)."""
+    p = np.asarray(p, dtype=np.float64).reshape(len(p), -1)
+    q = np.asarray(p_ref, dtype=np.float64).reshape(len(p_ref), -1)
+    return np.linalg.norm(p - q, axis=1) / np.linalg.norm(q, axis=1)

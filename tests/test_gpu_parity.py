@@ -1,0 +1,203 @@
+"""Parity of the CUDA engine (through the C ABI) with the oracle and the
+reference engine's golden outputs.
+
+Error statistic: per-sim config-norm ||p - p_ref|| / ||p_ref|| over all 3N
+momentum components (python/analysis/plot_precision.py:52-56).
+
+Tolerances, stated once:
+  TIGHT point (rtol 1e-6, atol 1e-7, pe_stop 1e-7): every sim within 1e-5 of the
+      reference f32 engine, of the reference f64 engine and of the scipy oracle
+      (<= 1e-5 relative momentum error, max over the set).
+  PRODUCTION point (rtol 1e-4, atol 1e-7, pe_stop 1e-5): the reference's own f32
+      and f64 engines already differ by up to ~5e-5 there (accept/reject flips),
+      so parity is statistical: median <= 1e-6, p99 <= 2e-5, max <= 5e-4.
+"""
+from __future__ import annotations
+
+import json
+
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+TIGHT_MAX = 1e-5
+PROD_MEDIAN, PROD_P99, PROD_MAX = 1e-6, 2e-5, 5e-4
+
+
+def cfg_for(ce, point, mode=0, **kw):
+    rtol, atol, pes = point
+    return ce.RunConfig(rtol=rtol, atol=atol, pe_stop_fraction=pes, precision_mode=mode, **kw)
+
+
+def run(engine, ce, mol_m, mol_q, pos, point, mode=0, diagnostics=False, **kw):
+    engine.set_molecule(mol_m, mol_q)
+    return engine.run(np.asarray(pos, np.float32), cfg_for(ce, point, mode, **kw), diagnostics=diagnostics)
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
+def test_ch4_tight_matches_reference_engine(engine, ce, wl, golden_ch4, mode):
+    g = golden_ch4
+    r = run(engine, ce, g["masses"], g["charges"], g["pos"], wl.TIGHT, mode)
+    assert (r.status == 0).all()
+    for bits in (32, 64):
+        err = ol.config_norm_error(r.momenta, g[f"p_tight_f{bits}"])
+        assert err.max() <= TIGHT_MAX, (bits, err.max())
+    steps_ref = g["steps_tight_f32"].astype(float)
+    assert abs(r.steps.mean() - steps_ref.mean()) <= 0.03 * steps_ref.mean()
+
+
+def test_ch4_tight_matches_scipy_oracle(engine, ce, wl, golden_ch4):
+    g = golden_ch4
+    n = len(g["p_scipy"])
+    r = run(engine, ce, g["masses"], g["charges"], g["pos"][:n], wl.TIGHT, 3)
+    err = ol.config_norm_error(r.momenta, g["p_scipy"])
+    assert err.max() <= TIGHT_MAX, err.max()
+
+
+def test_ch4_production_point_statistics(engine, ce, wl, golden_ch4):
+    g = golden_ch4
+    r = run(engine, ce, g["masses"], g["charges"], g["pos"], wl.PRODUCTION, 0)
+    assert (r.status == 0).all()
+    err = ol.config_norm_error(r.momenta, g["p_prod_f32"])
+    assert np.median(err) <= PROD_MEDIAN and np.percentile(err, 99) <= PROD_P99 and err.max() <= PROD_MAX, (
+        np.median(err), np.percentile(err, 99), err.max())
+    steps_ref = g["steps_prod_f32"].astype(float)
+    assert abs(r.steps.mean() - steps_ref.mean()) <= 0.03 * steps_ref.mean()
+
+
+@pytest.mark.parametrize("point", ["prod", "tight"])
+def test_stiff_h2o_matches_reference_engine(engine, ce, wl, golden_h2o, point):
+    g = golden_h2o
+    pt = wl.PRODUCTION if point == "prod" else wl.TIGHT
+    r = run(engine, ce, g["masses"], g["charges"], g["pos"], pt, 3)
+    assert (r.status == 0).all()
+    err = ol.config_norm_error(r.momenta, g[f"p_{point}_f64"])
+    if point == "tight":
+        assert err.max() <= TIGHT_MAX, err.max()
+    else:
+        assert np.median(err) <= 10 * PROD_MEDIAN and err.max() <= 10 * PROD_MAX, (np.median(err), err.max())
+
+
+def test_reference_golden_cases(engine, ce, wl):
+    doc = json.loads((GOLDEN / "reference_cases.json").read_text())
+    for c in doc["cases"]:
+        m, q = np.array(c["masses"]), np.array(c["charges"])
+        r = run(engine, ce, m, q, np.array(c["positions_init"])[None], wl.TIGHT, 3)
+        assert r.status[0] == 0
+        err = ol.config_norm_error(r.momenta, np.array(c["momenta_final"])[None])
+        assert err[0] <= TIGHT_MAX, (c["name"], err[0])
+        # KER = E_0 = PE_0 after redistribution (demo/sanity_check.py:89-96)
+        assert r.ker[0] == pytest.approx(c["potential_energy_init"], rel=1e-6)
+
+
+@pytest.mark.parametrize("n", list(range(1, 11)))
+def test_every_atom_count_matches_oracle(engine, ce, wl, n):
+    rng = np.random.default_rng(50 + n)
+    pos = wl.sample_ball(rng, 200, n, 2.0 * n ** (1 / 3), 0.5).astype(np.float32)
+    mass = rng.choice([1.008, 12.011, 14.007, 15.999, 32.06], n) * wl.AMU_TO_ME
+    q = rng.integers(1, 4, n).astype(float)
+    r = run(engine, ce, mass, q, pos, wl.TIGHT, 3)
+    ref = ol.run_batch(pos.astype(np.float64), mass, q, bits=64, rtol=wl.TIGHT[0], atol=wl.TIGHT[1],
+                       pe_stop=wl.TIGHT[2])
+    if n == 1:  # a lone ion: PE_0 = 0 = pe_stop, zero steps, zero momenta
+        assert (r.status == 0).all() and (r.steps == 0).all() and not r.momenta.any()
+        return
+    assert (r.status == 0).all()
+    err = ol.config_norm_error(r.momenta, ref["momenta"])
+    assert err.max() <= TIGHT_MAX, err.max()
+    np.testing.assert_allclose(r.ker, ref["ker"], rtol=1e-6)
+
+
+def test_diagnostics_and_energy_bookkeeping(engine, ce, wl, golden_ch4):
+    g = golden_ch4
+    r = run(engine, ce, g["masses"], g["charges"], g["pos"], wl.TIGHT, 3, diagnostics=True)
+    o = ol.run_batch(g["pos"], g["masses"], g["charges"], bits=32, mode=3, rtol=wl.TIGHT[0], atol=wl.TIGHT[1],
+                     pe_stop=wl.TIGHT[2])
+    pe0 = np.array([ol.potential(x, g["charges"]) for x in g["pos"]])
+    # stop criterion met: PE_final <= pe_stop * PE_0
+    assert (r.pe_final <= wl.TIGHT[2] * pe0 * (1 + 1e-5)).all()
+    # energy drift before redistribution |KE + PE_final - E_0| / E_0 is small
+    drift = np.abs(r.ke_before + r.pe_final - pe0) / pe0
+    assert drift.max() < 1e-5, drift.max()
+    np.testing.assert_allclose(r.t_final, o["t_final"], rtol=1e-3)
+    assert r.rejects.sum() >= 0
+
+
+def test_ragged_sizes_and_empty(engine, ce, wl):
+    mol = wl.CH4
+    engine.set_molecule(mol.masses_me, mol.charge_array)
+    cfg = cfg_for(ce, wl.TIGHT, 0)
+    r0 = engine.run(np.zeros((0, 5, 3), np.float32), cfg)
+    assert r0.momenta.shape == (0, 5, 3)
+    pos = wl.sample_molecule(mol, 1000, seed=11).astype(np.float32)
+    full = engine.run(pos, cfg)
+    for S in (1, 31, 33, 257, 999):
+        part = engine.run(pos[:S], cfg)
+        np.testing.assert_array_equal(part.momenta, full.momenta[:S])
+        np.testing.assert_array_equal(part.steps, full.steps[:S])
+
+
+def test_results_independent_of_launch_shape(engine, ce, wl):
+    # Each sim's arithmetic is private to its thread, so block size, grid size
+    # and refill granularity cannot change a single bit of the output.
+    mol = wl.CH4
+    engine.set_molecule(mol.masses_me, mol.charge_array)
+    pos = wl.sample_molecule(mol, 3000, seed=12).astype(np.float32)
+    cfg = cfg_for(ce, wl.TIGHT, 3)
+    base = engine.run(pos, cfg)
+    try:
+        for bt, bps, thr in ((32, 0, 1), (64, 1, 8), (256, 0, 32), (96, 2, 4)):
+            engine.set_tuning(block_threads=bt, blocks_per_sm=bps, refill_threshold=thr)
+            r = engine.run(pos, cfg)
+            np.testing.assert_array_equal(r.momenta, base.momenta)
+            np.testing.assert_array_equal(r.steps, base.steps)
+            np.testing.assert_array_equal(r.ker, base.ker)
+    finally:
+        engine.set_tuning()
+
+
+def test_failure_status_codes(engine, ce, wl):
+    mol = wl.CH4
+    engine.set_molecule(mol.masses_me, mol.charge_array)
+    pos = wl.sample_molecule(mol, 64, seed=13).astype(np.float32)
+    # max_steps reached first -> status 2, steps == max_steps (src/driver.cpp:20-23)
+    r = engine.run(pos, ce.RunConfig(rtol=1e-6, atol=1e-7, pe_stop_fraction=1e-7, max_steps=3))
+    assert (r.status == ce.CE_SIM_MAX_STEPS).all() and (r.steps == 3).all()
+    o = ol.run_batch(pos.astype(np.float64), mol.masses_me, mol.charge_array, bits=32, rtol=1e-6, atol=1e-7,
+                     pe_stop=1e-7, max_steps=3)
+    assert ol.config_norm_error(r.momenta, o["momenta"]).max() < 1e-5
+    # rejection limit -> status 1 (the reference throws, src/integrators.cpp:78-82)
+    r = engine.run(pos, ce.RunConfig(rtol=0.0, atol=1e-30, pe_stop_fraction=1e-7))
+    assert (r.status == ce.CE_SIM_REJECT_LIMIT).all()
+    # already below the stop (pe_stop_fraction >= 1): zero steps, at rest
+    r = engine.run(pos, ce.RunConfig(rtol=1e-6, atol=1e-7, pe_stop_fraction=1.0))
+    assert (r.status == 0).all() and (r.steps == 0).all() and not r.momenta.any()
+    # NaN coordinates and coincident atoms -> non-finite initial energy -> status 3
+    bad = pos[:4].copy()
+    bad[0, 2, 1] = np.nan
+    bad[1, 3] = bad[1, 0]
+    r = engine.run(bad, ce.RunConfig(rtol=1e-6, atol=1e-7, pe_stop_fraction=1e-7))
+    assert r.status[0] == ce.CE_SIM_NONFINITE and r.status[1] == ce.CE_SIM_NONFINITE
+    assert (r.status[2:] == 0).all()
+    # redistribution off: KER is the raw kinetic energy, below E_0
+    r = engine.run(pos, ce.RunConfig(rtol=1e-6, atol=1e-7, pe_stop_fraction=1e-7, redistribute_energy=False),
+                   diagnostics=True)
+    np.testing.assert_allclose(r.ker, r.ke_before, rtol=1e-6)
+
+
+def test_invalid_arguments_are_rejected(engine, ce):
+    with pytest.raises(ce.EngineError):
+        engine.set_molecule(np.ones(11), np.ones(11))
+    with pytest.raises(ce.EngineError):
+        engine.set_molecule(np.array([1.0, -1.0]), np.ones(2))
+    engine.set_molecule(np.ones(2) * 1836.0, np.ones(2))
+    with pytest.raises(ce.EngineError):
+        engine.run(np.zeros((4, 2, 3), np.float32), ce.RunConfig(rtol=0.0, atol=0.0))
+    with pytest.raises(ce.EngineError):
+        engine.run(np.zeros((4, 2, 3), np.float32), ce.RunConfig(max_dt=0.0))
+    with pytest.raises(ce.EngineError):
+        engine.set_tuning(block_threads=48)
