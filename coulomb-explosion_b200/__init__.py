@@ -92,6 +92,11 @@ _SIGNATURES = {
     ),
     "ce_last_launch_count": ([C.c_void_p], C.c_int),
     "ce_probe_fp32_peak": ([C.c_int, C.POINTER(C.c_double)], C.c_int),
+    "ce_run_device_noalloc": (
+        [C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_uint64, C.c_void_p, C.POINTER(CeRunConfig),
+         C.POINTER(CeOutputs), C.c_void_p, C.c_char_p, C.c_size_t],
+        C.c_int,
+    ),
 }
 
 _lib = None

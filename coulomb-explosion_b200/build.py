@@ -27,7 +27,7 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-ftz=true", "-Xcompiler", "
                   "-I", str(INCLUDE), "-I", str(CSRC)]
 
 # (object name, source, extra flags)
-UNITS = [("ce_gpu.o", "ce_gpu.cu", []), ("probe.o", "probe.cu", [])] + [
+UNITS = [("ce_gpu.o", "ce_gpu.cu", []), ("probe.o", "probe.cu", []), ("noalloc.o", "noalloc.cu", [])] + [
     (f"kernels_fixed_m{m}.o", "kernels_fixed.cu", [f"-DCE_MODE={m}"]) for m in range(4)
 ]
 

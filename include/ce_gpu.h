@@ -137,6 +137,22 @@ int ce_run_device(ce_engine* e, uint64_t S, const float* pos, const ce_run_confi
 /* Number of kernel launches the last ce_run / ce_run_device issued. */
 int ce_last_launch_count(const ce_engine* e);
 
+/* ce_run_device for callers that cannot allocate device memory. No counterpart
+ * in the reference. It needs no engine: the molecule comes with the call, the
+ * inputs and outputs are the caller's device buffers (as for ce_run_device), and
+ * the kernel's only scratch, its work-queue cursor, lives in a 256-byte static
+ * device array that every GPU loading this library holds until exit. Nothing
+ * here calls cudaMalloc, cudaFree or an allocating library routine.
+ * Limits: 1 <= n <= 10 atoms and S <= 2^40 sims; anything outside is rejected
+ * with CE_ERR_INVALID before a launch. The first call on a device (that device
+ * current) resolves the array's address once, so make it before any stream
+ * capture. All calls share the cursor: each call clears it on `stream` first, and
+ * calls that overlap on the GPU race on it. `err` (may be NULL) receives a
+ * message of at most err_len bytes on failure. */
+int ce_run_device_noalloc(int n, const double* mass_me, const double* charge, double coulomb_k,
+                          uint64_t S, const float* pos, const ce_run_config* cfg,
+                          const ce_outputs* out, void* stream, char* err, size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif
