@@ -180,6 +180,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--sims", type=int, default=S_DEFAULT)
     ap.add_argument("--mode", type=int, default=3, help="CE_PREC_* bits")
+    ap.add_argument("--lanes", type=int, default=0, help="lanes per sim: 0 auto, 1 thread-per-sim, N lane-per-atom")
+    ap.add_argument("--block", type=int, default=0, help="threads per block (0: engine default)")
     ap.add_argument("--cpu-budget", type=float, default=8.0)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
@@ -213,6 +215,8 @@ def main():
     pos_host = wl.sample_molecule(mol, S, seed=SEED + rank).astype(np.float32)
     eng = ce.Engine(dev.index)
     eng.set_molecule(mol.masses_me, mol.charge_array)
+    if args.lanes or args.block:
+        eng.set_tuning(block_threads=args.block, lanes_per_sim=args.lanes)
 
     stream = torch.cuda.Stream(device=dev)
     pos_d = torch.from_numpy(pos_host).to(dev)
@@ -337,6 +341,7 @@ def main():
             "workload": f"CH4 Coulomb explosions, {S} sims per step per GPU (C+4H, q=+1, r 3.3, min pair 0.5)",
             "sims_per_step": S, "atoms": n, "rtol": rtol, "atol": atol, "pe_stop": pes,
             "precision_mode": args.mode, "parallelism": f"replicas x{world} (independent shards)",
+            "tuning": eng.get_tuning(),
             "l2": "flushed between timed steps (256 MiB write, outside the events)",
             "inputs": "seeded uniform-ball geometries (numpy PCG64), resident in HBM",
         },

@@ -13,6 +13,7 @@
 #include <string>
 
 #include "ce_gpu.h"
+#include "rk45_atom.cuh"
 #include "rk45_sim.cuh"
 
 namespace {
@@ -26,6 +27,25 @@ KernelFn select_fixed_kernel(int n, int mode) {
     case 2: return ce::fixed_kernel_m2(n);
     default: return ce::fixed_kernel_m3(n);
   }
+}
+
+KernelFn select_atom_kernel(int n, int mode) {
+  switch (mode & 3) {
+    case 0: return ce::atom_kernel_m0(n);
+    case 1: return ce::atom_kernel_m1(n);
+    case 2: return ce::atom_kernel_m2(n);
+    default: return ce::atom_kernel_m3(n);
+  }
+}
+
+// Layout picked when the tuning leaves lanes_per_sim at 0: one thread per sim
+// while a whole simulation fits in registers without spilling, one lane per
+// atom beyond that.
+bool use_atom_layout(int n, int lanes_per_sim) {
+  if (n < 2) return false;
+  if (lanes_per_sim == 1) return false;
+  if (lanes_per_sim >= 2) return true;
+  return n >= 7;
 }
 
 }  // namespace
@@ -145,6 +165,8 @@ int ce_set_molecule(ce_engine* e, int n, const double* mass_me, const double* ch
       return fail(e, CE_ERR_INVALID, "ce_set_molecule: charges must be finite");
     m.mass[i] = mass_me[i];
     m.inv_m[i] = static_cast<float>(1.0 / mass_me[i]);
+    m.q[i] = static_cast<float>(charge[i]);
+    m.kq[i] = static_cast<float>(coulomb_k * charge[i]);
     for (int j = 0; j < n; ++j)
       m.pc[i * n + j] = static_cast<float>(coulomb_k * charge[i] * charge[j]);
   }
@@ -165,9 +187,8 @@ int ce_set_tuning(ce_engine* e, const ce_tuning* t) {
   if (v.refill_threshold == 0) v.refill_threshold = 1;
   if (v.refill_threshold < 1 || v.refill_threshold > 32)
     return fail(e, CE_ERR_INVALID, "ce_set_tuning: refill_threshold must be in 1..32");
-  if (v.lanes_per_sim == 0) v.lanes_per_sim = 1;
-  if (v.lanes_per_sim != 1)
-    return fail(e, CE_ERR_INVALID, "ce_set_tuning: lanes_per_sim must be 1 for the fixed-molecule path");
+  if (v.lanes_per_sim < 0 || v.lanes_per_sim > CE_MAX_ATOMS)
+    return fail(e, CE_ERR_INVALID, "ce_set_tuning: lanes_per_sim must be 0 (auto), 1 or 2..10 (lane per atom)");
   e->tuning = v;
   return CE_OK;
 }
@@ -192,16 +213,22 @@ int ce_run_device(ce_engine* e, uint64_t S, const float* pos, const ce_run_confi
   cudaError_t st = cudaSetDevice(e->device);
   if (st != cudaSuccess) return cuda_fail(e, st, "cudaSetDevice");
 
-  const KernelFn fn = select_fixed_kernel(e->n, cfg->precision_mode);
+  const bool atom = use_atom_layout(e->n, e->tuning.lanes_per_sim);
+  const KernelFn fn = atom ? select_atom_kernel(e->n, cfg->precision_mode)
+                           : select_fixed_kernel(e->n, cfg->precision_mode);
   if (!fn) return fail(e, CE_ERR_INVALID, "ce_run: no kernel for this atom count");
   const int block = e->tuning.block_threads;
+  // Lane-per-atom: two 32-slot float4 buffers per warp; sims per block = warps * (32 / N).
+  const size_t smem = atom ? static_cast<size_t>(block / 32) * 64 * sizeof(float4) : 0;
+  const uint64_t sims_per_block =
+      atom ? static_cast<uint64_t>(block / 32) * static_cast<uint64_t>(32 / e->n) : static_cast<uint64_t>(block);
   int per_sm = e->tuning.blocks_per_sm;
   if (per_sm == 0) {
-    st = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, 0);
+    st = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem);
     if (st != cudaSuccess) return cuda_fail(e, st, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     if (per_sm < 1) per_sm = 1;
   }
-  const uint64_t need_blocks = (S + static_cast<uint64_t>(block) - 1) / static_cast<uint64_t>(block);
+  const uint64_t need_blocks = (S + sims_per_block - 1) / sims_per_block;
   const uint64_t grid = std::min<uint64_t>(static_cast<uint64_t>(e->sms) * per_sm, need_blocks);
 
   ce::RunParams P{};
@@ -228,7 +255,7 @@ int ce_run_device(ce_engine* e, uint64_t S, const float* pos, const ce_run_confi
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   st = cudaMemsetAsync(e->d_cursor, 0, sizeof(unsigned long long), s);
   if (st != cudaSuccess) return cuda_fail(e, st, "cudaMemsetAsync(cursor)");
-  fn<<<static_cast<unsigned>(grid), block, 0, s>>>(P, e->mol);
+  fn<<<static_cast<unsigned>(grid), block, smem, s>>>(P, e->mol);
   st = cudaGetLastError();
   if (st != cudaSuccess) return cuda_fail(e, st, "rk45 kernel launch");
   e->last_launches = 1;

@@ -103,6 +103,8 @@ extern "C" int ce_run_device_noalloc(int n, const double* mass_me, const double*
                     "ce_run_device_noalloc: masses must be finite and > 0, charges finite");
     m.mass[i] = mass_me[i];
     m.inv_m[i] = static_cast<float>(1.0 / mass_me[i]);
+    m.q[i] = static_cast<float>(charge[i]);
+    m.kq[i] = static_cast<float>(coulomb_k * charge[i]);
     for (int j = 0; j < n; ++j) m.pc[i * n + j] = static_cast<float>(coulomb_k * charge[i] * charge[j]);
   }
   if (S == 0) return CE_OK;

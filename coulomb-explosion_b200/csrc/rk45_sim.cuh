@@ -29,6 +29,8 @@ struct FixedMol {
   float pc[CE_MAX_ATOMS * CE_MAX_ATOMS];  // k q_i q_j, row-major [i*N + j], narrowed from double
   float inv_m[CE_MAX_ATOMS];              // 1 / m_i (float)
   double mass[CE_MAX_ATOMS];              // m_i (double, FP64 finalize)
+  float q[CE_MAX_ATOMS];                  // q_i (lane-per-atom layout: pair constant q_i * (k q_j))
+  float kq[CE_MAX_ATOMS];                 // k q_i
 };
 
 struct RunParams {

@@ -94,13 +94,20 @@ def test_reference_golden_cases(engine, ce, wl):
         assert r.ker[0] == pytest.approx(c["potential_energy_init"], rel=1e-6)
 
 
+@pytest.mark.parametrize("layout", ["sim", "atom"])
 @pytest.mark.parametrize("n", list(range(1, 11)))
-def test_every_atom_count_matches_oracle(engine, ce, wl, n):
+def test_every_atom_count_matches_oracle(engine, ce, wl, n, layout):
+    if layout == "atom" and n == 1:
+        pytest.skip("the lane-per-atom layout needs at least two atoms")
     rng = np.random.default_rng(50 + n)
     pos = wl.sample_ball(rng, 200, n, 2.0 * n ** (1 / 3), 0.5).astype(np.float32)
     mass = rng.choice([1.008, 12.011, 14.007, 15.999, 32.06], n) * wl.AMU_TO_ME
     q = rng.integers(1, 4, n).astype(float)
-    r = run(engine, ce, mass, q, pos, wl.TIGHT, 3)
+    engine.set_tuning(lanes_per_sim=1 if layout == "sim" else n)
+    try:
+        r = run(engine, ce, mass, q, pos, wl.TIGHT, 3)
+    finally:
+        engine.set_tuning()
     ref = ol.run_batch(pos.astype(np.float64), mass, q, bits=64, rtol=wl.TIGHT[0], atol=wl.TIGHT[1],
                        pe_stop=wl.TIGHT[2])
     if n == 1:  # a lone ion: PE_0 = 0 = pe_stop, zero steps, zero momenta
@@ -145,17 +152,19 @@ def test_ragged_sizes_and_empty(engine, ce, wl):
         np.testing.assert_array_equal(part.steps, full.steps[:S])
 
 
-def test_results_independent_of_launch_shape(engine, ce, wl):
-    # Each sim's arithmetic is private to its thread, so block size, grid size
-    # and refill granularity cannot change a single bit of the output.
+@pytest.mark.parametrize("lanes", [1, 5])
+def test_results_independent_of_launch_shape(engine, ce, wl, lanes):
+    # Each sim's arithmetic is private to its thread (or its lane group), so
+    # block size, grid size and refill granularity cannot change a single bit.
     mol = wl.CH4
     engine.set_molecule(mol.masses_me, mol.charge_array)
     pos = wl.sample_molecule(mol, 3000, seed=12).astype(np.float32)
     cfg = cfg_for(ce, wl.TIGHT, 3)
+    engine.set_tuning(lanes_per_sim=lanes)
     base = engine.run(pos, cfg)
     try:
         for bt, bps, thr in ((32, 0, 1), (64, 1, 8), (256, 0, 32), (96, 2, 4)):
-            engine.set_tuning(block_threads=bt, blocks_per_sm=bps, refill_threshold=thr)
+            engine.set_tuning(block_threads=bt, blocks_per_sm=bps, refill_threshold=thr, lanes_per_sim=lanes)
             r = engine.run(pos, cfg)
             np.testing.assert_array_equal(r.momenta, base.momenta)
             np.testing.assert_array_equal(r.steps, base.steps)
