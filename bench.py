@@ -182,6 +182,8 @@ def main():
     ap.add_argument("--mode", type=int, default=3, help="CE_PREC_* bits")
     ap.add_argument("--lanes", type=int, default=0, help="lanes per sim: 0 auto, 1 thread-per-sim, N lane-per-atom")
     ap.add_argument("--block", type=int, default=0, help="threads per block (0: engine default)")
+    ap.add_argument("--molecule", default="ch4", choices=["ch4", "c2h6", "h2o"],
+                    help="ch4 (the headline workload), c2h6 (10-atom C2H6-like), h2o (stiff H2O)")
     ap.add_argument("--cpu-budget", type=float, default=8.0)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
@@ -207,7 +209,10 @@ def main():
     import importlib
 
     wl = importlib.import_module("coulomb_explosion_b200.workloads")
-    mol = wl.CH4
+    mol = {"ch4": wl.CH4, "c2h6": wl.C2H6_LIKE, "h2o": wl.H2O_STIFF}[args.molecule]
+    mol_desc = {"ch4": "CH4 (C+4H, q=+1, r 3.3, min pair 0.5)",
+                "c2h6": "C2H6-like N=10 (2C q=+2, 8H q=+1, r 4.0, min pair 0.5)",
+                "h2o": "stiff H2O (O q=+3, 2H q=+1, r 2.0, min pair 0.3)"}[args.molecule]
     S, n = args.sims, mol.n
     rtol, atol, pes = TIGHT
     cfg = ce.RunConfig(rtol=rtol, atol=atol, pe_stop_fraction=pes, precision_mode=args.mode)
@@ -338,7 +343,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {
-            "workload": f"CH4 Coulomb explosions, {S} sims per step per GPU (C+4H, q=+1, r 3.3, min pair 0.5)",
+            "workload": f"{mol_desc} Coulomb explosions, {S} sims per step per GPU",
             "sims_per_step": S, "atoms": n, "rtol": rtol, "atol": atol, "pe_stop": pes,
             "precision_mode": args.mode, "parallelism": f"replicas x{world} (independent shards)",
             "tuning": eng.get_tuning(),

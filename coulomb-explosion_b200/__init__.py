@@ -75,6 +75,20 @@ class CeTuning(C.Structure):
     ]
 
 
+class CeMixedBatch(C.Structure):
+    _fields_ = [("n_atoms", C.c_void_p), ("mass_me", C.c_void_p), ("charge", C.c_void_p), ("pos", C.c_void_p)]
+
+
+class CeTuneResult(C.Structure):
+    _fields_ = [("t", CeTuning), ("sims_per_s", C.c_double), ("schedule", C.c_int32)]
+
+
+CE_SIM_BAD_INPUT = 4
+CE_SCHEDULE_ONE_LAUNCH = 0
+CE_SCHEDULE_PER_SIZE = 1
+MAX_ATOMS = 10
+
+
 # Every entry point include/ce_gpu.h declares, with its ctypes signature.
 _SIGNATURES = {
     "ce_version": ([], C.c_char_p),
@@ -92,6 +106,30 @@ _SIGNATURES = {
     ),
     "ce_last_launch_count": ([C.c_void_p], C.c_int),
     "ce_probe_fp32_peak": ([C.c_int, C.POINTER(C.c_double)], C.c_int),
+    "ce_reserve_mixed": ([C.c_void_p, C.c_uint64], C.c_int),
+    "ce_run_mixed_device": (
+        [C.c_void_p, C.c_uint64, C.POINTER(CeMixedBatch), C.c_double, C.POINTER(CeRunConfig), C.POINTER(CeOutputs),
+         C.c_int, C.c_void_p],
+        C.c_int,
+    ),
+    "ce_run_mixed": (
+        [C.c_void_p, C.c_uint64, C.POINTER(CeMixedBatch), C.c_double, C.POINTER(CeRunConfig), C.POINTER(CeOutputs)],
+        C.c_int,
+    ),
+    "ce_graph_begin": ([C.c_void_p, C.c_void_p], C.c_int),
+    "ce_graph_end": ([C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)], C.c_int),
+    "ce_graph_launch": ([C.c_void_p, C.c_void_p], C.c_int),
+    "ce_graph_destroy": ([C.c_void_p], None),
+    "ce_autotune_fixed": (
+        [C.c_void_p, C.c_uint64, C.c_void_p, C.POINTER(CeRunConfig), C.POINTER(CeTuneResult), C.c_int,
+         C.POINTER(C.c_int)],
+        C.c_int,
+    ),
+    "ce_autotune_mixed": (
+        [C.c_void_p, C.c_uint64, C.POINTER(CeMixedBatch), C.c_double, C.POINTER(CeRunConfig),
+         C.POINTER(CeTuneResult), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)],
+        C.c_int,
+    ),
     "ce_run_device_noalloc": (
         [C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_uint64, C.c_void_p, C.POINTER(CeRunConfig),
          C.POINTER(CeOutputs), C.c_void_p, C.c_char_p, C.c_size_t],
@@ -250,6 +288,98 @@ class Engine:
 
     def last_launch_count(self) -> int:
         return int(self.lib.ce_last_launch_count(self.h))
+
+    # ---- mixed molecules ----
+    def run_mixed(self, n_atoms, masses_me, charges, pos, cfg: RunConfig | None = None, coulomb_k: float = 1.0,
+                  diagnostics: bool = False) -> Result:
+        """Host-buffer mixed path (ce_run_mixed): n_atoms [S], masses/charges [S, 10],
+        pos [S, 10, 3] -> Result with momenta [S, 10, 3]."""
+        cfg = cfg or RunConfig()
+        n = np.ascontiguousarray(n_atoms, dtype=np.uint8)
+        m = np.ascontiguousarray(masses_me, dtype=np.float64)
+        q = np.ascontiguousarray(charges, dtype=np.float64)
+        x = np.ascontiguousarray(pos, dtype=np.float32)
+        S = n.size
+        if m.shape != (S, MAX_ATOMS) or q.shape != (S, MAX_ATOMS) or x.shape != (S, MAX_ATOMS, 3):
+            raise ValueError("mixed batch rows must be padded to 10 atoms")
+        r = Result(momenta=np.zeros((S, MAX_ATOMS, 3), np.float32), ker=np.zeros(S, np.float64),
+                   steps=np.zeros(S, np.uint32), status=np.zeros(S, np.uint8))
+        if diagnostics:
+            r.rejects = np.zeros(S, np.uint32)
+            r.t_final = np.zeros(S, np.float64)
+            r.pe_final = np.zeros(S, np.float64)
+            r.ke_before = np.zeros(S, np.float64)
+        out = CeOutputs(_ptr(r.momenta), _ptr(r.ker), _ptr(r.steps), _ptr(r.status), _ptr(r.rejects),
+                        _ptr(r.t_final), _ptr(r.pe_final), _ptr(r.ke_before))
+        batch = CeMixedBatch(_ptr(n), _ptr(m), _ptr(q), _ptr(x))
+        c = cfg.to_c()
+        self._check(self.lib.ce_run_mixed(self.h, S, C.byref(batch), float(coulomb_k), C.byref(c), C.byref(out)))
+        return r
+
+    def run_mixed_device(self, S: int, batch: CeMixedBatch, cfg: RunConfig, out: CeOutputs,
+                         schedule: int = CE_SCHEDULE_ONE_LAUNCH, stream: int = 0, coulomb_k: float = 1.0):
+        c = cfg.to_c()
+        self._check(self.lib.ce_run_mixed_device(self.h, int(S), C.byref(batch), float(coulomb_k), C.byref(c),
+                                                 C.byref(out), int(schedule), C.c_void_p(stream)))
+
+    def reserve_mixed(self, S: int):
+        self._check(self.lib.ce_reserve_mixed(self.h, int(S)))
+
+    # ---- graphs ----
+    def graph_begin(self, stream: int):
+        self._check(self.lib.ce_graph_begin(self.h, C.c_void_p(stream)))
+
+    def graph_end(self, stream: int) -> "Graph":
+        g = C.c_void_p()
+        self._check(self.lib.ce_graph_end(self.h, C.c_void_p(stream), C.byref(g)))
+        return Graph(self.lib, g)
+
+    # ---- autotuner ----
+    def autotune_fixed(self, S: int, pos_ptr: int, cfg: RunConfig, cap: int = 64) -> list[dict]:
+        rep = (CeTuneResult * cap)()
+        n = C.c_int(0)
+        c = cfg.to_c()
+        self._check(self.lib.ce_autotune_fixed(self.h, int(S), C.c_void_p(pos_ptr), C.byref(c), rep, cap, C.byref(n)))
+        return [_tune_dict(rep[i]) for i in range(n.value)]
+
+    def autotune_mixed(self, S: int, batch: CeMixedBatch, cfg: RunConfig, coulomb_k: float = 1.0, cap: int = 64):
+        rep = (CeTuneResult * cap)()
+        n = C.c_int(0)
+        best = C.c_int(0)
+        c = cfg.to_c()
+        self._check(self.lib.ce_autotune_mixed(self.h, int(S), C.byref(batch), float(coulomb_k), C.byref(c), rep, cap,
+                                               C.byref(n), C.byref(best)))
+        return [_tune_dict(rep[i]) for i in range(n.value)], int(best.value)
+
+
+def _tune_dict(r: CeTuneResult) -> dict:
+    return {"block_threads": r.t.block_threads, "blocks_per_sm": r.t.blocks_per_sm,
+            "refill_threshold": r.t.refill_threshold, "lanes_per_sim": r.t.lanes_per_sim,
+            "sims_per_s": r.sims_per_s, "schedule": r.schedule}
+
+
+class Graph:
+    """An instantiated CUDA graph of engine calls (ce_graph_*)."""
+
+    def __init__(self, lib, handle):
+        self.lib = lib
+        self.h = handle
+
+    def launch(self, stream: int):
+        rc = self.lib.ce_graph_launch(self.h, C.c_void_p(stream))
+        if rc != CE_OK:
+            raise EngineError(rc, "ce_graph_launch failed")
+
+    def close(self):
+        if self.h:
+            self.lib.ce_graph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def methane(charge_c: float = 1.0, charge_h: float = 1.0):

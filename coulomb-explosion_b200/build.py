@@ -27,7 +27,8 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-ftz=true", "-Xcompiler", "
                   "-I", str(INCLUDE), "-I", str(CSRC)]
 
 # (object name, source, extra flags)
-UNITS = [("ce_gpu.o", "ce_gpu.cu", []), ("probe.o", "probe.cu", []), ("noalloc.o", "noalloc.cu", [])] + [
+UNITS = [("ce_gpu.o", "ce_gpu.cu", []), ("probe.o", "probe.cu", []), ("noalloc.o", "noalloc.cu", []),
+         ("mixed.o", "mixed.cu", [])] + [
     (f"kernels_fixed_m{m}.o", "kernels_fixed.cu", [f"-DCE_MODE={m}"]) for m in range(4)
 ] + [(f"kernels_atom_m{m}.o", "kernels_atom.cu", [f"-DCE_MODE={m}"]) for m in range(4)]
 
@@ -40,7 +41,7 @@ def _nvcc() -> str:
 
 
 def _headers() -> list[Path]:
-    return list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
+    return list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.hpp")) + list(INCLUDE.glob("*.h"))
 
 
 def _stale(obj: Path, src: Path) -> bool:

@@ -1,9 +1,9 @@
-// ce_gpu.cu -- C ABI of the B200 Coulomb-explosion engine (include/ce_gpu.h).
+// ce_gpu.cu -- C ABI of the B200 Coulomb-explosion engine (include/ce_gpu.h):
+// engine lifetime, the fixed-molecule path and the host-buffer convenience path.
 //
-// Host side of the drop-in boundary: engine lifetime, molecule constants
-// (BatchedRK45 ctor, include/coulomb/batched_integrator.hpp:71-106), argument
-// checks (the reference throws std::invalid_argument; here CE_ERR_INVALID), the
-// persistent launch, and the host-buffer convenience path.
+// Host side of the drop-in boundary: molecule constants (BatchedRK45 ctor,
+// include/coulomb/batched_integrator.hpp:71-106), argument checks (the reference
+// throws std::invalid_argument; here CE_ERR_INVALID) and the persistent launch.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -13,90 +13,30 @@
 #include <string>
 
 #include "ce_gpu.h"
-#include "rk45_atom.cuh"
-#include "rk45_sim.cuh"
+#include "engine.hpp"
 
 namespace {
 
-using KernelFn = ce::FixedKernelFn;
-
-KernelFn select_fixed_kernel(int n, int mode) {
-  switch (mode & 3) {
-    case 0: return ce::fixed_kernel_m0(n);
-    case 1: return ce::fixed_kernel_m1(n);
-    case 2: return ce::fixed_kernel_m2(n);
-    default: return ce::fixed_kernel_m3(n);
-  }
-}
-
-KernelFn select_atom_kernel(int n, int mode) {
-  switch (mode & 3) {
-    case 0: return ce::atom_kernel_m0(n);
-    case 1: return ce::atom_kernel_m1(n);
-    case 2: return ce::atom_kernel_m2(n);
-    default: return ce::atom_kernel_m3(n);
-  }
-}
-
-// Layout picked when the tuning leaves lanes_per_sim at 0: one thread per sim
-// while a whole simulation fits in registers without spilling, one lane per
-// atom beyond that.
-bool use_atom_layout(int n, int lanes_per_sim) {
-  if (n < 2) return false;
-  if (lanes_per_sim == 1) return false;
-  if (lanes_per_sim >= 2) return true;
-  return n >= 7;
-}
-
-}  // namespace
-
-struct ce_engine {
-  int device = 0;
-  int sms = 0;
-  bool has_mol = false;
-  int n = 0;
-  ce::FixedMol mol{};
-  ce_tuning tuning{128, 0, 1, 1};
-  unsigned long long* d_cursor = nullptr;  // work-queue head (engine scratch)
-  cudaStream_t stream = nullptr;           // stream of the host-buffer path
-  void* d_arena = nullptr;                 // device buffers of the host-buffer path
-  size_t arena_bytes = 0;
-  int last_launches = 0;
-  std::string err;
-};
-
-namespace {
-
-int fail(ce_engine* e, int code, const std::string& msg) {
-  if (e) e->err = msg;
-  return code;
-}
-
-int cuda_fail(ce_engine* e, cudaError_t st, const char* what) {
-  return fail(e, CE_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(st));
-}
-
-bool finite_pos(double x) { return std::isfinite(x); }
-
-int check_config(ce_engine* e, const ce_run_config* cfg) {
-  if (!cfg) return fail(e, CE_ERR_INVALID, "ce_run: cfg is NULL");
-  if (!(cfg->rtol >= 0.0) || !(cfg->atol >= 0.0) || !finite_pos(cfg->rtol) || !finite_pos(cfg->atol))
-    return fail(e, CE_ERR_INVALID, "ce_run: rtol and atol must be finite and >= 0");
-  if (!(cfg->rtol > 0.0 || cfg->atol > 0.0))
-    return fail(e, CE_ERR_INVALID, "ce_run: rtol and atol cannot both be 0");
-  if (!(cfg->max_dt > 0.0)) return fail(e, CE_ERR_INVALID, "ce_run: max_dt must be > 0");
-  if (!finite_pos(cfg->pe_stop_fraction))
-    return fail(e, CE_ERR_INVALID, "ce_run: pe_stop_fraction must be finite");
-  if (cfg->precision_mode < 0 || cfg->precision_mode > 3)
-    return fail(e, CE_ERR_INVALID, "ce_run: precision_mode must be a combination of CE_PREC_* bits");
-  return CE_OK;
+// Launch shape for one run: explicit tuning fields win, then the autotuned
+// entry for this atom count, then the defaults (128 threads, occupancy-limited
+// grid, refill as soon as one lane or group is idle, one lane per atom for
+// N >= 2 -- measured faster on B200 than one thread per sim for CH4 and N = 10).
+ce_tuning effective_tuning(const ce_engine* e, int n) {
+  ce_tuning t = e->tuning;
+  const ce_tuned_entry& a = e->tuned_fixed[n];
+  if (t.block_threads == 0) t.block_threads = a.valid && a.t.block_threads ? a.t.block_threads : 128;
+  if (t.blocks_per_sm == 0 && a.valid) t.blocks_per_sm = a.t.blocks_per_sm;
+  if (t.refill_threshold == 0) t.refill_threshold = a.valid && a.t.refill_threshold ? a.t.refill_threshold : 1;
+  if (t.lanes_per_sim == 0) t.lanes_per_sim = a.valid && a.t.lanes_per_sim ? a.t.lanes_per_sim : (n >= 2 ? n : 1);
+  if (n < 2) t.lanes_per_sim = 1;
+  return t;
 }
 
 }  // namespace
 
 extern "C" {
 
-const char* ce_version(void) { return "ce_gpu 0.1 (sm_100a)"; }
+const char* ce_version(void) { return "ce_gpu 0.2 (sm_100a)"; }
 
 void ce_default_config(ce_run_config* cfg) {
   if (!cfg) return;
@@ -141,6 +81,7 @@ void ce_destroy(ce_engine* e) {
   cudaSetDevice(e->device);
   if (e->stream) cudaStreamSynchronize(e->stream);
   if (e->d_arena) cudaFree(e->d_arena);
+  if (e->d_mixed) cudaFree(e->d_mixed);
   if (e->d_cursor) cudaFree(e->d_cursor);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
@@ -154,15 +95,15 @@ int ce_set_molecule(ce_engine* e, int n, const double* mass_me, const double* ch
                     double coulomb_k) {
   if (!e) return CE_ERR_INVALID;
   if (n < 1 || n > CE_MAX_ATOMS)
-    return fail(e, CE_ERR_INVALID, "ce_set_molecule: n must be in 1..10");
-  if (!mass_me || !charge) return fail(e, CE_ERR_INVALID, "ce_set_molecule: NULL mass or charge");
-  if (!std::isfinite(coulomb_k)) return fail(e, CE_ERR_INVALID, "ce_set_molecule: non-finite k");
+    return ce::fail(e, CE_ERR_INVALID, "ce_set_molecule: n must be in 1..10");
+  if (!mass_me || !charge) return ce::fail(e, CE_ERR_INVALID, "ce_set_molecule: NULL mass or charge");
+  if (!std::isfinite(coulomb_k)) return ce::fail(e, CE_ERR_INVALID, "ce_set_molecule: non-finite k");
   ce::FixedMol m{};
   for (int i = 0; i < n; ++i) {
     if (!(mass_me[i] > 0.0) || !std::isfinite(mass_me[i]))
-      return fail(e, CE_ERR_INVALID, "ce_set_molecule: masses must be finite and > 0");
+      return ce::fail(e, CE_ERR_INVALID, "ce_set_molecule: masses must be finite and > 0");
     if (!std::isfinite(charge[i]))
-      return fail(e, CE_ERR_INVALID, "ce_set_molecule: charges must be finite");
+      return ce::fail(e, CE_ERR_INVALID, "ce_set_molecule: charges must be finite");
     m.mass[i] = mass_me[i];
     m.inv_m[i] = static_cast<float>(1.0 / mass_me[i]);
     m.q[i] = static_cast<float>(charge[i]);
@@ -178,24 +119,22 @@ int ce_set_molecule(ce_engine* e, int n, const double* mass_me, const double* ch
 
 int ce_set_tuning(ce_engine* e, const ce_tuning* t) {
   if (!e || !t) return CE_ERR_INVALID;
-  ce_tuning v = *t;
-  if (v.block_threads == 0) v.block_threads = 128;
-  if (v.block_threads < 32 || v.block_threads > 256 || (v.block_threads % 32) != 0)
-    return fail(e, CE_ERR_INVALID, "ce_set_tuning: block_threads must be a multiple of 32 in 32..256");
+  const ce_tuning v = *t;
+  if (v.block_threads != 0 && (v.block_threads < 32 || v.block_threads > 256 || (v.block_threads % 32) != 0))
+    return ce::fail(e, CE_ERR_INVALID, "ce_set_tuning: block_threads must be 0 or a multiple of 32 in 32..256");
   if (v.blocks_per_sm < 0 || v.blocks_per_sm > 64)
-    return fail(e, CE_ERR_INVALID, "ce_set_tuning: blocks_per_sm must be in 0..64");
-  if (v.refill_threshold == 0) v.refill_threshold = 1;
-  if (v.refill_threshold < 1 || v.refill_threshold > 32)
-    return fail(e, CE_ERR_INVALID, "ce_set_tuning: refill_threshold must be in 1..32");
+    return ce::fail(e, CE_ERR_INVALID, "ce_set_tuning: blocks_per_sm must be in 0..64");
+  if (v.refill_threshold < 0 || v.refill_threshold > 32)
+    return ce::fail(e, CE_ERR_INVALID, "ce_set_tuning: refill_threshold must be in 0..32");
   if (v.lanes_per_sim < 0 || v.lanes_per_sim > CE_MAX_ATOMS)
-    return fail(e, CE_ERR_INVALID, "ce_set_tuning: lanes_per_sim must be 0 (auto), 1 or 2..10 (lane per atom)");
+    return ce::fail(e, CE_ERR_INVALID, "ce_set_tuning: lanes_per_sim must be 0 (auto), 1 or 2..10 (lane per atom)");
   e->tuning = v;
   return CE_OK;
 }
 
 int ce_get_tuning(const ce_engine* e, ce_tuning* t) {
   if (!e || !t) return CE_ERR_INVALID;
-  *t = e->tuning;
+  *t = e->has_mol ? effective_tuning(e, e->n) : e->tuning;
   return CE_OK;
 }
 
@@ -203,61 +142,46 @@ int ce_run_device(ce_engine* e, uint64_t S, const float* pos, const ce_run_confi
                   const ce_outputs* out, void* stream) {
   if (!e) return CE_ERR_INVALID;
   e->last_launches = 0;
-  int rc = check_config(e, cfg);
+  int rc = ce::check_config(e, cfg);
   if (rc != CE_OK) return rc;
-  if (!e->has_mol) return fail(e, CE_ERR_STATE, "ce_run: no molecule set (ce_set_molecule)");
+  if (!e->has_mol) return ce::fail(e, CE_ERR_STATE, "ce_run: no molecule set (ce_set_molecule)");
   if (S == 0) return CE_OK;
   if (!pos || !out || !out->momenta)
-    return fail(e, CE_ERR_INVALID, "ce_run: pos and out->momenta are required");
-  if (S > (1ull << 40)) return fail(e, CE_ERR_INVALID, "ce_run: S too large");
+    return ce::fail(e, CE_ERR_INVALID, "ce_run: pos and out->momenta are required");
+  if (S > (1ull << 40)) return ce::fail(e, CE_ERR_INVALID, "ce_run: S too large");
   cudaError_t st = cudaSetDevice(e->device);
-  if (st != cudaSuccess) return cuda_fail(e, st, "cudaSetDevice");
+  if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaSetDevice");
 
-  const bool atom = use_atom_layout(e->n, e->tuning.lanes_per_sim);
-  const KernelFn fn = atom ? select_atom_kernel(e->n, cfg->precision_mode)
-                           : select_fixed_kernel(e->n, cfg->precision_mode);
-  if (!fn) return fail(e, CE_ERR_INVALID, "ce_run: no kernel for this atom count");
-  const int block = e->tuning.block_threads;
-  // Lane-per-atom: two 32-slot float4 buffers per warp; sims per block = warps * (32 / N).
-  const size_t smem = atom ? static_cast<size_t>(block / 32) * 64 * sizeof(float4) : 0;
+  const ce_tuning t = effective_tuning(e, e->n);
+  const bool atom = t.lanes_per_sim >= 2;
+  const ce::FixedKernelFn fn = atom ? ce::select_atom_kernel(e->n, cfg->precision_mode)
+                                    : ce::select_fixed_kernel(e->n, cfg->precision_mode);
+  if (!fn) return ce::fail(e, CE_ERR_INVALID, "ce_run: no kernel for this atom count");
+  const int block = t.block_threads;
+  const size_t smem = atom ? ce::atom_smem_bytes(block) : 0;
   const uint64_t sims_per_block =
       atom ? static_cast<uint64_t>(block / 32) * static_cast<uint64_t>(32 / e->n) : static_cast<uint64_t>(block);
-  int per_sm = e->tuning.blocks_per_sm;
+  int per_sm = t.blocks_per_sm;
   if (per_sm == 0) {
     st = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem);
-    if (st != cudaSuccess) return cuda_fail(e, st, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     if (per_sm < 1) per_sm = 1;
   }
   const uint64_t need_blocks = (S + sims_per_block - 1) / sims_per_block;
   const uint64_t grid = std::min<uint64_t>(static_cast<uint64_t>(e->sms) * per_sm, need_blocks);
 
   ce::RunParams P{};
+  ce::fill_run_params(P, cfg, out, t.refill_threshold);
   P.pos = pos;
-  P.momenta = out->momenta;
-  P.ker = out->ker;
-  P.steps = out->steps;
-  P.status = out->status;
-  P.rejects = out->rejects;
-  P.t_final = out->t_final;
-  P.pe_final = out->pe_final;
-  P.ke_before = out->ke_before;
   P.cursor = e->d_cursor;
   P.S = S;
-  P.rtol = static_cast<float>(cfg->rtol);
-  P.atol = static_cast<float>(cfg->atol);
-  P.max_dt = static_cast<float>(cfg->max_dt);
-  P.pe_stop_f = static_cast<float>(cfg->pe_stop_fraction);
-  P.pe_stop_d = cfg->pe_stop_fraction;
-  P.max_steps = cfg->max_steps > 0xffffffffull ? 0xffffffffu : static_cast<uint32_t>(cfg->max_steps);
-  P.redistribute = cfg->redistribute_energy ? 1 : 0;
-  P.refill_threshold = e->tuning.refill_threshold;
 
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   st = cudaMemsetAsync(e->d_cursor, 0, sizeof(unsigned long long), s);
-  if (st != cudaSuccess) return cuda_fail(e, st, "cudaMemsetAsync(cursor)");
+  if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMemsetAsync(cursor)");
   fn<<<static_cast<unsigned>(grid), block, smem, s>>>(P, e->mol);
   st = cudaGetLastError();
-  if (st != cudaSuccess) return cuda_fail(e, st, "rk45 kernel launch");
+  if (st != cudaSuccess) return ce::cuda_fail(e, st, "rk45 kernel launch");
   e->last_launches = 1;
   return CE_OK;
 }
@@ -265,14 +189,14 @@ int ce_run_device(ce_engine* e, uint64_t S, const float* pos, const ce_run_confi
 int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
            const ce_outputs* out) {
   if (!e) return CE_ERR_INVALID;
-  int rc = check_config(e, cfg);
+  int rc = ce::check_config(e, cfg);
   if (rc != CE_OK) return rc;
-  if (!e->has_mol) return fail(e, CE_ERR_STATE, "ce_run: no molecule set (ce_set_molecule)");
+  if (!e->has_mol) return ce::fail(e, CE_ERR_STATE, "ce_run: no molecule set (ce_set_molecule)");
   if (S == 0) return CE_OK;
   if (!pos || !out || !out->momenta)
-    return fail(e, CE_ERR_INVALID, "ce_run: pos and out->momenta are required");
+    return ce::fail(e, CE_ERR_INVALID, "ce_run: pos and out->momenta are required");
   cudaError_t st = cudaSetDevice(e->device);
-  if (st != cudaSuccess) return cuda_fail(e, st, "cudaSetDevice");
+  if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaSetDevice");
 
   const size_t n3 = static_cast<size_t>(e->n) * 3;
   auto al = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
@@ -287,7 +211,7 @@ int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
     e->d_arena = nullptr;
     e->arena_bytes = 0;
     st = cudaMalloc(&e->d_arena, total);
-    if (st != cudaSuccess) return cuda_fail(e, st, "cudaMalloc(arena)");
+    if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMalloc(arena)");
     e->arena_bytes = total;
   }
   char* base = static_cast<char*>(e->d_arena);
@@ -316,7 +240,7 @@ int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
   d.status = out->status ? d_status : nullptr;
 
   st = cudaMemcpyAsync(d_pos, pos, S * n3 * sizeof(float), cudaMemcpyHostToDevice, e->stream);
-  if (st != cudaSuccess) return cuda_fail(e, st, "cudaMemcpyAsync(pos H2D)");
+  if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMemcpyAsync(pos H2D)");
   rc = ce_run_device(e, S, d_pos, cfg, &d, e->stream);
   if (rc != CE_OK) return rc;
   struct Copy {
@@ -331,10 +255,10 @@ int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
   for (const Copy& c : copies) {
     if (!c.dst) continue;
     st = cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, e->stream);
-    if (st != cudaSuccess) return cuda_fail(e, st, "cudaMemcpyAsync(D2H)");
+    if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMemcpyAsync(D2H)");
   }
   st = cudaStreamSynchronize(e->stream);
-  if (st != cudaSuccess) return cuda_fail(e, st, "cudaStreamSynchronize");
+  if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaStreamSynchronize");
   return CE_OK;
 }
 

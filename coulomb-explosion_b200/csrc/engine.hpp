@@ -1,0 +1,117 @@
+// engine.hpp -- the engine object behind the C ABI and the helpers the host
+// translation units share (ce_gpu.cu: fixed molecule; mixed.cu: mixed batches,
+// graphs, autotuning).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <string>
+
+#include "ce_gpu.h"
+#include "rk45_atom.cuh"
+#include "rk45_sim.cuh"
+
+struct ce_tuned_entry {
+  bool valid = false;
+  ce_tuning t{};
+};
+
+struct ce_engine {
+  int device = 0;
+  int sms = 0;
+  bool has_mol = false;
+  int n = 0;
+  ce::FixedMol mol{};
+  ce_tuning tuning{0, 0, 0, 0};  // all fields automatic (autotuned entry, else default)
+  // Autotuned launch shapes, per atom count (fixed path) and for the mixed path.
+  ce_tuned_entry tuned_fixed[CE_MAX_ATOMS + 1];
+  ce_tuned_entry tuned_mixed;
+  unsigned long long* d_cursor = nullptr;  // fixed path work-queue head (engine scratch)
+  cudaStream_t stream = nullptr;           // stream of the host-buffer paths
+  void* d_arena = nullptr;                 // device buffers of the host-buffer paths
+  size_t arena_bytes = 0;
+  // Mixed-batch scratch: 4 x 11 u64 bucket tables, then the S-entry permutation.
+  void* d_mixed = nullptr;
+  size_t mixed_bytes = 0;
+  int last_launches = 0;
+  std::string err;
+};
+
+namespace ce {
+
+inline int fail(ce_engine* e, int code, const std::string& msg) {
+  if (e) e->err = msg;
+  return code;
+}
+
+inline int cuda_fail(ce_engine* e, cudaError_t st, const char* what) {
+  return fail(e, CE_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(st));
+}
+
+inline int check_config(ce_engine* e, const ce_run_config* cfg) {
+  if (!cfg) return fail(e, CE_ERR_INVALID, "ce_run: cfg is NULL");
+  if (!(cfg->rtol >= 0.0) || !(cfg->atol >= 0.0) || !std::isfinite(cfg->rtol) || !std::isfinite(cfg->atol))
+    return fail(e, CE_ERR_INVALID, "ce_run: rtol and atol must be finite and >= 0");
+  if (!(cfg->rtol > 0.0 || cfg->atol > 0.0))
+    return fail(e, CE_ERR_INVALID, "ce_run: rtol and atol cannot both be 0");
+  if (!(cfg->max_dt > 0.0)) return fail(e, CE_ERR_INVALID, "ce_run: max_dt must be > 0");
+  if (!std::isfinite(cfg->pe_stop_fraction))
+    return fail(e, CE_ERR_INVALID, "ce_run: pe_stop_fraction must be finite");
+  if (cfg->precision_mode < 0 || cfg->precision_mode > 3)
+    return fail(e, CE_ERR_INVALID, "ce_run: precision_mode must be a combination of CE_PREC_* bits");
+  return CE_OK;
+}
+
+inline void fill_run_params(RunParams& P, const ce_run_config* cfg, const ce_outputs* out, int refill_threshold) {
+  P.momenta = out->momenta;
+  P.ker = out->ker;
+  P.steps = out->steps;
+  P.status = out->status;
+  P.rejects = out->rejects;
+  P.t_final = out->t_final;
+  P.pe_final = out->pe_final;
+  P.ke_before = out->ke_before;
+  P.rtol = static_cast<float>(cfg->rtol);
+  P.atol = static_cast<float>(cfg->atol);
+  P.max_dt = static_cast<float>(cfg->max_dt);
+  P.pe_stop_f = static_cast<float>(cfg->pe_stop_fraction);
+  P.pe_stop_d = cfg->pe_stop_fraction;
+  P.max_steps = cfg->max_steps > 0xffffffffull ? 0xffffffffu : static_cast<uint32_t>(cfg->max_steps);
+  P.redistribute = cfg->redistribute_energy ? 1 : 0;
+  P.refill_threshold = refill_threshold;
+}
+
+inline FixedKernelFn select_fixed_kernel(int n, int mode) {
+  switch (mode & 3) {
+    case 0: return fixed_kernel_m0(n);
+    case 1: return fixed_kernel_m1(n);
+    case 2: return fixed_kernel_m2(n);
+    default: return fixed_kernel_m3(n);
+  }
+}
+
+inline AtomKernelFn select_atom_kernel(int n, int mode) {
+  switch (mode & 3) {
+    case 0: return atom_kernel_m0(n);
+    case 1: return atom_kernel_m1(n);
+    case 2: return atom_kernel_m2(n);
+    default: return atom_kernel_m3(n);
+  }
+}
+
+inline MixedKernelFn select_mixed_kernel(int n, int mode) {
+  switch (mode & 3) {
+    case 0: return mixed_kernel_m0(n);
+    case 1: return mixed_kernel_m1(n);
+    case 2: return mixed_kernel_m2(n);
+    default: return mixed_kernel_m3(n);
+  }
+}
+
+// Dynamic shared memory of a lane-per-atom block.
+inline size_t atom_smem_bytes(int block) {
+  return static_cast<size_t>(block / 32) * kAtomBufSlots * sizeof(float4);
+}
+
+}  // namespace ce

@@ -1,0 +1,513 @@
+// mixed.cu -- mixed 2..10-atom batches, CUDA-graph capture and the autotuner
+// (include/ce_gpu.h).
+//
+// The reference runs one molecule per BatchedRK45 (every lane shares the
+// molecule, include/coulomb/batched_force.hpp:8-13); a mixed population takes
+// one reference engine per molecule. Here one call integrates any mix: a
+// device counting sort groups the sims by atom count (count -> scan -> scatter,
+// three small kernels), then either one persistent launch walks the size
+// buckets (CE_SCHEDULE_ONE_LAUNCH) or one launch per bucket runs them in
+// sequence (CE_SCHEDULE_PER_SIZE). Everything is stream-ordered and allocates
+// nothing once ce_reserve_mixed has sized the scratch, so it can be captured
+// into a CUDA graph.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "ce_gpu.h"
+#include "engine.hpp"
+
+namespace {
+
+constexpr int kBins = 16;  // bin 0 = invalid atom count, bins 1..10 = atoms per sim
+
+// Bucket tables at the head of the engine's mixed scratch (u64 each).
+struct BucketTables {
+  unsigned long long* cnt;     // [kBins]
+  unsigned long long* off;     // [kBins]
+  unsigned long long* fill;    // [kBins]
+  unsigned long long* cursor;  // [kBins]
+  uint32_t* perm;              // [S]
+};
+
+size_t mixed_scratch_bytes(uint64_t S) { return 4 * kBins * sizeof(unsigned long long) + S * sizeof(uint32_t); }
+
+BucketTables tables_of(void* base) {
+  auto* p = static_cast<unsigned long long*>(base);
+  BucketTables t;
+  t.cnt = p;
+  t.off = p + kBins;
+  t.fill = p + 2 * kBins;
+  t.cursor = p + 3 * kBins;
+  t.perm = reinterpret_cast<uint32_t*>(p + 4 * kBins);
+  return t;
+}
+
+__device__ __forceinline__ int bin_of(uint8_t n) { return (n >= 1 && n <= CE_MAX_ATOMS) ? n : 0; }
+
+__global__ void bucket_count_kernel(const uint8_t* __restrict__ n_per, uint64_t S, unsigned long long* cnt) {
+  __shared__ unsigned int h[kBins];
+  if (threadIdx.x < kBins) h[threadIdx.x] = 0u;
+  __syncthreads();
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < S;
+       i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+    atomicAdd(&h[bin_of(n_per[i])], 1u);
+  __syncthreads();
+  if (threadIdx.x < kBins && h[threadIdx.x]) atomicAdd(&cnt[threadIdx.x], static_cast<unsigned long long>(h[threadIdx.x]));
+}
+
+__global__ void bucket_scan_kernel(const unsigned long long* cnt, unsigned long long* off, unsigned long long* fill,
+                                   unsigned long long* cursor) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  unsigned long long acc = 0ull;
+  for (int b = 0; b < kBins; ++b) {
+    off[b] = acc;
+    acc += cnt[b];
+    fill[b] = 0ull;
+    cursor[b] = 0ull;
+  }
+}
+
+// Scatter sim indices into their bucket (order inside a bucket is irrelevant:
+// every sim is integrated independently). Sims with one atom (no pair, PE = 0,
+// converged at rest) and sims with an invalid atom count are written out here.
+__global__ void bucket_scatter_kernel(const uint8_t* __restrict__ n_per, uint64_t S, const unsigned long long* off,
+                                      unsigned long long* fill, uint32_t* perm, ce::RunParams P) {
+  __shared__ unsigned int h[kBins];
+  __shared__ unsigned long long b[kBins];
+  for (uint64_t t0 = blockIdx.x * static_cast<uint64_t>(blockDim.x); t0 < S;
+       t0 += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    if (threadIdx.x < kBins) h[threadIdx.x] = 0u;
+    __syncthreads();
+    const uint64_t i = t0 + threadIdx.x;
+    int bin = -1;
+    unsigned int r = 0u;
+    if (i < S) {
+      bin = bin_of(n_per[i]);
+      r = atomicAdd(&h[bin], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < kBins && h[threadIdx.x]) b[threadIdx.x] = atomicAdd(&fill[threadIdx.x], static_cast<unsigned long long>(h[threadIdx.x]));
+    __syncthreads();
+    if (bin >= 2) {
+      perm[off[bin] + b[bin] + r] = static_cast<uint32_t>(i);
+    } else if (bin >= 0) {
+      float* m = P.momenta + i * (3ull * ce::kMixedStride);
+      for (int c = 0; c < 3 * ce::kMixedStride; ++c) m[c] = 0.0f;
+      if (P.ker) P.ker[i] = 0.0;
+      if (P.steps) P.steps[i] = 0u;
+      if (P.status) P.status[i] = bin == 1 ? static_cast<uint8_t>(CE_SIM_OK) : static_cast<uint8_t>(CE_SIM_BAD_INPUT);
+      if (P.rejects) P.rejects[i] = 0u;
+      if (P.t_final) P.t_final[i] = 0.0;
+      if (P.pe_final) P.pe_final[i] = 0.0;
+      if (P.ke_before) P.ke_before[i] = 0.0;
+    }
+    __syncthreads();
+  }
+}
+
+ce_tuning mixed_tuning(const ce_engine* e) {
+  ce_tuning t = e->tuning;
+  const ce_tuned_entry& a = e->tuned_mixed;
+  if (t.block_threads == 0) t.block_threads = a.valid && a.t.block_threads ? a.t.block_threads : 128;
+  if (t.blocks_per_sm == 0 && a.valid) t.blocks_per_sm = a.t.blocks_per_sm;
+  if (t.refill_threshold == 0) t.refill_threshold = a.valid && a.t.refill_threshold ? a.t.refill_threshold : 1;
+  return t;
+}
+
+int check_mixed_args(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double k, const ce_run_config* cfg,
+                     const ce_outputs* out) {
+  int rc = ce::check_config(e, cfg);
+  if (rc != CE_OK) return rc;
+  if (S >= (1ull << 32)) return ce::fail(e, CE_ERR_INVALID, "ce_run_mixed: S must be below 2^32");
+  if (S == 0) return CE_OK;
+  if (!in || !in->n_atoms || !in->mass_me || !in->charge || !in->pos)
+    return ce::fail(e, CE_ERR_INVALID, "ce_run_mixed: n_atoms, mass_me, charge and pos are required");
+  if (!out || !out->momenta) return ce::fail(e, CE_ERR_INVALID, "ce_run_mixed: out->momenta is required");
+  if (!std::isfinite(k)) return ce::fail(e, CE_ERR_INVALID, "ce_run_mixed: non-finite Coulomb constant");
+  return CE_OK;
+}
+
+}  // namespace
+
+struct ce_graph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int device = 0;
+};
+
+extern "C" {
+
+int ce_reserve_mixed(ce_engine* e, uint64_t S) {
+  if (!e) return CE_ERR_INVALID;
+  if (S >= (1ull << 32)) return ce::fail(e, CE_ERR_INVALID, "ce_reserve_mixed: S must be below 2^32");
+  const size_t need = mixed_scratch_bytes(S);
+  if (need <= e->mixed_bytes) return CE_OK;
+  cudaError_t st = cudaSetDevice(e->device);
+  if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaSetDevice");
+  if (e->d_mixed) cudaFree(e->d_mixed);
+  e->d_mixed = nullptr;
+  e->mixed_bytes = 0;
+  st = cudaMalloc(&e->d_mixed, need);
+  if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMalloc(mixed scratch)");
+  e->mixed_bytes = need;
+  return CE_OK;
+}
+
+int ce_run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coulomb_k,
+                        const ce_run_config* cfg, const ce_outputs* out, int schedule, void* stream) {
+  if (!e) return CE_ERR_INVALID;
+  e->last_launches = 0;
+  int rc = check_mixed_args(e, S, in, coulomb_k, cfg, out);
+  if (rc != CE_OK || S == 0) return rc;
+  if (schedule != CE_SCHEDULE_ONE_LAUNCH && schedule != CE_SCHEDULE_PER_SIZE)
+    return ce::fail(e, CE_ERR_INVALID, "ce_run_mixed: unknown schedule");
+  cudaError_t st = cudaSetDevice(e->device);
+  if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaSetDevice");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (mixed_scratch_bytes(S) > e->mixed_bytes) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (s && cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone)
+      return ce::fail(e, CE_ERR_STATE, "ce_run_mixed: scratch too small during graph capture (ce_reserve_mixed first)");
+    rc = ce_reserve_mixed(e, S);
+    if (rc != CE_OK) return rc;
+  }
+  const BucketTables T = tables_of(e->d_mixed);
+  const ce_tuning t = mixed_tuning(e);
+
+  ce::RunParams P{};
+  ce::fill_run_params(P, cfg, out, t.refill_threshold);
+  P.pos = in->pos;
+  P.cursor = nullptr;
+  P.S = S;
+  ce::MixedIn X{in->n_atoms, in->mass_me, in->charge, coulomb_k};
+  ce::Buckets B{T.perm, T.off, T.cnt, T.cursor};
+
+  const int sort_block = 256;
+  const unsigned sort_grid =
+      static_cast<unsigned>(std::min<uint64_t>((S + sort_block - 1) / sort_block, static_cast<uint64_t>(e->sms) * 8));
+  st = cudaMemsetAsync(T.cnt, 0, kBins * sizeof(unsigned long long), s);
+  if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMemsetAsync(bucket counts)");
+  bucket_count_kernel<<<sort_grid, sort_block, 0, s>>>(in->n_atoms, S, T.cnt);
+  bucket_scan_kernel<<<1, 32, 0, s>>>(T.cnt, T.off, T.fill, T.cursor);
+  bucket_scatter_kernel<<<sort_grid, sort_block, 0, s>>>(in->n_atoms, S, T.off, T.fill, T.perm, P);
+  int launches = 3;
+
+  const int block = t.block_threads;
+  const size_t smem = ce::atom_smem_bytes(block);
+  if (schedule == CE_SCHEDULE_ONE_LAUNCH) {
+    const ce::MixedKernelFn fn = ce::select_mixed_kernel(0, cfg->precision_mode);
+    int per_sm = t.blocks_per_sm;
+    if (per_sm == 0) {
+      st = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem);
+      if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+      if (per_sm < 1) per_sm = 1;
+    }
+    // Enough groups for the smallest molecules, never more than one wave.
+    const uint64_t sims_per_block = static_cast<uint64_t>(block / 32) * (32 / 2);
+    const uint64_t grid = std::min<uint64_t>(static_cast<uint64_t>(e->sms) * per_sm, (S + sims_per_block - 1) / sims_per_block);
+    fn<<<static_cast<unsigned>(std::max<uint64_t>(grid, 1)), block, smem, s>>>(P, X, B);
+    ++launches;
+  } else {
+    for (int n = CE_MAX_ATOMS; n >= 2; --n) {
+      const ce::MixedKernelFn fn = ce::select_mixed_kernel(n, cfg->precision_mode);
+      int per_sm = t.blocks_per_sm;
+      if (per_sm == 0) {
+        st = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem);
+        if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+        if (per_sm < 1) per_sm = 1;
+      }
+      const uint64_t sims_per_block = static_cast<uint64_t>(block / 32) * (32 / n);
+      const uint64_t grid = std::min<uint64_t>(static_cast<uint64_t>(e->sms) * per_sm, (S + sims_per_block - 1) / sims_per_block);
+      fn<<<static_cast<unsigned>(std::max<uint64_t>(grid, 1)), block, smem, s>>>(P, X, B);
+      ++launches;
+    }
+  }
+  st = cudaGetLastError();
+  if (st != cudaSuccess) return ce::cuda_fail(e, st, "mixed kernel launch");
+  e->last_launches = launches;
+  return CE_OK;
+}
+
+int ce_run_mixed(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coulomb_k, const ce_run_config* cfg,
+                 const ce_outputs* out) {
+  if (!e) return CE_ERR_INVALID;
+  int rc = check_mixed_args(e, S, in, coulomb_k, cfg, out);
+  if (rc != CE_OK || S == 0) return rc;
+  cudaError_t st = cudaSetDevice(e->device);
+  if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaSetDevice");
+  const size_t A = CE_MAX_ATOMS;
+  auto al = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
+  const size_t sizes[] = {al(S),                              // n_atoms
+                          al(S * A * sizeof(double)),         // mass
+                          al(S * A * sizeof(double)),         // charge
+                          al(S * A * 3 * sizeof(float)),      // pos
+                          al(S * A * 3 * sizeof(float)),      // momenta
+                          al(S * sizeof(double)) * 4,         // ker, t_final, pe_final, ke_before
+                          al(S * sizeof(uint32_t)) * 2,       // steps, rejects
+                          al(S)};                             // status
+  size_t total = 0;
+  for (size_t b : sizes) total += b;
+  if (total > e->arena_bytes) {
+    if (e->d_arena) cudaFree(e->d_arena);
+    e->d_arena = nullptr;
+    e->arena_bytes = 0;
+    st = cudaMalloc(&e->d_arena, total);
+    if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMalloc(arena)");
+    e->arena_bytes = total;
+  }
+  char* p = static_cast<char*>(e->d_arena);
+  ce_mixed_batch d_in;
+  d_in.n_atoms = reinterpret_cast<const uint8_t*>(p);
+  char* d_n = p;
+  p += sizes[0];
+  char* d_m = p;
+  d_in.mass_me = reinterpret_cast<const double*>(p);
+  p += sizes[1];
+  char* d_q = p;
+  d_in.charge = reinterpret_cast<const double*>(p);
+  p += sizes[2];
+  char* d_x = p;
+  d_in.pos = reinterpret_cast<const float*>(p);
+  p += sizes[3];
+  ce_outputs d{};
+  d.momenta = reinterpret_cast<float*>(p);
+  p += sizes[4];
+  const size_t bd = al(S * sizeof(double));
+  d.ker = out->ker ? reinterpret_cast<double*>(p) : nullptr;
+  d.t_final = out->t_final ? reinterpret_cast<double*>(p + bd) : nullptr;
+  d.pe_final = out->pe_final ? reinterpret_cast<double*>(p + 2 * bd) : nullptr;
+  d.ke_before = out->ke_before ? reinterpret_cast<double*>(p + 3 * bd) : nullptr;
+  p += sizes[5];
+  const size_t bu = al(S * sizeof(uint32_t));
+  d.steps = out->steps ? reinterpret_cast<uint32_t*>(p) : nullptr;
+  d.rejects = out->rejects ? reinterpret_cast<uint32_t*>(p + bu) : nullptr;
+  p += sizes[6];
+  d.status = out->status ? reinterpret_cast<uint8_t*>(p) : nullptr;
+
+  struct Copy {
+    void* dst;
+    const void* src;
+    size_t bytes;
+  };
+  const Copy h2d[] = {{d_n, in->n_atoms, S},
+                      {d_m, in->mass_me, S * A * sizeof(double)},
+                      {d_q, in->charge, S * A * sizeof(double)},
+                      {d_x, in->pos, S * A * 3 * sizeof(float)}};
+  for (const Copy& c : h2d) {
+    st = cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyHostToDevice, e->stream);
+    if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMemcpyAsync(H2D)");
+  }
+  rc = ce_run_mixed_device(e, S, &d_in, coulomb_k, cfg, &d, CE_SCHEDULE_ONE_LAUNCH, e->stream);
+  if (rc != CE_OK) return rc;
+  const Copy d2h[] = {{out->momenta, d.momenta, S * A * 3 * sizeof(float)}, {out->ker, d.ker, S * sizeof(double)},
+                      {out->t_final, d.t_final, S * sizeof(double)},     {out->pe_final, d.pe_final, S * sizeof(double)},
+                      {out->ke_before, d.ke_before, S * sizeof(double)}, {out->steps, d.steps, S * sizeof(uint32_t)},
+                      {out->rejects, d.rejects, S * sizeof(uint32_t)},   {out->status, d.status, S}};
+  for (const Copy& c : d2h) {
+    if (!c.dst) continue;
+    st = cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, e->stream);
+    if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMemcpyAsync(D2H)");
+  }
+  st = cudaStreamSynchronize(e->stream);
+  if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaStreamSynchronize");
+  return CE_OK;
+}
+
+// ---- CUDA graphs ----------------------------------------------------------
+
+int ce_graph_begin(ce_engine* e, void* stream) {
+  if (!e) return CE_ERR_INVALID;
+  if (!stream) return ce::fail(e, CE_ERR_INVALID, "ce_graph_begin: capture needs a non-default stream");
+  cudaError_t st = cudaSetDevice(e->device);
+  if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaSetDevice");
+  st = cudaStreamBeginCapture(static_cast<cudaStream_t>(stream), cudaStreamCaptureModeThreadLocal);
+  if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaStreamBeginCapture");
+  return CE_OK;
+}
+
+int ce_graph_end(ce_engine* e, void* stream, ce_graph** out) {
+  if (!e || !out) return CE_ERR_INVALID;
+  *out = nullptr;
+  cudaGraph_t g = nullptr;
+  cudaError_t st = cudaStreamEndCapture(static_cast<cudaStream_t>(stream), &g);
+  if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaStreamEndCapture");
+  cudaGraphExec_t x = nullptr;
+  st = cudaGraphInstantiate(&x, g, 0);
+  if (st != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return ce::cuda_fail(e, st, "cudaGraphInstantiate");
+  }
+  ce_graph* h = new ce_graph();
+  h->graph = g;
+  h->exec = x;
+  h->device = e->device;
+  *out = h;
+  return CE_OK;
+}
+
+int ce_graph_launch(ce_graph* g, void* stream) {
+  if (!g) return CE_ERR_INVALID;
+  if (cudaSetDevice(g->device) != cudaSuccess) return CE_ERR_CUDA;
+  return cudaGraphLaunch(g->exec, static_cast<cudaStream_t>(stream)) == cudaSuccess ? CE_OK : CE_ERR_CUDA;
+}
+
+void ce_graph_destroy(ce_graph* g) {
+  if (!g) return;
+  cudaSetDevice(g->device);
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  delete g;
+}
+
+}  // extern "C"
+
+// ---- autotuner ------------------------------------------------------------
+
+namespace {
+
+// Time one call on the engine's stream (after one untimed warm-up call).
+template <typename F>
+int time_call(ce_engine* e, F&& call, double* ms_out) {
+  cudaEvent_t a, b;
+  if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) return CE_ERR_CUDA;
+  int rc = call();
+  if (rc == CE_OK) {
+    cudaEventRecord(a, e->stream);
+    rc = call();
+    cudaEventRecord(b, e->stream);
+    if (rc == CE_OK && cudaEventSynchronize(b) != cudaSuccess) rc = CE_ERR_CUDA;
+    float ms = 0.0f;
+    if (rc == CE_OK) cudaEventElapsedTime(&ms, a, b);
+    *ms_out = ms;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return rc;
+}
+
+struct Outputs {
+  void* mem = nullptr;
+  ce_outputs o{};
+};
+
+int alloc_outputs(ce_engine* e, uint64_t S, int atoms_per_row, Outputs* out) {
+  const size_t mom = S * atoms_per_row * 3 * sizeof(float);
+  const size_t total = mom + S * (sizeof(double) + sizeof(uint32_t) + 1) + 1024;
+  cudaError_t st = cudaMalloc(&out->mem, total);
+  if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMalloc(autotune outputs)");
+  char* p = static_cast<char*>(out->mem);
+  out->o.momenta = reinterpret_cast<float*>(p);
+  p += (mom + 255) & ~static_cast<size_t>(255);
+  out->o.ker = reinterpret_cast<double*>(p);
+  p += ((S * sizeof(double)) + 255) & ~static_cast<size_t>(255);
+  out->o.steps = reinterpret_cast<uint32_t*>(p);
+  p += ((S * sizeof(uint32_t)) + 255) & ~static_cast<size_t>(255);
+  out->o.status = reinterpret_cast<uint8_t*>(p);
+  return CE_OK;
+}
+
+void record(ce_tune_result* report, int cap, int* n, const ce_tuning& t, double rate, int schedule) {
+  if (report && *n < cap) {
+    report[*n].t = t;
+    report[*n].sims_per_s = rate;
+    report[*n].schedule = schedule;
+  }
+  ++*n;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ce_autotune_fixed(ce_engine* e, uint64_t S, const float* pos_dev, const ce_run_config* cfg,
+                      ce_tune_result* report, int cap, int* n_report) {
+  if (!e || !pos_dev || !cfg || S == 0) return CE_ERR_INVALID;
+  if (!e->has_mol) return ce::fail(e, CE_ERR_STATE, "ce_autotune_fixed: no molecule set");
+  if (cudaSetDevice(e->device) != cudaSuccess) return CE_ERR_CUDA;
+  Outputs out;
+  int rc = alloc_outputs(e, S, e->n, &out);
+  if (rc != CE_OK) return rc;
+  const ce_tuning saved = e->tuning;
+  e->tuned_fixed[e->n].valid = false;
+  std::vector<int> layouts = {1};
+  if (e->n >= 2) layouts.push_back(e->n);
+  const int blocks[] = {64, 128, 256};
+  const int refills[] = {1, 2, 4};
+  double best = -1.0;
+  ce_tuning best_t{};
+  int count = 0;
+  for (int L : layouts)
+    for (int B : blocks)
+      for (int R : refills) {
+        ce_tuning t{B, 0, R, L};
+        e->tuning = t;
+        double ms = 0.0;
+        rc = time_call(e, [&] { return ce_run_device(e, S, pos_dev, cfg, &out.o, e->stream); }, &ms);
+        if (rc != CE_OK) break;
+        const double rate = ms > 0.0 ? static_cast<double>(S) / (ms * 1e-3) : 0.0;
+        record(report, cap, &count, t, rate, CE_SCHEDULE_ONE_LAUNCH);
+        if (rate > best) {
+          best = rate;
+          best_t = t;
+        }
+      }
+  e->tuning = saved;
+  cudaFree(out.mem);
+  if (rc != CE_OK) return rc;
+  e->tuned_fixed[e->n].valid = true;
+  e->tuned_fixed[e->n].t = best_t;
+  if (n_report) *n_report = std::min(count, cap);
+  return CE_OK;
+}
+
+int ce_autotune_mixed(ce_engine* e, uint64_t S, const ce_mixed_batch* dev_in, double coulomb_k,
+                      const ce_run_config* cfg, ce_tune_result* report, int cap, int* n_report, int* best_schedule) {
+  if (!e || !dev_in || !cfg || S == 0) return CE_ERR_INVALID;
+  if (cudaSetDevice(e->device) != cudaSuccess) return CE_ERR_CUDA;
+  int rc = ce_reserve_mixed(e, S);
+  if (rc != CE_OK) return rc;
+  Outputs out;
+  rc = alloc_outputs(e, S, CE_MAX_ATOMS, &out);
+  if (rc != CE_OK) return rc;
+  const ce_tuning saved = e->tuning;
+  e->tuned_mixed.valid = false;
+  const int blocks[] = {64, 128, 256};
+  const int refills[] = {1, 2, 4};
+  const int schedules[] = {CE_SCHEDULE_ONE_LAUNCH, CE_SCHEDULE_PER_SIZE};
+  double best = -1.0;
+  ce_tuning best_t{};
+  int best_s = CE_SCHEDULE_ONE_LAUNCH;
+  int count = 0;
+  for (int sch : schedules)
+    for (int B : blocks)
+      for (int R : refills) {
+        ce_tuning t{B, 0, R, 0};
+        e->tuning = t;
+        double ms = 0.0;
+        rc = time_call(e, [&] { return ce_run_mixed_device(e, S, dev_in, coulomb_k, cfg, &out.o, sch, e->stream); },
+                       &ms);
+        if (rc != CE_OK) break;
+        const double rate = ms > 0.0 ? static_cast<double>(S) / (ms * 1e-3) : 0.0;
+        record(report, cap, &count, t, rate, sch);
+        if (rate > best) {
+          best = rate;
+          best_t = t;
+          best_s = sch;
+        }
+      }
+  e->tuning = saved;
+  cudaFree(out.mem);
+  if (rc != CE_OK) return rc;
+  e->tuned_mixed.valid = true;
+  e->tuned_mixed.t = best_t;
+  if (best_schedule) *best_schedule = best_s;
+  if (n_report) *n_report = std::min(count, cap);
+  return CE_OK;
+}
+
+}  // extern "C"

@@ -7,20 +7,27 @@
 // x, v and six stage accelerations (~3x fewer registers than a whole sim per
 // thread), so occupancy is high and N = 10 needs no spills.
 //
-// Per force evaluation a lane publishes (x, y, z, k q_i) to its slot of a
-// per-warp shared-memory buffer (double-buffered, one __syncwarp per
-// evaluation) and reads its N-1 partners with 16-byte loads; the partner set is
-// fixed per lane, so there is no self pair. The pair term is computed twice
-// (once on each side) instead of using Newton's third law. Sums over a
-// simulation (error norm, potential, kinetic energy, Hairer norms) are
-// gathered with N shuffles in a fixed order, so every lane of a group holds the
-// bit-identical value and takes the same accept/reject and stop decisions.
+// Per force evaluation a lane publishes (x, y, z) to its slot of a per-warp
+// shared-memory buffer (three rotating buffers, one __syncwarp per evaluation)
+// and reads its N-1 partners with 16-byte loads; the partner set is fixed per
+// lane, so there is no self pair, and the lane's pair constants k q_i q_j sit in
+// registers. The pair term is computed on both sides instead of using Newton's
+// third law. Sums over a simulation (error norm, potential, kinetic energy,
+// Hairer norms) are gathered with N shuffles in a fixed order, so every lane of
+// a group holds the bit-identical value and takes the same accept/reject and
+// stop decisions.
 //
 // Control flow is warp-uniform: every lane executes every attempt (lanes whose
 // simulation is finished, or that carry no atom, compute on stale data and
 // commit nothing), which keeps the shared-memory exchange fully synchronised.
-// The six stage force evaluations share one copy of the code (rolled stage
-// loop, coefficients from constant memory), which keeps the hot loop small.
+// The stage loop is unrolled: a lane carries three components, so the six
+// force loops stay small and every coefficient is a compile-time operand.
+//
+// One warp loop (atom_loop<N, MODE, MIXED>) serves three kernels:
+//   rk45_atom_kernel<N, MODE>    one fixed molecule (include/ce_gpu.h ce_run*)
+//   rk45_mixed_kernel<MODE>      mixed 2..10-atom molecules, one persistent
+//                                launch walking the size buckets 10 -> 2
+//   rk45_bucket_kernel<N, MODE>  one size bucket (the per-size launch schedule)
 #pragma once
 
 #include <cstdint>
@@ -32,6 +39,9 @@
 
 namespace ce {
 
+constexpr int kMixedStride = CE_MAX_ATOMS;  // atoms per sim row in the mixed layout
+constexpr int kAtomBufSlots = 96;           // float4 per warp: three 32-slot buffers
+
 template <int N>
 struct AtomShape {
   static constexpr int G = 32 / N;     // simulations per warp
@@ -39,10 +49,25 @@ struct AtomShape {
 };
 
 struct AtomConsts {
-  float qi;      // q_i (pair constant = q_i * (k q_j))
-  float kqi;     // k q_i, published with the position
   float inv_m;   // 1 / m_i
   double mass;   // m_i
+};
+
+// Per-sim molecule arrays of the mixed layout (rows of kMixedStride atoms).
+struct MixedIn {
+  const uint8_t* n_per;   // [S] atoms per sim
+  const double* mass;     // [S][10] electron masses
+  const double* charge;   // [S][10]
+  double coulomb_k;
+};
+
+// Size buckets produced by the device counting sort (ce_gpu.cu): sims of size n
+// are perm[off[n] .. off[n] + cnt[n]); cursor[n] is that bucket's work queue.
+struct Buckets {
+  const uint32_t* perm;
+  const unsigned long long* off;  // [11]
+  const unsigned long long* cnt;  // [11]
+  unsigned long long* cursor;     // [11]
 };
 
 // Fixed-order sum over the N lanes [base, base + N) of a group; every lane of
@@ -70,16 +95,17 @@ struct AtomLane {
   unsigned long long sim;
 };
 
-// One force evaluation for every lane of the warp: publish (xs, kq_i), read the
-// N-1 partners, accumulate a_i and (optionally) this lane's half of the pair
-// potential. `slot` is this lane's buffer index, `nbr[d]` the partners'.
+// One force evaluation for every lane of the warp: publish xs, read the N-1
+// partners, accumulate a_i and (optionally) this lane's half of the pair
+// potential. `which` (0..2) selects one of three 32-slot buffers; consecutive
+// calls always use different buffers, so a lane never overwrites a slot that a
+// slower lane is still reading from the previous evaluation.
 template <int N, typename Acc>
-__device__ __forceinline__ void lane_force(float4* __restrict__ buf, int& par, int slot, const int (&nbr)[N - 1],
-                                           const float (&xs)[3], const AtomConsts& ac, bool want_pe,
-                                           float (&a)[3], Acc& pe_half) {
-  float4* b = buf + par * 32;
-  par ^= 1;
-  b[slot] = make_float4(xs[0], xs[1], xs[2], ac.kqi);
+__device__ __forceinline__ void lane_force(float4* __restrict__ buf, int which, int slot, const int (&nbr)[N - 1],
+                                           const float (&pcv)[N - 1], const float (&xs)[3], const AtomConsts& ac,
+                                           bool want_pe, float (&a)[3], Acc& pe_half) {
+  float4* b = buf + which * 32;
+  b[slot] = make_float4(xs[0], xs[1], xs[2], 0.0f);
   __syncwarp();
   float ax = 0.0f, ay = 0.0f, az = 0.0f;
   Acc pe = Acc(0);
@@ -91,7 +117,7 @@ __device__ __forceinline__ void lane_force(float4* __restrict__ buf, int& par, i
     const float rz = xs[2] - o.z;
     const float d2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
     const float rinv = rsqrtf(d2);
-    const float u = (ac.qi * o.w) * rinv;  // k q_i q_j / r
+    const float u = pcv[d] * rinv;  // k q_i q_j / r
     if (want_pe) pe += static_cast<Acc>(u);
     const float s = u * (rinv * rinv);
     ax = fmaf(rx, s, ax);
@@ -107,7 +133,7 @@ __device__ __forceinline__ void lane_force(float4* __restrict__ buf, int& par, i
 // FP64 finalize, executed by every lane of the warp (the reductions are full-warp
 // shuffles); lanes with status < 0 compute but write nothing. Each finishing
 // lane writes its atom's momentum, lane i = 0 of the group the per-sim scalars.
-template <int N, int MODE>
+template <int N, int MODE, int STRIDE>
 __device__ __forceinline__ void atom_finalize(const AtomLane<N, MODE>& s, int status, double pe_final,
                                               const AtomConsts& ac, int ai, int base, const RunParams& P) {
   const double vx = s.v[0], vy = s.v[1], vz = s.v[2];
@@ -119,7 +145,7 @@ __device__ __forceinline__ void atom_finalize(const AtomLane<N, MODE>& s, int st
   const double px = mm * vx, py = mm * vy, pz = mm * vz;
   const double ker = gsum<N>((px * px + py * py + pz * pz) / (2.0 * ac.mass), base);
   if (status < 0) return;
-  float* dst = P.momenta + s.sim * (3ull * N) + 3 * ai;
+  float* dst = P.momenta + s.sim * (3ull * STRIDE) + 3 * ai;
   dst[0] = static_cast<float>(px);
   dst[1] = static_cast<float>(py);
   dst[2] = static_cast<float>(pz);
@@ -134,16 +160,19 @@ __device__ __forceinline__ void atom_finalize(const AtomLane<N, MODE>& s, int st
   }
 }
 
-// Persistent lane-per-atom kernel for one fixed molecule. Block = 32 * W
-// threads; each warp owns 2 x 32 float4 of shared memory.
-template <int N, int MODE>
-__global__ void __launch_bounds__(256) rk45_atom_kernel(const RunParams P, const FixedMol M) {
+// The warp loop: keep this warp's G groups busy with sims of exactly N atoms
+// drawn from one work queue (cursor over [0, count), mapped through perm when
+// non-null) until the queue is empty and every group has finished. MIXED reads
+// each sim's masses and charges from X; otherwise the fixed molecule M.
+template <int N, int MODE, bool MIXED>
+__device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M, const MixedIn& X,
+                                          unsigned long long* cursor, unsigned long long count,
+                                          const uint32_t* perm, float4* buf) {
   using L = AtomLane<N, MODE>;
   using Acc = typename L::Acc;
   constexpr int G = AtomShape<N>::G;
   constexpr int USED = AtomShape<N>::USED;
-  extern __shared__ float4 smem_pos[];
-  float4* buf = smem_pos + (threadIdx.x >> 5) * 64;
+  constexpr int STRIDE = MIXED ? kMixedStride : N;
   const int lane = static_cast<int>(threadIdx.x & 31u);
   const bool has_atom = lane < USED;
   const int g = has_atom ? lane / N : G;  // idle lanes form their own (empty) group
@@ -151,17 +180,27 @@ __global__ void __launch_bounds__(256) rk45_atom_kernel(const RunParams P, const
   const int base = has_atom ? g * N : lane;
   const bool leader = has_atom && ai == 0;
   int nbr[N - 1];
+  int pidx[N - 1];  // partner atom index j for each d
 #pragma unroll
   for (int d = 0; d < N - 1; ++d) {
     int j = ai + 1 + d;
     if (j >= N) j -= N;
+    pidx[d] = j;
     nbr[d] = has_atom ? base + j : lane;
   }
   AtomConsts ac;
-  ac.qi = M.q[ai];
-  ac.kqi = M.kq[ai];
-  ac.inv_m = M.inv_m[ai];
-  ac.mass = M.mass[ai];
+  float pcv[N - 1];
+  if (!MIXED) {
+    ac.inv_m = M.inv_m[ai];
+    ac.mass = M.mass[ai];
+#pragma unroll
+    for (int d = 0; d < N - 1; ++d) pcv[d] = M.pc[ai * N + pidx[d]];
+  } else {
+    ac.inv_m = 1.0f;
+    ac.mass = 1.0;
+#pragma unroll
+    for (int d = 0; d < N - 1; ++d) pcv[d] = 0.0f;
+  }
   L s;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
@@ -174,9 +213,8 @@ __global__ void __launch_bounds__(256) rk45_atom_kernel(const RunParams P, const
   s.steps = s.rejects = s.rej_in_step = 0u;
   s.rej_once = false;
   s.sim = 0ull;
-  int par = 0;
   bool active = false;
-  bool queue_empty = false;
+  bool queue_empty = count == 0ull;
   const unsigned lt_mask = (1u << lane) - 1u;
 
   for (;;) {
@@ -188,22 +226,22 @@ __global__ void __launch_bounds__(256) rk45_atom_kernel(const RunParams P, const
       const int cnt = __popc(idle);
       const int first = __ffs(idle) - 1;
       unsigned long long b0 = 0ull;
-      if (lane == first) b0 = atomicAdd(P.cursor, static_cast<unsigned long long>(cnt));
+      if (lane == first) b0 = atomicAdd(cursor, static_cast<unsigned long long>(cnt));
       b0 = __shfl_sync(0xffffffffu, b0, first);
-      queue_empty = (b0 + static_cast<unsigned long long>(cnt) >= P.S);
+      queue_empty = (b0 + static_cast<unsigned long long>(cnt) >= count);
       unsigned long long mine = ~0ull;
       if (leader && !active) mine = b0 + static_cast<unsigned long long>(__popc(idle & lt_mask));
       mine = __shfl_sync(0xffffffffu, mine, base);
-      if (has_atom && !active && mine < P.S) {
+      if (has_atom && !active && mine < count) {
         fresh = true;
-        s.sim = mine;
+        s.sim = perm ? static_cast<unsigned long long>(perm[mine]) : mine;
       }
     }
     // ---- init of freshly claimed sims (all lanes take part in the exchange) ----
     if (__ballot_sync(0xffffffffu, fresh) != 0u) {
       int fin_st = -1;
       if (fresh) {
-        const float* src = P.pos + s.sim * (3ull * N) + 3 * ai;
+        const float* src = P.pos + s.sim * (3ull * STRIDE) + 3 * ai;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           s.x[c] = __ldg(src + c);
@@ -211,9 +249,27 @@ __global__ void __launch_bounds__(256) rk45_atom_kernel(const RunParams P, const
           s.cx[c] = s.cv[c] = 0.0f;
         }
       }
+      if (MIXED) {
+        // This sim's constants: pair constants (k q_i) q_j formed in double and
+        // narrowed, as the fixed path does (batched_integrator.hpp:79-87).
+        double qi = 0.0, mi = 1.0;
+        if (fresh) {
+          qi = __ldg(X.charge + s.sim * kMixedStride + ai);
+          mi = __ldg(X.mass + s.sim * kMixedStride + ai);
+        }
+#pragma unroll
+        for (int d = 0; d < N - 1; ++d) {
+          const double qj = __shfl_sync(0xffffffffu, qi, nbr[d]);
+          if (fresh) pcv[d] = static_cast<float>(X.coulomb_k * qi * qj);
+        }
+        if (fresh) {
+          ac.mass = mi;
+          ac.inv_m = static_cast<float>(1.0 / mi);
+        }
+      }
       float a0[3];
       Acc peh;
-      lane_force<N, Acc>(buf, par, lane, nbr, s.x, ac, true, a0, peh);
+      lane_force<N, Acc>(buf, 2, lane, nbr, pcv, s.x, ac, true, a0, peh);  // stages use buffers 1, 0, 1, ...
       const Acc pe0 = gsum<N>(peh, base) * Acc(0.5);
       // Hairer norms from rest (sv = atol, probe accelerations = k1).
       float d0p = 0.0f, d1p = 0.0f;
@@ -262,7 +318,7 @@ __global__ void __launch_bounds__(256) rk45_atom_kernel(const RunParams P, const
         if (fin_st >= 0) active = false;
       }
       if (__ballot_sync(0xffffffffu, fin_st >= 0) != 0u)
-        atom_finalize<N, MODE>(s, fin_st, static_cast<double>(pe0), ac, ai, base, P);
+        atom_finalize<N, MODE, STRIDE>(s, fin_st, static_cast<double>(pe0), ac, ai, base, P);
     }
     if (__ballot_sync(0xffffffffu, active) == 0u) {
       if (queue_empty) break;
@@ -274,16 +330,14 @@ __global__ void __launch_bounds__(256) rk45_atom_kernel(const RunParams P, const
     float xs[3], a[3];
     float cxn[3] = {0.0f, 0.0f, 0.0f};
     Acc pe_half = Acc(0);
-#pragma unroll 1
+#pragma unroll
     for (int si = 1; si <= 6; ++si) {
-      const float cs = c_c[si + 1];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         float sum = 0.0f;
 #pragma unroll
-        for (int l = 0; l < 5; ++l)
-          if (l + 1 < si) sum = fmaf(c_abar[si + 1][l + 1], s.k[l][c], sum);
-        const float inc = hh * fmaf(hh, sum, cs * s.v[c]);
+        for (int l = 0; l + 1 < si; ++l) sum = fmaf(c_abar[si + 1][l + 1], s.k[l][c], sum);
+        const float inc = hh * fmaf(hh, sum, c_c[si + 1] * s.v[c]);
         if (L::kKahan && si == 6) {
           const float y = inc - s.cx[c];
           xs[c] = s.x[c] + y;
@@ -292,14 +346,10 @@ __global__ void __launch_bounds__(256) rk45_atom_kernel(const RunParams P, const
           xs[c] = s.x[c] + inc;
         }
       }
-      lane_force<N, Acc>(buf, par, lane, nbr, xs, ac, si == 6, a, pe_half);
-      switch (si) {
-        case 1: s.k[1][0] = a[0]; s.k[1][1] = a[1]; s.k[1][2] = a[2]; break;
-        case 2: s.k[2][0] = a[0]; s.k[2][1] = a[1]; s.k[2][2] = a[2]; break;
-        case 3: s.k[3][0] = a[0]; s.k[3][1] = a[1]; s.k[3][2] = a[2]; break;
-        case 4: s.k[4][0] = a[0]; s.k[4][1] = a[1]; s.k[4][2] = a[2]; break;
-        case 5: s.k[5][0] = a[0]; s.k[5][1] = a[1]; s.k[5][2] = a[2]; break;
-        default: break;
+      lane_force<N, Acc>(buf, si & 1, lane, nbr, pcv, xs, ac, si == 6, a, pe_half);
+      if (si <= 5) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) s.k[si][c] = a[c];
       }
     }
     // Stage 7 done: xs = x_new, a = k7. Velocity update and error estimate.
@@ -368,8 +418,58 @@ __global__ void __launch_bounds__(256) rk45_atom_kernel(const RunParams P, const
       if (fin_st >= 0) active = false;
     }
     if (__ballot_sync(0xffffffffu, fin_st >= 0) != 0u)
-      atom_finalize<N, MODE>(s, fin_st, static_cast<double>(pe_new), ac, ai, base, P);
+      atom_finalize<N, MODE, STRIDE>(s, fin_st, static_cast<double>(pe_new), ac, ai, base, P);
   }
+}
+
+// Persistent lane-per-atom kernel for one fixed molecule. Block = 32 * W
+// threads; each warp owns kAtomBufSlots float4 of dynamic shared memory.
+template <int N, int MODE>
+__global__ void __launch_bounds__(256) rk45_atom_kernel(const RunParams P, const FixedMol M) {
+  extern __shared__ float4 smem_pos[];
+  float4* buf = smem_pos + (threadIdx.x >> 5) * kAtomBufSlots;
+  const MixedIn none{};
+  atom_loop<N, MODE, false>(P, M, none, P.cursor, P.S, nullptr, buf);
+}
+
+// Mixed molecules in one persistent launch: every warp walks the size buckets
+// from 10 atoms down to 2 (the longest simulations first, and all warps on the
+// same N at nearly the same time, so one N's code is hot in the instruction
+// cache), serving each bucket from its own queue until it is empty. Capped at
+// the register budget of a single-size kernel (128), which each bucket's loop
+// fits without spilling, so the merged kernel keeps the same occupancy.
+template <int MODE>
+__global__ void __launch_bounds__(256, 2) rk45_mixed_kernel(const RunParams P, const MixedIn X, const Buckets B) {
+  extern __shared__ float4 smem_pos[];
+  float4* buf = smem_pos + (threadIdx.x >> 5) * kAtomBufSlots;
+  const FixedMol none{};
+#pragma unroll 1
+  for (int n = CE_MAX_ATOMS; n >= 2; --n) {
+    const unsigned long long cnt = B.cnt[n];
+    if (cnt == 0ull) continue;
+    const uint32_t* perm = B.perm + B.off[n];
+    unsigned long long* cur = B.cursor + n;
+    switch (n) {
+      case 10: atom_loop<10, MODE, true>(P, none, X, cur, cnt, perm, buf); break;
+      case 9: atom_loop<9, MODE, true>(P, none, X, cur, cnt, perm, buf); break;
+      case 8: atom_loop<8, MODE, true>(P, none, X, cur, cnt, perm, buf); break;
+      case 7: atom_loop<7, MODE, true>(P, none, X, cur, cnt, perm, buf); break;
+      case 6: atom_loop<6, MODE, true>(P, none, X, cur, cnt, perm, buf); break;
+      case 5: atom_loop<5, MODE, true>(P, none, X, cur, cnt, perm, buf); break;
+      case 4: atom_loop<4, MODE, true>(P, none, X, cur, cnt, perm, buf); break;
+      case 3: atom_loop<3, MODE, true>(P, none, X, cur, cnt, perm, buf); break;
+      default: atom_loop<2, MODE, true>(P, none, X, cur, cnt, perm, buf); break;
+    }
+  }
+}
+
+// One size bucket of a mixed batch (the per-size launch schedule).
+template <int N, int MODE>
+__global__ void __launch_bounds__(256) rk45_bucket_kernel(const RunParams P, const MixedIn X, const Buckets B) {
+  extern __shared__ float4 smem_pos[];
+  float4* buf = smem_pos + (threadIdx.x >> 5) * kAtomBufSlots;
+  const FixedMol none{};
+  atom_loop<N, MODE, true>(P, none, X, B.cursor + N, B.cnt[N], B.perm + B.off[N], buf);
 }
 
 using AtomKernelFn = void (*)(RunParams, FixedMol);
@@ -377,5 +477,13 @@ AtomKernelFn atom_kernel_m0(int n);
 AtomKernelFn atom_kernel_m1(int n);
 AtomKernelFn atom_kernel_m2(int n);
 AtomKernelFn atom_kernel_m3(int n);
+
+using MixedKernelFn = void (*)(RunParams, MixedIn, Buckets);
+// mixed_kernel_m*(0) = the one-launch kernel; mixed_kernel_m*(n), n in 2..10 =
+// the single-bucket kernel for n atoms.
+MixedKernelFn mixed_kernel_m0(int n);
+MixedKernelFn mixed_kernel_m1(int n);
+MixedKernelFn mixed_kernel_m2(int n);
+MixedKernelFn mixed_kernel_m3(int n);
 
 }  // namespace ce

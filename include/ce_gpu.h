@@ -53,6 +53,7 @@ extern "C" {
 #define CE_SIM_MAX_STEPS 2    /* max_steps reached first (converged = false,
                                  src/driver.cpp:20-23)                                */
 #define CE_SIM_NONFINITE 3    /* non-finite initial potential energy (NaN input)    */
+#define CE_SIM_BAD_INPUT 4    /* mixed batches: atom count outside 1..10            */
 
 /* ---- precision mode bits (ce_run_config.precision_mode) ---- */
 #define CE_PREC_FP32 0  /* FP32 state, FP32 time and stop test (reference f32 engine)   */
@@ -101,12 +102,12 @@ typedef struct ce_outputs {
   double* ke_before;
 } ce_outputs;
 
-/* Launch-shape knobs picked by the autotuner (0 = engine default). */
+/* Launch-shape knobs (0 = autotuned value if any, else the engine default). */
 typedef struct ce_tuning {
-  int32_t block_threads;    /* threads per block (thread-per-sim: sims per block)   */
+  int32_t block_threads;    /* threads per block, multiple of 32 up to 256          */
   int32_t blocks_per_sm;    /* persistent grid = SMs * this (0: occupancy limit)    */
-  int32_t refill_threshold; /* refill a warp once this many lanes are idle (1..32)  */
-  int32_t lanes_per_sim;    /* 1 = one thread per sim; 0 = engine picks by N        */
+  int32_t refill_threshold; /* refill a warp once this many sims are idle (1..32)   */
+  int32_t lanes_per_sim;    /* 1 = one thread per sim; 2..10 = one lane per atom    */
 } ce_tuning;
 
 /* Engine lifetime. ce_create selects `device` and allocates the engine's small
@@ -136,6 +137,65 @@ int ce_run_device(ce_engine* e, uint64_t S, const float* pos, const ce_run_confi
 
 /* Number of kernel launches the last ce_run / ce_run_device issued. */
 int ce_last_launch_count(const ce_engine* e);
+
+/* ---- mixed molecules ---------------------------------------------------
+ * The reference builds one BatchedRK45 per molecule (all lanes share it,
+ * include/coulomb/batched_force.hpp:8-13) and its scalar driver takes any
+ * Molecule (src/driver.cpp:7); a mixed population therefore takes one reference
+ * call per molecule. These entry points integrate any mix of 1..10-atom
+ * molecules in one call. Rows are padded to CE_MAX_ATOMS atoms:
+ *   n_atoms [S] uint8, mass_me [S][10] double, charge [S][10] double,
+ *   pos [S][10][3] float;  out->momenta [S][10][3] float (rows past n untouched
+ *   except for one-atom and invalid sims, which are zero-filled).
+ * A sim with n outside 1..10 gets status CE_SIM_BAD_INPUT. S < 2^32. */
+typedef struct ce_mixed_batch {
+  const uint8_t* n_atoms;
+  const double* mass_me;
+  const double* charge;
+  const float* pos;
+} ce_mixed_batch;
+
+#define CE_SCHEDULE_ONE_LAUNCH 0 /* one persistent launch walks the size buckets 10 -> 2 */
+#define CE_SCHEDULE_PER_SIZE 1   /* one launch per size bucket, in sequence            */
+
+/* Size the engine's mixed-batch scratch (bucket tables + a 4-byte-per-sim
+ * permutation) for up to S sims, so later calls, and graph captures, allocate
+ * nothing. ce_run_mixed_device grows it on demand outside a capture. */
+int ce_reserve_mixed(ce_engine* e, uint64_t S);
+int ce_run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coulomb_k,
+                        const ce_run_config* cfg, const ce_outputs* out, int schedule, void* stream);
+/* Host buffers, synchronous, one-launch schedule. */
+int ce_run_mixed(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coulomb_k,
+                 const ce_run_config* cfg, const ce_outputs* out);
+
+/* ---- CUDA graphs ---------------------------------------------------------
+ * Capture the engine calls issued on `stream` (non-default) between begin and
+ * end into an instantiated graph; ce_graph_launch replays it on any stream.
+ * The captured calls must not need to grow engine scratch (ce_reserve_mixed). */
+typedef struct ce_graph ce_graph;
+int ce_graph_begin(ce_engine* e, void* stream);
+int ce_graph_end(ce_engine* e, void* stream, ce_graph** out);
+int ce_graph_launch(ce_graph* g, void* stream);
+void ce_graph_destroy(ce_graph* g);
+
+/* ---- autotuner -----------------------------------------------------------
+ * Time candidate launch shapes on the device -- threads per block (sims per
+ * block), refill granularity, and for the fixed path the layout (one thread per
+ * sim or one lane per atom) -- over the caller's device inputs, and keep the
+ * fastest in the engine; it then applies wherever the matching ce_tuning field
+ * is 0 (fixed path: per atom count; mixed path: one entry, plus the faster
+ * schedule in *best_schedule). `report` (may be NULL) receives up to `cap`
+ * candidates with their measured sims/s; *n_report their number. */
+typedef struct ce_tune_result {
+  ce_tuning t;
+  double sims_per_s;
+  int32_t schedule;
+} ce_tune_result;
+int ce_autotune_fixed(ce_engine* e, uint64_t S, const float* pos_dev, const ce_run_config* cfg,
+                      ce_tune_result* report, int cap, int* n_report);
+int ce_autotune_mixed(ce_engine* e, uint64_t S, const ce_mixed_batch* dev_in, double coulomb_k,
+                      const ce_run_config* cfg, ce_tune_result* report, int cap, int* n_report,
+                      int* best_schedule);
 
 /* ce_run_device for callers that cannot allocate device memory. No counterpart
  * in the reference. It needs no engine: the molecule comes with the call, the

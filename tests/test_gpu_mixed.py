@@ -1,0 +1,172 @@
+"""Mixed 2..10-atom batches (one persistent launch over size buckets, or one
+launch per size), CUDA-graph capture and the autotuner, through the C ABI.
+
+Parity bar as in test_gpu_parity.py: at the tight point every sim within 1e-5
+config-norm relative momentum error of the reference engine (golden mixed set:
+the reference's scalar engine run per molecule) and of the oracle.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+
+pytestmark = pytest.mark.gpu
+
+TIGHT_MAX = 1e-5
+
+
+def tight(ce, wl, mode=3, **kw):
+    r, a, p = wl.TIGHT
+    return ce.RunConfig(rtol=r, atol=a, pe_stop_fraction=p, precision_mode=mode, **kw)
+
+
+def per_sim_err(r, ref, n_per):
+    errs = []
+    for s, n in enumerate(n_per):
+        errs.append(ol.config_norm_error(r.momenta[s:s + 1, :n], ref[s:s + 1, :n])[0])
+    return np.array(errs)
+
+
+@pytest.mark.parametrize("bits", [32, 64])
+def test_mixed_golden_matches_reference_engine(engine, ce, wl, golden_mixed, bits):
+    g = golden_mixed
+    r = engine.run_mixed(g["n_per"], g["masses"], g["charges"], g["pos"], tight(ce, wl))
+    assert (r.status == 0).all()
+    err = per_sim_err(r, g[f"p_tight_f{bits}"], g["n_per"])
+    assert err.max() <= TIGHT_MAX, err.max()
+
+
+def test_mixed_matches_oracle_and_padding(engine, ce, wl):
+    n_per, m, q, pos = wl.sample_mixed(3000, seed=31)
+    r = engine.run_mixed(n_per, m, q, pos, tight(ce, wl))
+    o = ol.run_batch_mixed(n_per, m, q, pos.astype(np.float32).astype(np.float64), bits=64, rtol=wl.TIGHT[0],
+                           atol=wl.TIGHT[1], pe_stop=wl.TIGHT[2])
+    assert (r.status == 0).all()
+    assert per_sim_err(r, o["momenta"], n_per).max() <= TIGHT_MAX
+    np.testing.assert_allclose(r.ker, o["ker"], rtol=1e-6)
+    # rows past each sim's atom count are untouched (zero here)
+    for n in range(2, 10):
+        assert not r.momenta[n_per == n][:, n:].any()
+
+
+def test_mixed_equals_fixed_molecule_path(engine, ce, wl):
+    # A mixed batch of one molecule is bit-identical to the fixed-molecule
+    # lane-per-atom path (same pair constants, same arithmetic).
+    mol = wl.CH4
+    S = 2000
+    pos5 = wl.sample_molecule(mol, S, seed=32).astype(np.float32)
+    n_per = np.full(S, 5, np.uint8)
+    m = np.ones((S, 10))
+    q = np.zeros((S, 10))
+    m[:, :5] = mol.masses_me
+    q[:, :5] = mol.charge_array
+    pos = np.zeros((S, 10, 3), np.float32)
+    pos[:, :5] = pos5
+    rm = engine.run_mixed(n_per, m, q, pos, tight(ce, wl))
+    engine.set_molecule(mol.masses_me, mol.charge_array)
+    engine.set_tuning(lanes_per_sim=5)
+    try:
+        rf = engine.run(pos5, tight(ce, wl))
+    finally:
+        engine.set_tuning()
+    np.testing.assert_array_equal(rm.momenta[:, :5], rf.momenta)
+    np.testing.assert_array_equal(rm.steps, rf.steps)
+    np.testing.assert_array_equal(rm.ker, rf.ker)
+
+
+def test_one_atom_and_invalid_counts(engine, ce, wl):
+    n_per, m, q, pos = wl.sample_mixed(64, seed=33)
+    n_per = n_per.copy()
+    n_per[3] = 1
+    n_per[5] = 0
+    n_per[7] = 11
+    r = engine.run_mixed(n_per, m, q, pos, tight(ce, wl))
+    assert r.status[3] == ce.CE_SIM_OK and r.steps[3] == 0 and not r.momenta[3].any() and r.ker[3] == 0.0
+    assert r.status[5] == ce.CE_SIM_BAD_INPUT and r.status[7] == ce.CE_SIM_BAD_INPUT
+    ok = np.ones(64, bool)
+    ok[[3, 5, 7]] = False
+    assert (r.status[ok] == 0).all()
+
+
+def _device_batch(torch, ce, n_per, m, q, pos):
+    d = dict(n=torch.from_numpy(np.ascontiguousarray(n_per, np.uint8)).cuda(),
+             m=torch.from_numpy(np.ascontiguousarray(m, np.float64)).cuda(),
+             q=torch.from_numpy(np.ascontiguousarray(q, np.float64)).cuda(),
+             x=torch.from_numpy(np.ascontiguousarray(pos, np.float32)).cuda())
+    b = ce.CeMixedBatch(d["n"].data_ptr(), d["m"].data_ptr(), d["q"].data_ptr(), d["x"].data_ptr())
+    return d, b
+
+
+def _device_out(torch, ce, S):
+    d = dict(m=torch.zeros((S, 10, 3), dtype=torch.float32, device="cuda"),
+             k=torch.zeros(S, dtype=torch.float64, device="cuda"),
+             s=torch.zeros(S, dtype=torch.int32, device="cuda"),
+             t=torch.zeros(S, dtype=torch.uint8, device="cuda"))
+    o = ce.CeOutputs(d["m"].data_ptr(), d["k"].data_ptr(), d["s"].data_ptr(), d["t"].data_ptr(), None, None, None,
+                     None)
+    return d, o
+
+
+def test_schedules_and_graph_replay_are_bit_identical(engine, ce, wl):
+    torch = pytest.importorskip("torch")
+    S = 5000
+    n_per, m, q, pos = wl.sample_mixed(S, seed=34)
+    keep, batch = _device_batch(torch, ce, n_per, m, q, pos)
+    cfg = tight(ce, wl)
+    stream = torch.cuda.Stream()
+    outs = []
+    for sched in (ce.CE_SCHEDULE_ONE_LAUNCH, ce.CE_SCHEDULE_PER_SIZE):
+        d, o = _device_out(torch, ce, S)
+        engine.run_mixed_device(S, batch, cfg, o, sched, stream.cuda_stream)
+        stream.synchronize()
+        outs.append({k: v.cpu().numpy() for k, v in d.items()})
+    for k in outs[0]:
+        np.testing.assert_array_equal(outs[0][k], outs[1][k])
+    # capture the one-launch call into a graph and replay it twice
+    engine.reserve_mixed(S)
+    d, o = _device_out(torch, ce, S)
+    engine.graph_begin(stream.cuda_stream)
+    engine.run_mixed_device(S, batch, cfg, o, ce.CE_SCHEDULE_ONE_LAUNCH, stream.cuda_stream)
+    g = engine.graph_end(stream.cuda_stream)
+    try:
+        for _ in range(2):
+            d["m"].zero_()
+            torch.cuda.synchronize()
+            g.launch(stream.cuda_stream)
+            stream.synchronize()
+            np.testing.assert_array_equal(d["m"].cpu().numpy(), outs[0]["m"])
+            np.testing.assert_array_equal(d["s"].cpu().numpy(), outs[0]["s"])
+    finally:
+        g.close()
+
+
+def test_autotuner_picks_a_measured_candidate_and_keeps_results(ce, wl):
+    torch = pytest.importorskip("torch")
+    engine = ce.Engine(0)  # its own engine: tuned entries stay out of the shared one
+    S = 20000
+    n_per, m, q, pos = wl.sample_mixed(S, seed=35)
+    keep, batch = _device_batch(torch, ce, n_per, m, q, pos)
+    cfg = tight(ce, wl)
+    stream = torch.cuda.Stream()
+    d0, o0 = _device_out(torch, ce, S)
+    engine.run_mixed_device(S, batch, cfg, o0, ce.CE_SCHEDULE_ONE_LAUNCH, stream.cuda_stream)
+    stream.synchronize()
+    report, best = engine.autotune_mixed(S, batch, cfg)
+    assert len(report) == 18 and all(r["sims_per_s"] > 0 for r in report)
+    assert best in (ce.CE_SCHEDULE_ONE_LAUNCH, ce.CE_SCHEDULE_PER_SIZE)
+    d1, o1 = _device_out(torch, ce, S)
+    engine.run_mixed_device(S, batch, cfg, o1, best, stream.cuda_stream)
+    stream.synchronize()
+    np.testing.assert_array_equal(d1["m"].cpu().numpy(), d0["m"].cpu().numpy())
+    # fixed path
+    mol = wl.CH4
+    engine.set_molecule(mol.masses_me, mol.charge_array)
+    x = torch.from_numpy(wl.sample_molecule(mol, S, seed=36).astype(np.float32)).cuda()
+    rep = engine.autotune_fixed(S, x.data_ptr(), cfg)
+    assert len(rep) == 18 and {r["lanes_per_sim"] for r in rep} == {1, 5}
+    t = engine.get_tuning()
+    best_f = max(rep, key=lambda r: r["sims_per_s"])
+    assert (t["block_threads"], t["refill_threshold"], t["lanes_per_sim"]) == (
+        best_f["block_threads"], best_f["refill_threshold"], best_f["lanes_per_sim"])
