@@ -83,6 +83,17 @@ class CeTuneResult(C.Structure):
     _fields_ = [("t", CeTuning), ("sims_per_s", C.c_double), ("schedule", C.c_int32)]
 
 
+class CeBallSampler(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("radius", C.c_double), ("min_separation", C.c_double),
+                ("max_attempts", C.c_uint32)]
+
+
+class CeMixedSampler(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("n_min", C.c_int32), ("n_max", C.c_int32), ("radius_coeff", C.c_double),
+                ("min_separation", C.c_double), ("max_attempts", C.c_uint32), ("q_min", C.c_int32),
+                ("q_max", C.c_int32), ("n_species", C.c_int32), ("species_amu", C.c_double * 8)]
+
+
 CE_SIM_BAD_INPUT = 4
 CE_SCHEDULE_ONE_LAUNCH = 0
 CE_SCHEDULE_PER_SIZE = 1
@@ -130,6 +141,17 @@ _SIGNATURES = {
          C.POINTER(CeTuneResult), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)],
         C.c_int,
     ),
+    "ce_sample_ball_device": (
+        [C.c_int, C.c_uint64, C.c_uint64, C.POINTER(CeBallSampler), C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "ce_sample_ball_host": (
+        [C.c_int, C.c_uint64, C.c_uint64, C.POINTER(CeBallSampler), C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "ce_sample_mixed_device": (
+        [C.c_uint64, C.c_uint64, C.POINTER(CeMixedSampler), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+         C.c_void_p, C.c_void_p], C.c_int),
+    "ce_sample_mixed_host": (
+        [C.c_uint64, C.c_uint64, C.POINTER(CeMixedSampler), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+         C.c_void_p, C.c_void_p], C.c_int),
+    "ce_philox4x32_10": ([C.c_void_p, C.c_void_p, C.c_void_p], None),
     "ce_run_device_noalloc": (
         [C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_uint64, C.c_void_p, C.POINTER(CeRunConfig),
          C.POINTER(CeOutputs), C.c_void_p, C.c_char_p, C.c_size_t],

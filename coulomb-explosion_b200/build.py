@@ -28,7 +28,7 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-ftz=true", "-Xcompiler", "
 
 # (object name, source, extra flags)
 UNITS = [("ce_gpu.o", "ce_gpu.cu", []), ("probe.o", "probe.cu", []), ("noalloc.o", "noalloc.cu", []),
-         ("mixed.o", "mixed.cu", [])] + [
+         ("mixed.o", "mixed.cu", []), ("sampler.o", "sampler.cu", ["-Xcompiler", "-ffp-contract=off"])] + [
     (f"kernels_fixed_m{m}.o", "kernels_fixed.cu", [f"-DCE_MODE={m}"]) for m in range(4)
 ] + [(f"kernels_atom_m{m}.o", "kernels_atom.cu", [f"-DCE_MODE={m}"]) for m in range(4)]
 
@@ -41,7 +41,8 @@ def _nvcc() -> str:
 
 
 def _headers() -> list[Path]:
-    return list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.hpp")) + list(INCLUDE.glob("*.h"))
+    return (list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.hpp")) + list(CSRC.glob("*.h"))
+            + list(INCLUDE.glob("*.h")))
 
 
 def _stale(obj: Path, src: Path) -> bool:

@@ -27,6 +27,7 @@ struct ce_engine {
   // Autotuned launch shapes, per atom count (fixed path) and for the mixed path.
   ce_tuned_entry tuned_fixed[CE_MAX_ATOMS + 1];
   ce_tuned_entry tuned_mixed;
+  int tuned_schedule = CE_SCHEDULE_ONE_LAUNCH;  // schedule ce_run_mixed uses (autotuner's pick)
   unsigned long long* d_cursor = nullptr;  // fixed path work-queue head (engine scratch)
   cudaStream_t stream = nullptr;           // stream of the host-buffer paths
   void* d_arena = nullptr;                 // device buffers of the host-buffer paths

@@ -302,7 +302,7 @@ int ce_run_mixed(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coul
     st = cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyHostToDevice, e->stream);
     if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMemcpyAsync(H2D)");
   }
-  rc = ce_run_mixed_device(e, S, &d_in, coulomb_k, cfg, &d, CE_SCHEDULE_ONE_LAUNCH, e->stream);
+  rc = ce_run_mixed_device(e, S, &d_in, coulomb_k, cfg, &d, e->tuned_schedule, e->stream);
   if (rc != CE_OK) return rc;
   const Copy d2h[] = {{out->momenta, d.momenta, S * A * 3 * sizeof(float)}, {out->ker, d.ker, S * sizeof(double)},
                       {out->t_final, d.t_final, S * sizeof(double)},     {out->pe_final, d.pe_final, S * sizeof(double)},
@@ -505,6 +505,7 @@ int ce_autotune_mixed(ce_engine* e, uint64_t S, const ce_mixed_batch* dev_in, do
   if (rc != CE_OK) return rc;
   e->tuned_mixed.valid = true;
   e->tuned_mixed.t = best_t;
+  e->tuned_schedule = best_s;
   if (best_schedule) *best_schedule = best_s;
   if (n_report) *n_report = std::min(count, cap);
   return CE_OK;

@@ -432,17 +432,24 @@ __global__ void __launch_bounds__(256) rk45_atom_kernel(const RunParams P, const
   atom_loop<N, MODE, false>(P, M, none, P.cursor, P.S, nullptr, buf);
 }
 
+// One size bucket of the one-launch mixed kernel, kept out of line so each
+// size gets its own register allocation (inlined into one function, the nine
+// loops together needed ~230 registers; apart, the largest needs 128).
+template <int N, int MODE>
+__device__ __noinline__ void mixed_bucket(const RunParams P, const MixedIn X, unsigned long long* cur,
+                                          unsigned long long cnt, const uint32_t* perm, float4* buf) {
+  const FixedMol none{};
+  atom_loop<N, MODE, true>(P, none, X, cur, cnt, perm, buf);
+}
+
 // Mixed molecules in one persistent launch: every warp walks the size buckets
 // from 10 atoms down to 2 (the longest simulations first, and all warps on the
 // same N at nearly the same time, so one N's code is hot in the instruction
-// cache), serving each bucket from its own queue until it is empty. Capped at
-// the register budget of a single-size kernel (128), which each bucket's loop
-// fits without spilling, so the merged kernel keeps the same occupancy.
+// cache), serving each bucket from its own queue until it is empty.
 template <int MODE>
-__global__ void __launch_bounds__(256, 2) rk45_mixed_kernel(const RunParams P, const MixedIn X, const Buckets B) {
+__global__ void __launch_bounds__(256) rk45_mixed_kernel(const RunParams P, const MixedIn X, const Buckets B) {
   extern __shared__ float4 smem_pos[];
   float4* buf = smem_pos + (threadIdx.x >> 5) * kAtomBufSlots;
-  const FixedMol none{};
 #pragma unroll 1
   for (int n = CE_MAX_ATOMS; n >= 2; --n) {
     const unsigned long long cnt = B.cnt[n];
@@ -450,15 +457,15 @@ __global__ void __launch_bounds__(256, 2) rk45_mixed_kernel(const RunParams P, c
     const uint32_t* perm = B.perm + B.off[n];
     unsigned long long* cur = B.cursor + n;
     switch (n) {
-      case 10: atom_loop<10, MODE, true>(P, none, X, cur, cnt, perm, buf); break;
-      case 9: atom_loop<9, MODE, true>(P, none, X, cur, cnt, perm, buf); break;
-      case 8: atom_loop<8, MODE, true>(P, none, X, cur, cnt, perm, buf); break;
-      case 7: atom_loop<7, MODE, true>(P, none, X, cur, cnt, perm, buf); break;
-      case 6: atom_loop<6, MODE, true>(P, none, X, cur, cnt, perm, buf); break;
-      case 5: atom_loop<5, MODE, true>(P, none, X, cur, cnt, perm, buf); break;
-      case 4: atom_loop<4, MODE, true>(P, none, X, cur, cnt, perm, buf); break;
-      case 3: atom_loop<3, MODE, true>(P, none, X, cur, cnt, perm, buf); break;
-      default: atom_loop<2, MODE, true>(P, none, X, cur, cnt, perm, buf); break;
+      case 10: mixed_bucket<10, MODE>(P, X, cur, cnt, perm, buf); break;
+      case 9: mixed_bucket<9, MODE>(P, X, cur, cnt, perm, buf); break;
+      case 8: mixed_bucket<8, MODE>(P, X, cur, cnt, perm, buf); break;
+      case 7: mixed_bucket<7, MODE>(P, X, cur, cnt, perm, buf); break;
+      case 6: mixed_bucket<6, MODE>(P, X, cur, cnt, perm, buf); break;
+      case 5: mixed_bucket<5, MODE>(P, X, cur, cnt, perm, buf); break;
+      case 4: mixed_bucket<4, MODE>(P, X, cur, cnt, perm, buf); break;
+      case 3: mixed_bucket<3, MODE>(P, X, cur, cnt, perm, buf); break;
+      default: mixed_bucket<2, MODE>(P, X, cur, cnt, perm, buf); break;
     }
   }
 }

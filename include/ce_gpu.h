@@ -164,7 +164,8 @@ typedef struct ce_mixed_batch {
 int ce_reserve_mixed(ce_engine* e, uint64_t S);
 int ce_run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coulomb_k,
                         const ce_run_config* cfg, const ce_outputs* out, int schedule, void* stream);
-/* Host buffers, synchronous, one-launch schedule. */
+/* Host buffers, synchronous; one-launch schedule unless ce_autotune_mixed found
+ * the per-size schedule faster. */
 int ce_run_mixed(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coulomb_k,
                  const ce_run_config* cfg, const ce_outputs* out);
 
