@@ -89,8 +89,51 @@ def build_cuda(verbose: bool = False, ptxas_info: bool = False) -> Path:
     return LIB
 
 
+HOST = PKG / "host"
+BIN = PKG / "bin"
+HOST_LIB = PKG / "libce_host.so"
+CUDA_LIB = Path("/usr/local/cuda/lib64")
+
+
+def _cxx() -> str:
+    for cand in ("/usr/bin/g++", shutil.which("g++")):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("g++ not found")
+
+
+def _run(cmd: list[str]) -> None:
+    p = subprocess.run(cmd, capture_output=True, text=True)
+    if p.returncode != 0:
+        raise RuntimeError(f"build step failed: {' '.join(cmd)}\n{p.stderr}")
+
+
+def build_host() -> None:
+    """libce_host.so (the coulomb:: host API over the C ABI), the dataset
+    generator example and the C++ test driver, linked against libce_gpu.so."""
+    cxx = _cxx()
+    inc = ["-I", str(HOST / "include"), "-I", str(INCLUDE)]
+    flags = ["-std=c++20", "-O2", "-ffp-contract=off", "-Wall", "-Wextra"]
+    srcs = sorted((HOST / "src").glob("*.cpp"))
+    hdrs = list((HOST / "include").rglob("*.hpp")) + list(INCLUDE.glob("*.h"))
+    newest_in = max(p.stat().st_mtime for p in [*srcs, *hdrs, LIB])
+    if not HOST_LIB.exists() or HOST_LIB.stat().st_mtime < newest_in:
+        _run([cxx, *flags, "-fPIC", "-shared", *inc, *map(str, srcs), "-L", str(PKG), "-lce_gpu",
+              "-Wl,-rpath,$ORIGIN", "-o", str(HOST_LIB)])
+    BIN.mkdir(exist_ok=True)
+    progs = {"ce_generate_dataset": HOST / "examples" / "generate_dataset.cpp",
+             "ce_test_host": ROOT / "tests" / "cpp" / "test_host.cpp"}
+    for name, src in progs.items():
+        out = BIN / name
+        if out.exists() and out.stat().st_mtime >= max(src.stat().st_mtime, HOST_LIB.stat().st_mtime):
+            continue
+        _run([cxx, *flags, *inc, "-I", "/usr/local/cuda/include", str(src), "-L", str(PKG), "-lce_host", "-lce_gpu",
+              "-L", str(CUDA_LIB), "-lcudart", "-Wl,-rpath,$ORIGIN/..", "-Wl,-rpath," + str(CUDA_LIB), "-o", str(out)])
+
+
 def build_all(verbose: bool = False) -> None:
     build_cuda(verbose=verbose)
+    build_host()
 
 
 if __name__ == "__main__":
