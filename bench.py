@@ -298,6 +298,80 @@ def run_mixed(args):
     return 0
 
 
+def run_precision(args):
+    """Config-3 study: CH4 and stiff H2O (O q=+3, 2 H q=+1, 2.0-bohr ball, pairs
+    >= 0.3), 1e6 sims each, every precision mode at the production and tight
+    points. Errors against the FP64 reference (oracle f64 at rtol 1e-12 /
+    atol 1e-20 / pe_stop 1e-13) on a 1e4 subset: per-atom |dp_i| / |p_i| and the
+    per-sim config norm; energy drift |KE + PE_final - E0| / E0 before
+    redistribution; accepted steps per sim."""
+    import importlib
+
+    import torch
+
+    from __graft_entry__ import load_package
+
+    ce = load_package()
+    wl = importlib.import_module("coulomb_explosion_b200.workloads")
+    sp = importlib.import_module("coulomb_explosion_b200.sampling")
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_lib as ol
+
+    S = args.sims
+    n_sub = min(10_000, S)
+    eng = ce.Engine(0)
+    rows = []
+    for name, mol in (("CH4", wl.CH4), ("H2O-stiff", wl.H2O_STIFF)):
+        pos, pos64, flags = sp.sample_ball_host(mol, S, seed=SEED)
+        assert not flags.any()
+        sub = np.linspace(0, S - 1, n_sub).astype(np.int64)
+        ref = ol.run_batch(pos[sub].astype(np.float64), mol.masses_me, mol.charge_array, bits=64, rtol=1e-12,
+                           atol=1e-20, pe_stop=1e-13)
+        pe0 = np.array([ol.potential(x, mol.charge_array) for x in pos[sub].astype(np.float64)])
+        eng.set_molecule(mol.masses_me, mol.charge_array)
+        x_d = torch.from_numpy(pos).cuda()
+        for point_name, (rtol, atol, pes) in (("production", wl.PRODUCTION), ("tight", wl.TIGHT)):
+            for mode in (0, 1, 2, 3):
+                cfg = ce.RunConfig(rtol=rtol, atol=atol, pe_stop_fraction=pes, precision_mode=mode)
+                mom = torch.empty((S, mol.n, 3), dtype=torch.float32, device="cuda")
+                ker = torch.empty(S, dtype=torch.float64, device="cuda")
+                stp = torch.empty(S, dtype=torch.int32, device="cuda")
+                sts = torch.empty(S, dtype=torch.uint8, device="cuda")
+                pef = torch.empty(S, dtype=torch.float64, device="cuda")
+                keb = torch.empty(S, dtype=torch.float64, device="cuda")
+                out = ce.CeOutputs(mom.data_ptr(), ker.data_ptr(), stp.data_ptr(), sts.data_ptr(), None, None,
+                                   pef.data_ptr(), keb.data_ptr())
+                stream = torch.cuda.current_stream().cuda_stream
+                eng.run_device(S, x_d.data_ptr(), cfg, out, stream)  # warm-up
+                torch.cuda.synchronize()
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record()
+                eng.run_device(S, x_d.data_ptr(), cfg, out, stream)
+                b.record()
+                torch.cuda.synchronize()
+                ms = a.elapsed_time(b)
+                p = mom.cpu().numpy()[sub].astype(np.float64)
+                atom_err = np.linalg.norm(p - ref["momenta"], axis=2) / np.linalg.norm(ref["momenta"], axis=2)
+                cn = ol.config_norm_error(p, ref["momenta"])
+                drift = np.abs(keb.cpu().numpy()[sub] + pef.cpu().numpy()[sub] - pe0) / pe0
+                rows.append({
+                    "molecule": name, "point": point_name, "rtol": rtol, "atol": atol, "pe_stop": pes,
+                    "mode": {0: "fp32", 1: "fp32+kahan", 2: "fp32+fp64 t/E", 3: "fp32+kahan+fp64 t/E"}[mode],
+                    "explosions_per_s": S / (ms / 1e3),
+                    "atom_rel_err": {"median": float(np.median(atom_err)), "p99": float(np.percentile(atom_err, 99)),
+                                     "max": float(atom_err.max())},
+                    "config_rel_err": {"median": float(np.median(cn)), "p99": float(np.percentile(cn, 99)),
+                                       "max": float(cn.max())},
+                    "energy_drift": {"median": float(np.median(drift)), "max": float(drift.max())},
+                    "mean_steps": float(stp.cpu().numpy().mean()),
+                    "status_ok_frac": float((sts.cpu().numpy() == 0).mean()),
+                })
+    eng.close()
+    print(json.dumps({"metric": "precision study (config 3)", "sims_per_case": S, "fp64_subset": n_sub,
+                      "fp64_reference": "oracle f64, rtol 1e-12, atol 1e-20, pe_stop 1e-13", "rows": rows}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -312,13 +386,15 @@ def main():
                     help="ch4 (the headline workload), c2h6 (10-atom C2H6-like), h2o (stiff H2O)")
     ap.add_argument("--cpu-budget", type=float, default=8.0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="fixed", choices=["fixed", "mixed"],
+    ap.add_argument("--workload", default="fixed", choices=["fixed", "mixed", "precision"],
                     help="fixed: one molecule (--molecule); mixed: 2..10-atom population, one launch vs per size")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
     if args.workload == "mixed":
         return run_mixed(args)
+    if args.workload == "precision":
+        return run_precision(args)
 
     import torch
 
