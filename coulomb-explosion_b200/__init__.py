@@ -152,6 +152,21 @@ _SIGNATURES = {
         [C.c_uint64, C.c_uint64, C.POINTER(CeMixedSampler), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
          C.c_void_p, C.c_void_p], C.c_int),
     "ce_philox4x32_10": ([C.c_void_p, C.c_void_p, C.c_void_p], None),
+    "ce_mlp_create": ([C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_uint64],
+                      C.c_int),
+    "ce_mlp_destroy": ([C.c_void_p], None),
+    "ce_mlp_last_error": ([C.c_void_p], C.c_char_p),
+    "ce_mlp_param_count": ([C.c_void_p], C.c_uint64),
+    "ce_mlp_set_params": ([C.c_void_p, C.c_void_p], C.c_int),
+    "ce_mlp_get_params": ([C.c_void_p, C.c_void_p], C.c_int),
+    "ce_mlp_forward": ([C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p], C.c_int),
+    "ce_mlp_gradients": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
+                          C.c_void_p], C.c_int),
+    "ce_mlp_train_step": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_float, C.c_void_p,
+                           C.c_void_p], C.c_int),
+    "ce_mlp_check": ([C.c_void_p, C.c_void_p], C.c_int),
+    "ce_umma_gemm_f32": ([C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                          C.c_void_p, C.c_void_p], C.c_int),
     "ce_run_device_noalloc": (
         [C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_uint64, C.c_void_p, C.POINTER(CeRunConfig),
          C.POINTER(CeOutputs), C.c_void_p, C.c_char_p, C.c_size_t],
