@@ -372,6 +372,213 @@ def run_precision(args):
     return 0
 
 
+def run_closure(args):
+    """Config-4 study: the learned closure on the mixed 2..10-atom population.
+
+    Training pairs: `--train-sims` sims (default 5e6) integrated to the loose
+    stop (PE <= 5% PE_0, no rescale) and, for targets, to convergence by plain
+    RK45 at the tight point; a seeded 2% of them is held out for validation and
+    gate calibration. The network is trained by the library's tensor-core
+    kernels (Adam, cosine schedule). Serving: `--sims` (default 1e7) further
+    sims from a disjoint Philox counter range, closure (ce_closure_serve) and
+    plain RK45 (ce_run_mixed_device) timed back to back with CUDA events, L2
+    flushed between steps. Errors: per-sim config norm against plain RK45 on
+    every sim and against the FP64 oracle on a subset."""
+    import importlib
+
+    import torch
+
+    from __graft_entry__ import load_package
+
+    ce = load_package()
+    cl = importlib.import_module("coulomb_explosion_b200.closure")
+    sp = importlib.import_module("coulomb_explosion_b200.sampling")
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_lib as ol
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    rtol, atol, pes = TIGHT
+    cfg = ce.RunConfig(rtol=rtol, atol=atol, pe_stop_fraction=pes, precision_mode=args.mode)
+    S_train = args.train_sims
+    S = args.sims if args.sims != S_DEFAULT else 10_000_000
+    mb = args.minibatch
+    eng = ce.Engine(0)
+    seed = SEED + 4
+
+    # ---- training pairs
+    t0 = time.perf_counter()
+    tb = cl.sample_mixed_device(S_train, seed=seed)
+    ts, loose_t, base_t, plain_t = cl.make_training_set(eng, tb, cfg, minibatch=mb)
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t0
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    perm = torch.randperm(S_train, generator=g, device=dev)
+    n_val = max(mb, S_train // 50)
+    val_rows, train_rows = perm[:n_val], perm[n_val:]
+    train_rows = train_rows[ts.valid[train_rows]]
+
+    # ---- training
+    net = cl.Network(max_batch=65536, seed=seed)
+    rep = cl.train(net, ts, epochs=args.epochs, minibatch=mb, lr=args.lr, lr_final=args.lr * 1e-2, seed=seed,
+                   train_rows=train_rows)
+    net.scale_output_layer(1.0 / cl.TARGET_SCALE)
+    losses = np.array(rep.losses)
+
+    # ---- validation: errors of the three closures and gate calibration
+    out_t = cl.net_forward(net, ts.feats)
+    stats = cl.gate_stats(tb, loose_t, base_t, out_t)
+    vmask = torch.zeros(S_train, dtype=torch.bool, device=dev)
+    vmask[val_rows] = True
+    vmask &= ts.valid
+    gate = cl.calibrate_gate(stats, vmask, quantile=args.gate_quantile)
+    p_net = cl.predict(tb, base_t, out_t)
+    p_ana = base_t["p_base"]
+    pl = loose_t["momenta"].double()
+    live = (torch.arange(10, device=dev)[None, :] < tb.n[:, None].long()).double()
+    m_ = torch.where(live > 0, tb.mass, torch.ones_like(tb.mass))
+    ke = 0.5 * ((pl * pl).sum(-1) / m_ * live).sum(-1)
+    p_red = pl * torch.sqrt(loose_t["e0"] / ke)[:, None, None]
+
+    def dist(e):
+        e = e.float()
+        return {"median": float(e.median()), "p99": float(torch.quantile(e[: 1 << 24], 0.99)),
+                "max": float(e.max())}
+
+    ref_v = plain_t["momenta"][vmask]
+    val = {"sims": int(vmask.sum()), "network": dist(cl.rel_err(p_net[vmask], ref_v)),
+           "analytic_only": dist(cl.rel_err(p_ana[vmask], ref_v)),
+           "redistribution_only": dist(cl.rel_err(p_red[vmask], ref_v))}
+    keep = {k: stats[k][vmask] for k in stats}
+    passed = (keep["rho"] <= gate.tol_energy) & (keep["mu"] <= gate.tol_momentum) & (keep["corr"] <= gate.tol_correction)
+    val["gate_pass_frac"] = float(passed.float().mean())
+    del ts, loose_t, base_t, plain_t, out_t, stats, p_net, p_ana, p_red, pl, tb
+    torch.cuda.empty_cache()
+
+    # ---- serving: held-out sims, closure vs plain
+    sb = cl.sample_mixed_device(S, seed=seed, first_sim=S_train)
+    eng.reserve_mixed(S)
+    clo = cl.Closure(eng, net, S)
+
+    def outs():
+        d = {"momenta": torch.zeros((S, 10, 3), dtype=torch.float32, device=dev),
+             "ker": torch.zeros(S, dtype=torch.float64, device=dev),
+             "steps": torch.zeros(S, dtype=torch.int32, device=dev),
+             "status": torch.zeros(S, dtype=torch.uint8, device=dev)}
+        return d, ce.CeOutputs(d["momenta"].data_ptr(), d["ker"].data_ptr(), d["steps"].data_ptr(),
+                               d["status"].data_ptr())
+
+    oc, c_oc = outs()
+    op, c_op = outs()
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    batch_c = sb.c()
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(i & 0xFF)
+                ev[i][0].record(stream)
+            fn()
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in ev) / args.steps
+
+    with ClockSampler(0) as clk:
+        ms_plain = timed(lambda: eng.run_mixed_device(S, batch_c, cfg, c_op, ce.CE_SCHEDULE_ONE_LAUNCH, stream.cuda_stream))
+        ms_clo = timed(lambda: clo.serve(sb, cfg, gate, c_oc, stream=stream.cuda_stream, cbatch=batch_c))
+    acc, fbk = clo.counts()
+    fbf = clo.fallback_flags(S, stream.cuda_stream)
+    torch.cuda.synchronize()
+
+    # network forward alone (tensor-core roofline of the learned part)
+    feats = torch.zeros((cl.pad128(S), 96), dtype=torch.bfloat16, device=dev)
+    fl_row = 2 * (96 * net.hidden + (net.depth - 1) * net.hidden * net.hidden + net.hidden * 32)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    cl.net_forward(net, feats[:65536])
+    torch.cuda.synchronize()
+    a.record()
+    cl.net_forward(net, feats)
+    b.record()
+    torch.cuda.synchronize()
+    ms_fwd = a.elapsed_time(b)
+    fwd_tflops = fl_row * feats.shape[0] / (ms_fwd / 1e3) / 1e12
+    del feats
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        pass
+    bf16_peak = peaks.get("bf16_tflops") or 1590.0
+
+    okc = (oc["status"] == 0) & (op["status"] == 0) & (sb.n >= 2)
+    accepted = okc & (fbf == 0)
+    e_all = cl.rel_err(oc["momenta"][okc], op["momenta"][okc])
+    e_acc = cl.rel_err(oc["momenta"][accepted], op["momenta"][accepted])
+
+    # FP64 oracle on a subset of the served sims
+    n_sub = args.fp64_subset
+    sub = np.linspace(0, S - 1, n_sub).astype(np.int64)
+    nn_s, mm_s, qq_s, xx_s = [], [], [], []
+    for i in sub:
+        a_, b_, c_, x32, _, _ = sp.sample_mixed_host(1, seed, first_sim=int(S_train + i))
+        nn_s.append(a_[0]), mm_s.append(b_[0]), qq_s.append(c_[0]), xx_s.append(x32[0].astype(np.float64))
+    nn_s, mm_s, qq_s, xx_s = np.array(nn_s), np.array(mm_s), np.array(qq_s), np.array(xx_s)
+    ref = ol.run_batch_mixed(nn_s, mm_s, qq_s, xx_s, bits=64, rtol=1e-10, atol=1e-16, pe_stop=1e-11)
+    pc, pp = oc["momenta"].cpu().numpy()[sub], op["momenta"].cpu().numpy()[sub]
+    acc_np = accepted.cpu().numpy()[sub]
+    e64_c = np.array([ol.config_norm_error(pc[j:j + 1, :k], ref["momenta"][j:j + 1, :k])[0]
+                      for j, k in enumerate(nn_s)])
+    e64_p = np.array([ol.config_norm_error(pp[j:j + 1, :k], ref["momenta"][j:j + 1, :k])[0]
+                      for j, k in enumerate(nn_s)])
+
+    def d_np(e):
+        return {"median": float(np.median(e)), "p99": float(np.percentile(e, 99)), "max": float(e.max())} if len(
+            e) else None
+
+    steps_c = oc["steps"].double()
+    line = {
+        "metric": METRIC + " [config 4: learned closure vs plain RK45, mixed 2..10-atom population]",
+        "value": S / (ms_clo / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_clo, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 integration, bf16/f32-accumulate network", "data": "synthetic",
+        "config": {"workload": f"closure serving of {S} held-out mixed sims per step (N ~ U{{2..10}}, species "
+                               "U{H,C,N,O,S}, q ~ U{+1,+2,+3}, radius 2.0 N^(1/3), min pair 0.5, Philox on device)",
+                   "rtol": rtol, "atol": atol, "pe_stop": pes, "loose_pe_stop": cl.LOOSE_PE_STOP,
+                   "network": f"96 -> {net.depth} x {net.hidden} SiLU -> 32, bf16 weights/activations, f32 accumulate",
+                   "l2": "flushed between timed steps (256 MiB write, outside the events)"},
+        "plain": {"value": S / (ms_plain / 1e3), "unit": UNIT, "ms_per_step": ms_plain,
+                  "mean_steps": float(op["steps"].double().mean())},
+        "speedup_vs_plain": ms_plain / ms_clo,
+        "accepted_frac": acc / max(1, acc + fbk), "fallback_sims": fbk,
+        "mean_steps_closure_path": float(steps_c[accepted].mean()) if bool(accepted.any()) else None,
+        "gate": {"tol_energy": gate.tol_energy, "tol_momentum": gate.tol_momentum,
+                 "tol_correction": gate.tol_correction, "calibration": f"{args.gate_quantile} quantile on validation"},
+        "rel_err_vs_plain": {"all": dist(e_all), "accepted": dist(e_acc)},
+        "rel_err_vs_fp64": {"subset": int(n_sub), "closure_all": d_np(e64_c), "closure_accepted": d_np(e64_c[acc_np]),
+                            "plain": d_np(e64_p), "fp64": "oracle f64, rtol 1e-10, atol 1e-16, pe_stop 1e-11"},
+        "training": {"sims": S_train, "generation_s": gen_s, "train_rows": int(train_rows.numel()),
+                     "epochs": rep.epochs, "steps": rep.steps, "minibatch": mb, "seconds": rep.seconds,
+                     "samples_per_s": rep.samples_per_s, "loss_first": float(losses[:20].mean()),
+                     "loss_last": float(losses[-50:].mean())},
+        "validation": val,
+        "network_forward": {"rows": int(cl.pad128(S)), "ms": ms_fwd, "tflops": fwd_tflops,
+                            "frac_of_bf16_peak": fwd_tflops / bf16_peak,
+                            "peak_source": "MEASURED_PEAKS.json bf16_tflops" if peaks else "fallback 1590"},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+    clo.close()
+    net.close()
+    eng.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -386,8 +593,15 @@ def main():
                     help="ch4 (the headline workload), c2h6 (10-atom C2H6-like), h2o (stiff H2O)")
     ap.add_argument("--cpu-budget", type=float, default=8.0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="fixed", choices=["fixed", "mixed", "precision"],
-                    help="fixed: one molecule (--molecule); mixed: 2..10-atom population, one launch vs per size")
+    ap.add_argument("--workload", default="fixed", choices=["fixed", "mixed", "precision", "closure"],
+                    help="fixed: one molecule (--molecule); mixed: 2..10-atom population, one launch vs per size; "
+                         "closure: learned closure vs plain RK45 on the mixed population")
+    ap.add_argument("--train-sims", type=int, default=5_000_000, help="closure: training pairs")
+    ap.add_argument("--epochs", type=int, default=20, help="closure: training epochs")
+    ap.add_argument("--minibatch", type=int, default=8192, help="closure: rows per training step")
+    ap.add_argument("--lr", type=float, default=1e-3, help="closure: peak Adam learning rate")
+    ap.add_argument("--gate-quantile", type=float, default=0.99, help="closure: gate bounds quantile")
+    ap.add_argument("--fp64-subset", type=int, default=300, help="closure: sims checked against the FP64 oracle")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -395,6 +609,8 @@ def main():
         return run_mixed(args)
     if args.workload == "precision":
         return run_precision(args)
+    if args.workload == "closure":
+        return run_closure(args)
 
     import torch
 

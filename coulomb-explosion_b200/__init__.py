@@ -63,6 +63,8 @@ class CeOutputs(C.Structure):
         ("t_final", C.c_void_p),
         ("pe_final", C.c_void_p),
         ("ke_before", C.c_void_p),
+        ("positions", C.c_void_p),
+        ("e0", C.c_void_p),
     ]
 
 
@@ -94,6 +96,17 @@ class CeMixedSampler(C.Structure):
                 ("q_max", C.c_int32), ("n_species", C.c_int32), ("species_amu", C.c_double * 8)]
 
 
+class CeClosureState(C.Structure):
+    _fields_ = [("positions", C.c_void_p), ("momenta", C.c_void_p), ("e0", C.c_void_p), ("pe_final", C.c_void_p),
+                ("status", C.c_void_p)]
+
+
+class CeClosureGate(C.Structure):
+    _fields_ = [("tol_energy", C.c_float), ("tol_momentum", C.c_float), ("tol_correction", C.c_float)]
+
+
+CLOSURE_FEATURES = 96
+CLOSURE_OUTPUTS = 32
 CE_SIM_BAD_INPUT = 4
 CE_SCHEDULE_ONE_LAUNCH = 0
 CE_SCHEDULE_PER_SIZE = 1
@@ -167,6 +180,22 @@ _SIGNATURES = {
     "ce_mlp_check": ([C.c_void_p, C.c_void_p], C.c_int),
     "ce_umma_gemm_f32": ([C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
                           C.c_void_p, C.c_void_p], C.c_int),
+    "ce_mlp_shape": ([C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                      C.POINTER(C.c_uint64)], C.c_int),
+    "ce_closure_default_gate": ([C.POINTER(CeClosureGate)], None),
+    "ce_closure_features": ([C.c_uint64, C.POINTER(CeMixedBatch), C.c_double, C.POINTER(CeClosureState), C.c_void_p,
+                             C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+                            C.c_int),
+    "ce_closure_apply": ([C.c_uint64, C.POINTER(CeMixedBatch), C.POINTER(CeClosureState), C.c_void_p, C.c_void_p,
+                          C.c_void_p, C.c_void_p, C.POINTER(CeClosureGate), C.POINTER(CeOutputs), C.c_void_p,
+                          C.c_void_p, C.c_void_p], C.c_int),
+    "ce_closure_create": ([C.POINTER(C.c_void_p), C.c_void_p, C.c_void_p, C.c_uint64], C.c_int),
+    "ce_closure_destroy": ([C.c_void_p], None),
+    "ce_closure_last_error": ([C.c_void_p], C.c_char_p),
+    "ce_closure_serve": ([C.c_void_p, C.c_uint64, C.POINTER(CeMixedBatch), C.c_double, C.POINTER(CeRunConfig),
+                          C.c_double, C.POINTER(CeClosureGate), C.POINTER(CeOutputs), C.c_void_p], C.c_int),
+    "ce_closure_counts": ([C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)], C.c_int),
+    "ce_closure_fallback_flags": ([C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p], C.c_int),
     "ce_run_device_noalloc": (
         [C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_uint64, C.c_void_p, C.POINTER(CeRunConfig),
          C.POINTER(CeOutputs), C.c_void_p, C.c_char_p, C.c_size_t],
@@ -236,6 +265,8 @@ class Result:
     t_final: np.ndarray | None = None
     pe_final: np.ndarray | None = None
     ke_before: np.ndarray | None = None
+    positions: np.ndarray | None = None  # [S, N, 3] float32 positions at termination
+    e0: np.ndarray | None = None  # [S] float64 initial energy (= PE_0)
     extra: dict = field(default_factory=dict)
 
     @property
@@ -311,8 +342,10 @@ class Engine:
             r.t_final = np.zeros(S, np.float64)
             r.pe_final = np.zeros(S, np.float64)
             r.ke_before = np.zeros(S, np.float64)
+            r.positions = np.zeros_like(r.momenta)
+            r.e0 = np.zeros(S, np.float64)
         out = CeOutputs(_ptr(r.momenta), _ptr(r.ker), _ptr(r.steps), _ptr(r.status), _ptr(r.rejects),
-                        _ptr(r.t_final), _ptr(r.pe_final), _ptr(r.ke_before))
+                        _ptr(r.t_final), _ptr(r.pe_final), _ptr(r.ke_before), _ptr(r.positions), _ptr(r.e0))
         c = cfg.to_c()
         self._check(self.lib.ce_run(self.h, S, _ptr(x), C.byref(c), C.byref(out)))
         return r
@@ -346,8 +379,10 @@ class Engine:
             r.t_final = np.zeros(S, np.float64)
             r.pe_final = np.zeros(S, np.float64)
             r.ke_before = np.zeros(S, np.float64)
+            r.positions = np.zeros_like(r.momenta)
+            r.e0 = np.zeros(S, np.float64)
         out = CeOutputs(_ptr(r.momenta), _ptr(r.ker), _ptr(r.steps), _ptr(r.status), _ptr(r.rejects),
-                        _ptr(r.t_final), _ptr(r.pe_final), _ptr(r.ke_before))
+                        _ptr(r.t_final), _ptr(r.pe_final), _ptr(r.ke_before), _ptr(r.positions), _ptr(r.e0))
         batch = CeMixedBatch(_ptr(n), _ptr(m), _ptr(q), _ptr(x))
         c = cfg.to_c()
         self._check(self.lib.ce_run_mixed(self.h, S, C.byref(batch), float(coulomb_k), C.byref(c), C.byref(out)))

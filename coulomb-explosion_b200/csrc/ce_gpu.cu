@@ -205,7 +205,7 @@ int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
   const size_t b_d = al(S * sizeof(double));
   const size_t b_u = al(S * sizeof(uint32_t));
   const size_t b_s = al(S);
-  const size_t total = b_pos + b_mom + 4 * b_d + 2 * b_u + b_s;
+  const size_t total = b_pos + 2 * b_mom + 5 * b_d + 2 * b_u + b_s;
   if (total > e->arena_bytes) {
     if (e->d_arena) cudaFree(e->d_arena);
     e->d_arena = nullptr;
@@ -220,8 +220,10 @@ int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
   ce_outputs d{};
   d.momenta = reinterpret_cast<float*>(base);
   base += b_mom;
-  double* dd[4];
-  for (int i = 0; i < 4; ++i) {
+  float* d_xout = reinterpret_cast<float*>(base);
+  base += b_mom;
+  double* dd[5];
+  for (int i = 0; i < 5; ++i) {
     dd[i] = reinterpret_cast<double*>(base);
     base += b_d;
   }
@@ -235,6 +237,8 @@ int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
   d.t_final = out->t_final ? dd[1] : nullptr;
   d.pe_final = out->pe_final ? dd[2] : nullptr;
   d.ke_before = out->ke_before ? dd[3] : nullptr;
+  d.e0 = out->e0 ? dd[4] : nullptr;
+  d.positions = out->positions ? d_xout : nullptr;
   d.steps = out->steps ? du[0] : nullptr;
   d.rejects = out->rejects ? du[1] : nullptr;
   d.status = out->status ? d_status : nullptr;
@@ -251,7 +255,8 @@ int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
       {out->momenta, d.momenta, S * n3 * sizeof(float)}, {out->ker, d.ker, S * sizeof(double)},
       {out->t_final, d.t_final, S * sizeof(double)},    {out->pe_final, d.pe_final, S * sizeof(double)},
       {out->ke_before, d.ke_before, S * sizeof(double)}, {out->steps, d.steps, S * sizeof(uint32_t)},
-      {out->rejects, d.rejects, S * sizeof(uint32_t)},  {out->status, d.status, S}};
+      {out->rejects, d.rejects, S * sizeof(uint32_t)},  {out->status, d.status, S},
+      {out->positions, d.positions, S * n3 * sizeof(float)}, {out->e0, d.e0, S * sizeof(double)}};
   for (const Copy& c : copies) {
     if (!c.dst) continue;
     st = cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, e->stream);

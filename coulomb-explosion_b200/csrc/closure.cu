@@ -1,0 +1,657 @@
+// closure.cu -- the learned asymptotic closure around the mixed-batch engine
+// (include/ce_closure.h): input features and the analytic ballistic base at a
+// loose stop, the conservation gate, the fallback merge, and the serving
+// pipeline loose run -> features -> network -> gate -> plain rerun of the
+// doubtful sims.
+//
+// The reference stops at PE <= f * PE_0 and moves the residual potential energy
+// into kinetic energy by one uniform velocity rescale (src/driver.cpp:38-42).
+// Here the engine stops much earlier (f = 0.05) and replaces the missing tail
+// of the trajectory by
+//   1. the straight-line (ballistic) impulse of every pair from the stop to
+//      t -> infinity, in closed form:
+//        dp_i = sum_j k q_i q_j (r_ij I0 + w_ij I1),
+//        I0 = int_0^inf |r + w t|^-3 dt = 1 / (|r| (|r||w| + r.w)),
+//        I1 = int_0^inf t |r + w t|^-3 dt = 1 / (|w| (|r||w| + r.w)),
+//      with r_ij = x_i - x_j and w_ij = v_i - v_j at the stop;
+//   2. the reference's energy rescale applied to that base (KE = E_0);
+//   3. the network's correction, predicted in units of the base's RMS atom
+//      momentum.
+// Every sim whose corrected momenta break energy or momentum conservation by
+// more than the gate's bounds, or whose correction is implausibly large, is
+// integrated again by plain RK45 from its initial geometry.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <string>
+
+#include "ce_closure.h"
+#include "ce_gpu.h"
+#include "engine.hpp"
+
+namespace {
+
+using bf16 = __nv_bfloat16;
+
+constexpr int kA = CE_MAX_ATOMS;  // atoms per padded row
+constexpr int kFeat = CE_CLOSURE_FEATURES;
+constexpr int kOut = CE_CLOSURE_OUTPUTS;
+constexpr double kMassUnit = 1822.888486209;  // m_e per amu (include/coulomb/units.hpp:11)
+constexpr float kLogMassScale = 1.0f / 3.5f;  // ln(32.06 amu / 1 amu) ~ 3.47
+
+struct FeatArgs {
+  uint64_t S, S_pad;
+  const uint8_t* n_atoms;
+  const double* mass;
+  const double* charge;
+  const float* x;
+  const float* p;
+  const double* e0;
+  const double* pe_final;
+  const uint8_t* status;
+  double k;
+  const float* p_true;  // optional [S][10][3]
+  float w_scale;
+  bf16* feats;     // [S_pad][kFeat]
+  float* p_base;   // [S][10][3]
+  float* p_scale;  // [S]
+  float* target;   // optional [S_pad][kOut]
+  float* weight;   // optional [S_pad][kOut]
+};
+
+__device__ __forceinline__ void zero_row(const FeatArgs& A, uint64_t s) {
+  uint4* f = reinterpret_cast<uint4*>(A.feats + s * kFeat);  // 192 B row, 16-B aligned
+#pragma unroll
+  for (int c = 0; c < kFeat * 2 / 16; ++c) f[c] = make_uint4(0u, 0u, 0u, 0u);
+  if (A.target) {
+    float4* t = reinterpret_cast<float4*>(A.target + s * kOut);
+    float4* w = reinterpret_cast<float4*>(A.weight + s * kOut);
+#pragma unroll
+    for (int c = 0; c < kOut / 4; ++c) {
+      t[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+      w[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(128) closure_features_kernel(const FeatArgs A) {
+  for (uint64_t s = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; s < A.S_pad;
+       s += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    if (s >= A.S) {
+      zero_row(A, s);
+      continue;
+    }
+    const int n = A.n_atoms[s];
+    const bool ok = n >= 2 && n <= kA && A.status[s] == CE_SIM_OK;
+    if (!ok) {
+      zero_row(A, s);
+      for (int c = 0; c < 3 * kA; ++c) A.p_base[s * 3 * kA + c] = 0.0f;
+      A.p_scale[s] = 0.0f;
+      continue;
+    }
+    const double* ms = A.mass + s * kA;
+    const double* qs = A.charge + s * kA;
+    const float* xs = A.x + s * 3 * kA;
+    const float* ps = A.p + s * 3 * kA;
+    float x[kA][3], p[kA][3], im[kA], q[kA];
+    double msum = 0.0, cx = 0.0, cy = 0.0, cz = 0.0;
+#pragma unroll
+    for (int i = 0; i < kA; ++i) {
+      const bool on = i < n;
+      const double mi = on ? ms[i] : 1.0;
+      im[i] = on ? static_cast<float>(1.0 / mi) : 0.0f;
+      q[i] = on ? static_cast<float>(qs[i]) : 0.0f;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        x[i][c] = on ? xs[3 * i + c] : 0.0f;
+        p[i][c] = on ? ps[3 * i + c] : 0.0f;
+      }
+      if (on) {
+        msum += mi;
+        cx += mi * x[i][0];
+        cy += mi * x[i][1];
+        cz += mi * x[i][2];
+      }
+    }
+    const float com[3] = {static_cast<float>(cx / msum), static_cast<float>(cy / msum), static_cast<float>(cz / msum)};
+
+    // Ballistic pair impulses from the stop to t -> infinity.
+    float dp[kA][3];
+#pragma unroll
+    for (int i = 0; i < kA; ++i) dp[i][0] = dp[i][1] = dp[i][2] = 0.0f;
+    bool bad = false;
+    const float kf = static_cast<float>(A.k);
+#pragma unroll
+    for (int i = 0; i < kA; ++i) {
+#pragma unroll
+      for (int j = i + 1; j < kA; ++j) {
+        if (j < n) {
+          const float rx = x[i][0] - x[j][0], ry = x[i][1] - x[j][1], rz = x[i][2] - x[j][2];
+          const float wx = p[i][0] * im[i] - p[j][0] * im[j];
+          const float wy = p[i][1] * im[i] - p[j][1] * im[j];
+          const float wz = p[i][2] * im[i] - p[j][2] * im[j];
+          const float a = wx * wx + wy * wy + wz * wz;
+          const float b = rx * wx + ry * wy + rz * wz;
+          const float c = rx * rx + ry * ry + rz * rz;
+          const float sa = sqrtf(a), sc = sqrtf(c), sac = sa * sc;
+          float g;
+          if (b >= 0.0f) {
+            g = sac + b;
+          } else {  // approaching pair: |r|^2|w|^2 - (r.w)^2 = |r x w|^2 avoids the cancellation
+            const float ux = ry * wz - rz * wy, uy = rz * wx - rx * wz, uz = rx * wy - ry * wx;
+            g = (ux * ux + uy * uy + uz * uz) / (sac - b);
+          }
+          const float I0 = 1.0f / (sc * g), I1 = 1.0f / (sa * g);
+          if (!(g > 0.0f) || !isfinite(I0) || !isfinite(I1)) bad = true;
+          const float f = kf * q[i] * q[j];
+          const float tx = f * (rx * I0 + wx * I1), ty = f * (ry * I0 + wy * I1), tz = f * (rz * I0 + wz * I1);
+          dp[i][0] += tx;
+          dp[i][1] += ty;
+          dp[i][2] += tz;
+          dp[j][0] -= tx;
+          dp[j][1] -= ty;
+          dp[j][2] -= tz;
+        }
+      }
+    }
+    // Base = (p + dp) rescaled to KE = E_0 (src/driver.cpp:38-42 on the ballistic state).
+    double ke = 0.0;
+#pragma unroll
+    for (int i = 0; i < kA; ++i) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        dp[i][c] += p[i][c];
+        ke += 0.5 * static_cast<double>(dp[i][c]) * dp[i][c] * im[i];
+      }
+    }
+    const double e0 = A.e0[s];
+    const float sc = static_cast<float>(sqrt(e0 / ke));
+    double p2 = 0.0, r2 = 0.0;
+#pragma unroll
+    for (int i = 0; i < kA; ++i) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        dp[i][c] *= sc;
+        p2 += static_cast<double>(dp[i][c]) * dp[i][c];
+        if (i < n) {
+          const double d = x[i][c] - com[c];
+          r2 += d * d;
+        }
+      }
+    }
+    const float P = static_cast<float>(sqrt(p2 / n));
+    const float L = static_cast<float>(sqrt(r2 / n));
+    if (bad || !(ke > 0.0) || !isfinite(sc) || !(P > 0.0f) || !isfinite(P) || !(L > 0.0f)) {
+      zero_row(A, s);
+      for (int c = 0; c < 3 * kA; ++c) A.p_base[s * 3 * kA + c] = 0.0f;
+      A.p_scale[s] = __int_as_float(0x7fc00000);  // NaN: the gate sends the sim to plain integration
+      continue;
+    }
+    float* pb = A.p_base + s * 3 * kA;
+#pragma unroll
+    for (int i = 0; i < kA; ++i) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) pb[3 * i + c] = dp[i][c];
+    }
+    A.p_scale[s] = P;
+
+    // Features: per atom (x - x_com)/L, p/P, q/3, ln(m/amu)/3.5, 1; then the
+    // remaining PE fraction at the stop and n/10; zeros to the padded width.
+    const float iL = 1.0f / L, iP = 1.0f / P;
+    __align__(16) bf16 f[kFeat];
+#pragma unroll
+    for (int i = 0; i < kA; ++i) {
+      const bool on = i < n;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        f[9 * i + c] = __float2bfloat16_rn(on ? (x[i][c] - com[c]) * iL : 0.0f);
+        f[9 * i + 3 + c] = __float2bfloat16_rn(on ? p[i][c] * iP : 0.0f);
+      }
+      f[9 * i + 6] = __float2bfloat16_rn(on ? q[i] * (1.0f / 3.0f) : 0.0f);
+      f[9 * i + 7] = __float2bfloat16_rn(on ? static_cast<float>(log(ms[i] / kMassUnit)) * kLogMassScale : 0.0f);
+      f[9 * i + 8] = __float2bfloat16_rn(on ? 1.0f : 0.0f);
+    }
+    f[9 * kA] = __float2bfloat16_rn(static_cast<float>(A.pe_final[s] / e0) * 20.0f);
+    f[9 * kA + 1] = __float2bfloat16_rn(static_cast<float>(n) * 0.1f);
+#pragma unroll
+    for (int c = 9 * kA + 2; c < kFeat; ++c) f[c] = __float2bfloat16_rn(0.0f);
+    uint4* fo = reinterpret_cast<uint4*>(A.feats + s * kFeat);
+    const uint4* fi = reinterpret_cast<const uint4*>(f);
+#pragma unroll
+    for (int c = 0; c < kFeat * 2 / 16; ++c) fo[c] = fi[c];
+
+    if (A.target) {
+      const float* pt = A.p_true + s * 3 * kA;
+      float* t = A.target + s * kOut;
+      float* w = A.weight + s * kOut;
+      const float wv = A.w_scale / static_cast<float>(3 * n);
+#pragma unroll
+      for (int i = 0; i < kA; ++i) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          t[3 * i + c] = i < n ? (pt[3 * i + c] - dp[i][c]) * iP : 0.0f;
+          w[3 * i + c] = i < n ? wv : 0.0f;
+        }
+      }
+      for (int c = 3 * kA; c < kOut; ++c) t[c] = w[c] = 0.0f;
+    }
+  }
+}
+
+struct ApplyArgs {
+  uint64_t S;
+  const uint8_t* n_atoms;
+  const double* mass;
+  const double* e0;
+  const uint8_t* status_loose;
+  const uint32_t* steps_loose;
+  const float* p_base;
+  const float* p_scale;
+  const float* net_out;  // [S_pad][kOut]
+  float tol_e, tol_p, tol_c;
+  float* momenta;     // [S][10][3]
+  double* ker;        // optional
+  uint32_t* steps;    // optional
+  uint8_t* status;    // optional
+  uint8_t* fallback;  // [S]: n for sims sent back to plain integration, else 0
+  unsigned long long* counts;  // [0] accepted, [1] fallback
+};
+
+__device__ __forceinline__ void warp_count(bool pred, unsigned long long* ctr) {
+  const unsigned mask = __activemask();
+  const unsigned b = __ballot_sync(mask, pred);
+  const int leader = __ffs(mask) - 1;
+  if ((threadIdx.x & 31) == leader && b) atomicAdd(ctr, static_cast<unsigned long long>(__popc(b)));
+}
+
+__global__ void __launch_bounds__(128) closure_apply_kernel(const ApplyArgs A) {
+  for (uint64_t s = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; s < A.S;
+       s += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const int n = A.n_atoms[s];
+    float* mo = A.momenta + s * 3 * kA;
+    bool accepted = false, fb = false;
+    if (n < 2 || n > kA) {  // one-atom and invalid sims: the loose run's answer is final
+      for (int c = 0; c < 3 * kA; ++c) mo[c] = 0.0f;
+      if (A.ker) A.ker[s] = 0.0;
+      if (A.steps) A.steps[s] = A.steps_loose[s];
+      if (A.status) A.status[s] = A.status_loose[s];
+    } else {
+      const float P = A.p_scale[s];
+      fb = A.status_loose[s] != CE_SIM_OK || !(P > 0.0f) || !isfinite(P);
+      if (!fb) {
+        const double* ms = A.mass + s * kA;
+        const float* pb = A.p_base + s * 3 * kA;
+        const float* o = A.net_out + s * kOut;
+        float p[kA][3];
+        double ke = 0.0, sx = 0.0, sy = 0.0, sz = 0.0, pabs = 0.0, d2 = 0.0, b2 = 0.0, msum = 0.0;
+        float im[kA];
+#pragma unroll
+        for (int i = 0; i < kA; ++i) {
+          const bool on = i < n;
+          const double mi = on ? ms[i] : 1.0;
+          im[i] = on ? static_cast<float>(1.0 / mi) : 0.0f;
+          if (on) msum += mi;
+          double pi2 = 0.0;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const float base = on ? pb[3 * i + c] : 0.0f;
+            const float d = on ? P * o[3 * i + c] : 0.0f;
+            p[i][c] = base + d;
+            d2 += static_cast<double>(d) * d;
+            b2 += static_cast<double>(base) * base;
+            pi2 += static_cast<double>(p[i][c]) * p[i][c];
+          }
+          ke += 0.5 * pi2 * im[i];
+          pabs += sqrt(pi2);
+          sx += p[i][0];
+          sy += p[i][1];
+          sz += p[i][2];
+        }
+        const double e0 = A.e0[s];
+        const double rho = ke / e0 - 1.0;
+        const double mu = sqrt(sx * sx + sy * sy + sz * sz) / pabs;
+        const double corr = sqrt(d2 / b2);
+        accepted = isfinite(rho) && isfinite(mu) && isfinite(corr) && fabs(rho) <= A.tol_e && mu <= A.tol_p &&
+                   corr <= A.tol_c;
+        fb = !accepted;
+        if (accepted) {
+          // Project onto the conservation laws: remove the net momentum (mass
+          // weighted, so the centre of mass stays at rest), then rescale to KE = E_0.
+          double ke2 = 0.0;
+#pragma unroll
+          for (int i = 0; i < kA; ++i) {
+            if (i < n) {
+              const double w = ms[i] / msum;
+              p[i][0] -= static_cast<float>(w * sx);
+              p[i][1] -= static_cast<float>(w * sy);
+              p[i][2] -= static_cast<float>(w * sz);
+              ke2 += 0.5 * (static_cast<double>(p[i][0]) * p[i][0] + static_cast<double>(p[i][1]) * p[i][1] +
+                            static_cast<double>(p[i][2]) * p[i][2]) * im[i];
+            }
+          }
+          const double sc = sqrt(e0 / ke2);
+          double ker = 0.0;
+#pragma unroll
+          for (int i = 0; i < kA; ++i) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              const float v = i < n ? static_cast<float>(sc * p[i][c]) : 0.0f;
+              mo[3 * i + c] = v;
+              ker += 0.5 * static_cast<double>(v) * v * im[i];
+            }
+          }
+          if (A.ker) A.ker[s] = ker;
+          if (A.steps) A.steps[s] = A.steps_loose[s];
+          if (A.status) A.status[s] = CE_SIM_OK;
+        }
+      }
+    }
+    A.fallback[s] = fb ? static_cast<uint8_t>(n) : static_cast<uint8_t>(0);
+    warp_count(accepted, A.counts);
+    warp_count(fb, A.counts + 1);
+  }
+}
+
+struct MergeArgs {
+  uint64_t S;
+  const uint8_t* fallback;
+  const float* fb_momenta;
+  const double* fb_ker;
+  const uint32_t* fb_steps;
+  const uint8_t* fb_status;
+  float* momenta;
+  double* ker;
+  uint32_t* steps;
+  uint8_t* status;
+};
+
+__global__ void __launch_bounds__(128) closure_merge_kernel(const MergeArgs A) {
+  for (uint64_t s = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; s < A.S;
+       s += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    if (!A.fallback[s]) continue;
+    const float* src = A.fb_momenta + s * 3 * kA;
+    float* dst = A.momenta + s * 3 * kA;
+    for (int c = 0; c < 3 * kA; ++c) dst[c] = src[c];
+    if (A.ker) A.ker[s] = A.fb_ker[s];
+    if (A.steps) A.steps[s] = A.fb_steps[s];
+    if (A.status) A.status[s] = A.fb_status[s];
+  }
+}
+
+int grid_for(uint64_t S, int device) {
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  const uint64_t need = (S + 127) / 128;
+  const uint64_t cap = static_cast<uint64_t>(sms) * 16;
+  return static_cast<int>(need < cap ? (need > 0 ? need : 1) : cap);
+}
+
+uint64_t pad128(uint64_t S) { return (S + 127) / 128 * 128; }
+
+int launch_features(uint64_t S, const ce_mixed_batch* in, double k, const ce_closure_state* st, const float* p_true,
+                     float w_scale, void* feats, float* p_base, float* p_scale, float* target, float* weight,
+                     cudaStream_t s) {
+  FeatArgs A{};
+  A.S = S;
+  A.S_pad = pad128(S);
+  A.n_atoms = in->n_atoms;
+  A.mass = in->mass_me;
+  A.charge = in->charge;
+  A.x = st->positions;
+  A.p = st->momenta;
+  A.e0 = st->e0;
+  A.pe_final = st->pe_final;
+  A.status = st->status;
+  A.k = k;
+  A.p_true = p_true;
+  A.w_scale = w_scale;
+  A.feats = static_cast<bf16*>(feats);
+  A.p_base = p_base;
+  A.p_scale = p_scale;
+  A.target = target;
+  A.weight = weight;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  closure_features_kernel<<<grid_for(A.S_pad, dev), 128, 0, s>>>(A);
+  return cudaGetLastError() == cudaSuccess ? CE_OK : CE_ERR_CUDA;
+}
+
+}  // namespace
+
+struct ce_closure {
+  ce_engine* e = nullptr;
+  ce_mlp* net = nullptr;
+  uint64_t max_batch = 0;
+  uint64_t cap = 0;
+  void* arena = nullptr;
+  // loose-stop state
+  float *xs = nullptr, *ps = nullptr;
+  double *e0 = nullptr, *pef = nullptr;
+  uint8_t* st = nullptr;
+  uint32_t* steps = nullptr;
+  // network
+  bf16* feats = nullptr;
+  float *out = nullptr, *pbase = nullptr, *pscale = nullptr;
+  // fallback
+  uint8_t* fb = nullptr;
+  float* fb_m = nullptr;
+  double* fb_ker = nullptr;
+  uint32_t* fb_steps = nullptr;
+  uint8_t* fb_st = nullptr;
+  unsigned long long* counts = nullptr;
+  cudaStream_t last_stream = nullptr;
+  std::string err;
+};
+
+namespace {
+int cfail(ce_closure* c, int code, const std::string& m) {
+  if (c) c->err = m;
+  return code;
+}
+}  // namespace
+
+extern "C" {
+
+void ce_closure_default_gate(ce_closure_gate* g) {
+  if (!g) return;
+  g->tol_energy = 2e-4f;
+  g->tol_momentum = 2e-4f;
+  g->tol_correction = 0.05f;
+}
+
+int ce_closure_features(uint64_t S, const ce_mixed_batch* in, double coulomb_k, const ce_closure_state* st,
+                        const float* p_true, float weight_scale, void* feats, float* p_base, float* p_scale,
+                        float* target, float* weight, void* stream) {
+  if (!in || !st || !feats || !p_base || !p_scale || !in->n_atoms || !in->mass_me || !in->charge || !st->positions ||
+      !st->momenta || !st->e0 || !st->pe_final || !st->status)
+    return CE_ERR_INVALID;
+  if ((target == nullptr) != (weight == nullptr) || (target && !p_true)) return CE_ERR_INVALID;
+  if (S == 0) return CE_OK;
+  return launch_features(S, in, coulomb_k, st, p_true, weight_scale, feats, p_base, p_scale, target, weight,
+                         static_cast<cudaStream_t>(stream));
+}
+
+int ce_closure_apply(uint64_t S, const ce_mixed_batch* in, const ce_closure_state* st, const uint32_t* steps_loose,
+                     const float* p_base, const float* p_scale, const float* net_out, const ce_closure_gate* gate,
+                     const ce_outputs* out, uint8_t* fallback, unsigned long long* counts, void* stream) {
+  if (!in || !st || !steps_loose || !p_base || !p_scale || !net_out || !gate || !out || !out->momenta || !fallback ||
+      !counts || !in->n_atoms || !in->mass_me || !st->e0 || !st->status)
+    return CE_ERR_INVALID;
+  if (S == 0) return CE_OK;
+  ApplyArgs A{};
+  A.S = S;
+  A.n_atoms = in->n_atoms;
+  A.mass = in->mass_me;
+  A.e0 = st->e0;
+  A.status_loose = st->status;
+  A.steps_loose = steps_loose;
+  A.p_base = p_base;
+  A.p_scale = p_scale;
+  A.net_out = net_out;
+  A.tol_e = gate->tol_energy;
+  A.tol_p = gate->tol_momentum;
+  A.tol_c = gate->tol_correction;
+  A.momenta = out->momenta;
+  A.ker = out->ker;
+  A.steps = out->steps;
+  A.status = out->status;
+  A.fallback = fallback;
+  A.counts = counts;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  closure_apply_kernel<<<grid_for(S, dev), 128, 0, static_cast<cudaStream_t>(stream)>>>(A);
+  return cudaGetLastError() == cudaSuccess ? CE_OK : CE_ERR_CUDA;
+}
+
+int ce_closure_create(ce_closure** out, ce_engine* e, ce_mlp* net, uint64_t max_sims) {
+  if (!out || !e || !net || max_sims == 0 || max_sims >= (1ull << 32)) return CE_ERR_INVALID;
+  *out = nullptr;
+  int in_dim = 0, out_dim = 0;
+  uint64_t mb = 0;
+  if (ce_mlp_shape(net, &in_dim, nullptr, nullptr, &out_dim, &mb) != CE_OK || in_dim != kFeat || out_dim != kOut)
+    return CE_ERR_INVALID;
+  ce_closure* c = new ce_closure;
+  c->e = e;
+  c->net = net;
+  c->max_batch = mb;
+  c->cap = max_sims;
+  const uint64_t S = max_sims, Sp = pad128(max_sims);
+  auto al = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
+  const size_t sizes[] = {al(S * 3 * kA * 4), al(S * 3 * kA * 4), al(S * 8), al(S * 8), al(S), al(S * 4),
+                          al(Sp * kFeat * 2), al(Sp * kOut * 4), al(S * 3 * kA * 4), al(S * 4),
+                          al(S), al(S * 3 * kA * 4), al(S * 8), al(S * 4), al(S), al(2 * 8)};
+  size_t total = 0;
+  for (size_t b : sizes) total += b;
+  if (cudaSetDevice(e->device) != cudaSuccess || cudaMalloc(&c->arena, total) != cudaSuccess) {
+    delete c;
+    return CE_ERR_CUDA;
+  }
+  char* p = static_cast<char*>(c->arena);
+  void* slot[16];
+  for (int i = 0; i < 16; ++i) {
+    slot[i] = p;
+    p += sizes[i];
+  }
+  c->xs = static_cast<float*>(slot[0]);
+  c->ps = static_cast<float*>(slot[1]);
+  c->e0 = static_cast<double*>(slot[2]);
+  c->pef = static_cast<double*>(slot[3]);
+  c->st = static_cast<uint8_t*>(slot[4]);
+  c->steps = static_cast<uint32_t*>(slot[5]);
+  c->feats = static_cast<bf16*>(slot[6]);
+  c->out = static_cast<float*>(slot[7]);
+  c->pbase = static_cast<float*>(slot[8]);
+  c->pscale = static_cast<float*>(slot[9]);
+  c->fb = static_cast<uint8_t*>(slot[10]);
+  c->fb_m = static_cast<float*>(slot[11]);
+  c->fb_ker = static_cast<double*>(slot[12]);
+  c->fb_steps = static_cast<uint32_t*>(slot[13]);
+  c->fb_st = static_cast<uint8_t*>(slot[14]);
+  c->counts = static_cast<unsigned long long*>(slot[15]);
+  // padded network rows stay finite
+  cudaMemset(c->out, 0, sizes[7]);
+  const int rc = ce_reserve_mixed(e, max_sims);
+  if (rc != CE_OK || cudaDeviceSynchronize() != cudaSuccess) {
+    cudaFree(c->arena);
+    delete c;
+    return rc != CE_OK ? rc : CE_ERR_CUDA;
+  }
+  *out = c;
+  return CE_OK;
+}
+
+void ce_closure_destroy(ce_closure* c) {
+  if (!c) return;
+  if (c->arena) {
+    cudaSetDevice(c->e->device);
+    cudaFree(c->arena);
+  }
+  delete c;
+}
+
+const char* ce_closure_last_error(const ce_closure* c) { return c ? c->err.c_str() : "null closure"; }
+
+int ce_closure_serve(ce_closure* c, uint64_t S, const ce_mixed_batch* in, double coulomb_k, const ce_run_config* cfg,
+                     double loose_pe_stop, const ce_closure_gate* gate, const ce_outputs* out, void* stream) {
+  if (!c) return CE_ERR_INVALID;
+  if (!in || !cfg || !gate || !out || !out->momenta) return cfail(c, CE_ERR_INVALID, "ce_closure_serve: NULL argument");
+  if (S > c->cap) return cfail(c, CE_ERR_INVALID, "ce_closure_serve: S exceeds the closure's max_sims");
+  if (!(loose_pe_stop > cfg->pe_stop_fraction) || !(loose_pe_stop < 1.0))
+    return cfail(c, CE_ERR_INVALID, "ce_closure_serve: loose_pe_stop must lie in (cfg->pe_stop_fraction, 1)");
+  if (S == 0) return CE_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (cudaSetDevice(c->e->device) != cudaSuccess) return cfail(c, CE_ERR_CUDA, "cudaSetDevice");
+  c->last_stream = s;
+  if (cudaMemsetAsync(c->counts, 0, 2 * sizeof(unsigned long long), s) != cudaSuccess)
+    return cfail(c, CE_ERR_CUDA, "memset counts");
+
+  // 1. integrate every sim to the loose stop, without the energy rescale
+  ce_run_config loose = *cfg;
+  loose.pe_stop_fraction = loose_pe_stop;
+  loose.redistribute_energy = 0;
+  ce_outputs lo{};
+  lo.momenta = c->ps;
+  lo.positions = c->xs;
+  lo.e0 = c->e0;
+  lo.pe_final = c->pef;
+  lo.status = c->st;
+  lo.steps = c->steps;
+  const int sched = c->e->tuned_schedule;
+  int rc = ce_run_mixed_device(c->e, S, in, coulomb_k, &loose, &lo, sched, stream);
+  if (rc != CE_OK) return cfail(c, rc, std::string("loose run: ") + ce_last_error(c->e));
+
+  // 2. features and the ballistic base
+  const ce_closure_state st{c->xs, c->ps, c->e0, c->pef, c->st};
+  rc = launch_features(S, in, coulomb_k, &st, nullptr, 0.0f, c->feats, c->pbase, c->pscale, nullptr, nullptr, s);
+  if (rc != CE_OK) return cfail(c, rc, "features launch");
+
+  // 3. network correction, in chunks of at most max_batch rows
+  const uint64_t Sp = pad128(S);
+  const uint64_t mb = c->max_batch;
+  for (uint64_t off = 0; off < Sp; off += mb) {
+    const uint64_t B = Sp - off < mb ? Sp - off : mb;
+    rc = ce_mlp_forward(c->net, c->feats + off * kFeat, B, c->out + off * kOut, stream);
+    if (rc != CE_OK) return cfail(c, rc, std::string("network: ") + ce_mlp_last_error(c->net));
+  }
+
+  // 4. gate; accepted sims are final, the rest are marked for plain integration
+  rc = ce_closure_apply(S, in, &st, c->steps, c->pbase, c->pscale, c->out, gate, out, c->fb, c->counts, stream);
+  if (rc != CE_OK) return cfail(c, rc, "apply launch");
+
+  // 5. plain RK45 from the initial geometry for the marked sims (n = 0 for the rest)
+  const ce_mixed_batch fbin{c->fb, in->mass_me, in->charge, in->pos};
+  ce_outputs fo{};
+  fo.momenta = c->fb_m;
+  fo.ker = c->fb_ker;
+  fo.steps = c->fb_steps;
+  fo.status = c->fb_st;
+  rc = ce_run_mixed_device(c->e, S, &fbin, coulomb_k, cfg, &fo, sched, stream);
+  if (rc != CE_OK) return cfail(c, rc, std::string("fallback run: ") + ce_last_error(c->e));
+  MergeArgs M{S, c->fb, c->fb_m, c->fb_ker, c->fb_steps, c->fb_st, out->momenta, out->ker, out->steps, out->status};
+  closure_merge_kernel<<<grid_for(S, c->e->device), 128, 0, s>>>(M);
+  if (cudaGetLastError() != cudaSuccess) return cfail(c, CE_ERR_CUDA, "merge launch");
+  return CE_OK;
+}
+
+int ce_closure_fallback_flags(const ce_closure* c, uint8_t* dst, uint64_t S, void* stream) {
+  if (!c || !dst || S > c->cap) return CE_ERR_INVALID;
+  if (S == 0) return CE_OK;
+  return cudaMemcpyAsync(dst, c->fb, S, cudaMemcpyDeviceToDevice, static_cast<cudaStream_t>(stream)) == cudaSuccess
+             ? CE_OK
+             : CE_ERR_CUDA;
+}
+
+int ce_closure_counts(ce_closure* c, uint64_t* accepted, uint64_t* fallback) {
+  if (!c) return CE_ERR_INVALID;
+  unsigned long long h[2] = {0, 0};
+  if (cudaSetDevice(c->e->device) != cudaSuccess ||
+      cudaMemcpyAsync(h, c->counts, sizeof h, cudaMemcpyDeviceToHost, c->last_stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->last_stream) != cudaSuccess)
+    return cfail(c, CE_ERR_CUDA, "ce_closure_counts: copy failed");
+  if (accepted) *accepted = h[0];
+  if (fallback) *fallback = h[1];
+  return ce_mlp_check(c->net, c->last_stream);
+}
+
+}  // extern "C"

@@ -73,6 +73,8 @@ inline void fill_run_params(RunParams& P, const ce_run_config* cfg, const ce_out
   P.t_final = out->t_final;
   P.pe_final = out->pe_final;
   P.ke_before = out->ke_before;
+  P.positions = out->positions;
+  P.e0 = out->e0;
   P.rtol = static_cast<float>(cfg->rtol);
   P.atol = static_cast<float>(cfg->atol);
   P.max_dt = static_cast<float>(cfg->max_dt);

@@ -105,6 +105,12 @@ __global__ void bucket_scatter_kernel(const uint8_t* __restrict__ n_per, uint64_
       if (P.t_final) P.t_final[i] = 0.0;
       if (P.pe_final) P.pe_final[i] = 0.0;
       if (P.ke_before) P.ke_before[i] = 0.0;
+      if (P.e0) P.e0[i] = 0.0;
+      if (P.positions) {
+        float* xp = P.positions + i * (3ull * ce::kMixedStride);
+        const float* x0 = P.pos + i * (3ull * ce::kMixedStride);
+        for (int c = 0; c < 3 * ce::kMixedStride; ++c) xp[c] = bin == 1 ? x0[c] : 0.0f;
+      }
     }
     __syncthreads();
   }
@@ -247,9 +253,10 @@ int ce_run_mixed(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coul
                           al(S * A * sizeof(double)),         // charge
                           al(S * A * 3 * sizeof(float)),      // pos
                           al(S * A * 3 * sizeof(float)),      // momenta
-                          al(S * sizeof(double)) * 4,         // ker, t_final, pe_final, ke_before
+                          al(S * sizeof(double)) * 5,         // ker, t_final, pe_final, ke_before, e0
                           al(S * sizeof(uint32_t)) * 2,       // steps, rejects
-                          al(S)};                             // status
+                          al(S),                              // status
+                          al(S * A * 3 * sizeof(float))};     // positions at termination
   size_t total = 0;
   for (size_t b : sizes) total += b;
   if (total > e->arena_bytes) {
@@ -282,12 +289,15 @@ int ce_run_mixed(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coul
   d.t_final = out->t_final ? reinterpret_cast<double*>(p + bd) : nullptr;
   d.pe_final = out->pe_final ? reinterpret_cast<double*>(p + 2 * bd) : nullptr;
   d.ke_before = out->ke_before ? reinterpret_cast<double*>(p + 3 * bd) : nullptr;
+  d.e0 = out->e0 ? reinterpret_cast<double*>(p + 4 * bd) : nullptr;
   p += sizes[5];
   const size_t bu = al(S * sizeof(uint32_t));
   d.steps = out->steps ? reinterpret_cast<uint32_t*>(p) : nullptr;
   d.rejects = out->rejects ? reinterpret_cast<uint32_t*>(p + bu) : nullptr;
   p += sizes[6];
   d.status = out->status ? reinterpret_cast<uint8_t*>(p) : nullptr;
+  p += sizes[7];
+  d.positions = out->positions ? reinterpret_cast<float*>(p) : nullptr;
 
   struct Copy {
     void* dst;
@@ -307,7 +317,8 @@ int ce_run_mixed(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coul
   const Copy d2h[] = {{out->momenta, d.momenta, S * A * 3 * sizeof(float)}, {out->ker, d.ker, S * sizeof(double)},
                       {out->t_final, d.t_final, S * sizeof(double)},     {out->pe_final, d.pe_final, S * sizeof(double)},
                       {out->ke_before, d.ke_before, S * sizeof(double)}, {out->steps, d.steps, S * sizeof(uint32_t)},
-                      {out->rejects, d.rejects, S * sizeof(uint32_t)},   {out->status, d.status, S}};
+                      {out->rejects, d.rejects, S * sizeof(uint32_t)},   {out->status, d.status, S},
+                      {out->positions, d.positions, S * A * 3 * sizeof(float)}, {out->e0, d.e0, S * sizeof(double)}};
   for (const Copy& c : d2h) {
     if (!c.dst) continue;
     st = cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, e->stream);

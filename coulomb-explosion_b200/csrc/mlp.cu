@@ -550,6 +550,16 @@ int ce_mlp_train_step(ce_mlp* n, const void* x, const float* target, const float
   return cudaGetLastError() == cudaSuccess ? CE_OK : set_err(n, CE_ERR_CUDA, "adam launch");
 }
 
+int ce_mlp_shape(const ce_mlp* n, int* in_dim, int* hidden, int* depth, int* out_dim, uint64_t* max_batch) {
+  if (!n) return CE_ERR_INVALID;
+  if (in_dim) *in_dim = n->in_dim;
+  if (hidden) *hidden = n->hidden;
+  if (depth) *depth = n->depth;
+  if (out_dim) *out_dim = n->out_dim;
+  if (max_batch) *max_batch = n->max_batch;
+  return CE_OK;
+}
+
 int ce_mlp_check(ce_mlp* n, void* stream) {
   if (!n) return CE_ERR_INVALID;
   return check_err_flag(n, static_cast<cudaStream_t>(stream));

@@ -138,6 +138,8 @@ extern "C" int ce_run_device_noalloc(int n, const double* mass_me, const double*
   P.t_final = out->t_final;
   P.pe_final = out->pe_final;
   P.ke_before = out->ke_before;
+  P.positions = out->positions;
+  P.e0 = out->e0;
   P.cursor = cursor;
   P.S = S;
   P.rtol = static_cast<float>(cfg->rtol);

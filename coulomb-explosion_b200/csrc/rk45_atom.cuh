@@ -149,6 +149,13 @@ __device__ __forceinline__ void atom_finalize(const AtomLane<N, MODE>& s, int st
   dst[0] = static_cast<float>(px);
   dst[1] = static_cast<float>(py);
   dst[2] = static_cast<float>(pz);
+  if (P.positions) {
+    float* xp = P.positions + s.sim * (3ull * STRIDE) + 3 * ai;
+    xp[0] = s.x[0];
+    xp[1] = s.x[1];
+    xp[2] = s.x[2];
+  }
+  if (ai == 0 && P.e0) P.e0[s.sim] = static_cast<double>(s.e0);
   if (ai == 0) {
     if (P.ker) P.ker[s.sim] = ker;
     if (P.steps) P.steps[s.sim] = s.steps;

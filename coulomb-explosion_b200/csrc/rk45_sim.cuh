@@ -43,6 +43,8 @@ struct RunParams {
   double* t_final;
   double* pe_final;
   double* ke_before;
+  float* positions;  // [S][N][3] positions at termination (optional)
+  double* e0;        // [S] initial energy (optional)
   unsigned long long* cursor;  // work-queue head (device scratch, zeroed per launch)
   unsigned long long S;
   float rtol, atol, max_dt;
@@ -144,6 +146,16 @@ __device__ __forceinline__ void finalize(const Sim<N, MODE>& s, int status, doub
   if (P.t_final) P.t_final[s.sim] = static_cast<double>(s.t);
   if (P.pe_final) P.pe_final[s.sim] = pe_final;
   if (P.ke_before) P.ke_before[s.sim] = ke;
+  if (P.e0) P.e0[s.sim] = static_cast<double>(s.e0);
+  if (P.positions) {
+    float* xp = P.positions + s.sim * (3ull * N);
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      xp[i * 3 + 0] = s.x[i][0];
+      xp[i * 3 + 1] = s.x[i][1];
+      xp[i * 3 + 2] = s.x[i][2];
+    }
+  }
 }
 
 // Hairer's initial step from rest (src/integrators.cpp:197-250 with v0 = 0:

@@ -90,7 +90,10 @@ void ce_default_config(ce_run_config* cfg);
  *   t_final   [S] double       simulated time at termination (RunResult::t_final)
  *   pe_final  [S] double       potential energy at termination (RunResult::pe_final)
  *   ke_before [S] double       kinetic energy before redistribution
- *                              (RunResult::ke_before_redist)                         */
+ *                              (RunResult::ke_before_redist)
+ *   positions [S][N][3] float  positions at termination (the state's positions
+ *                              after run_to_convergence, src/driver.cpp:7-46)
+ *   e0        [S] double       initial total energy E_0 = PE_0 (RunResult::energy_initial) */
 typedef struct ce_outputs {
   float* momenta;
   double* ker;
@@ -100,6 +103,8 @@ typedef struct ce_outputs {
   double* t_final;
   double* pe_final;
   double* ke_before;
+  float* positions;
+  double* e0;
 } ce_outputs;
 
 /* Launch-shape knobs (0 = autotuned value if any, else the engine default). */

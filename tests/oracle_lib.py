@@ -171,6 +171,19 @@ def potential(x, charge, *, bits=64, k=1.0):
     return getattr(oracle(), f"ce_oracle_pe_f{bits}")(x.shape[0], _p(x), _p(charge), k)
 
 
+def run_state(n, mass, charge, pos, *, k=1.0, **kw):
+    """Loose-stop state of one sim (f32 engine arithmetic): (x [n,3], p [n,3], stats)."""
+    lib = oracle()
+    x = np.zeros((n, 3))
+    p = np.zeros((n, 3))
+    st = OracleStats()
+    c = cfg(**kw)
+    lib.ce_oracle_run_state_f32(int(n), _p(np.ascontiguousarray(mass, np.float64)),
+                                _p(np.ascontiguousarray(charge, np.float64)), float(k),
+                                _p(np.ascontiguousarray(pos, np.float64)), C.byref(c), _p(x), _p(p), C.byref(st))
+    return x, p, st
+
+
 def config_norm_error(p, p_ref):
     """Per-sim ||p - p_ref||_2 / ||p_ref||_2 over all 3N components
     (python/analysis/plot_precision.py:52-56; examples/verify_subset.py:77-79)."""
