@@ -495,10 +495,25 @@ def run_closure(args):
     acc, fbk = clo.counts()
     fbf = clo.fallback_flags(S, stream.cuda_stream)
     torch.cuda.synchronize()
+    # stage breakdown: the loose run alone, and the plain rerun of the sims the gate sent back
+    lcfg = ce.RunConfig(rtol=rtol, atol=atol, pe_stop_fraction=cl.LOOSE_PE_STOP, redistribute_energy=False,
+                        precision_mode=args.mode)
+    lo_m = torch.empty((S, 10, 3), dtype=torch.float32, device=dev)
+    lo_x = torch.empty((S, 10, 3), dtype=torch.float32, device=dev)
+    lo_d = torch.empty((3, S), dtype=torch.float64, device=dev)
+    lo_s = torch.empty(S, dtype=torch.int32, device=dev)
+    lo_st = torch.empty(S, dtype=torch.uint8, device=dev)
+    c_lo = ce.CeOutputs(lo_m.data_ptr(), None, lo_s.data_ptr(), lo_st.data_ptr(), None, None, lo_d[1].data_ptr(),
+                        None, lo_x.data_ptr(), lo_d[2].data_ptr())
+    ms_loose = timed(lambda: eng.run_mixed_device(S, batch_c, lcfg, c_lo, ce.CE_SCHEDULE_ONE_LAUNCH,
+                                                  stream.cuda_stream))
+    fb_batch = ce.CeMixedBatch(fbf.data_ptr(), sb.mass.data_ptr(), sb.charge.data_ptr(), sb.pos.data_ptr())
+    ms_fb = timed(lambda: eng.run_mixed_device(S, fb_batch, cfg, c_lo, ce.CE_SCHEDULE_ONE_LAUNCH, stream.cuda_stream))
+    del lo_m, lo_x, lo_d, lo_s, lo_st
 
     # network forward alone (tensor-core roofline of the learned part)
-    feats = torch.zeros((cl.pad128(S), 96), dtype=torch.bfloat16, device=dev)
-    fl_row = 2 * (96 * net.hidden + (net.depth - 1) * net.hidden * net.hidden + net.hidden * 32)
+    feats = torch.zeros((cl.pad128(S), ce.CLOSURE_FEATURES), dtype=torch.bfloat16, device=dev)
+    fl_row = 2 * (ce.CLOSURE_FEATURES * net.hidden + (net.depth - 1) * net.hidden * net.hidden + net.hidden * 32)
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     cl.net_forward(net, feats[:65536])
     torch.cuda.synchronize()
@@ -550,11 +565,13 @@ def run_closure(args):
         "config": {"workload": f"closure serving of {S} held-out mixed sims per step (N ~ U{{2..10}}, species "
                                "U{H,C,N,O,S}, q ~ U{+1,+2,+3}, radius 2.0 N^(1/3), min pair 0.5, Philox on device)",
                    "rtol": rtol, "atol": atol, "pe_stop": pes, "loose_pe_stop": cl.LOOSE_PE_STOP,
-                   "network": f"96 -> {net.depth} x {net.hidden} SiLU -> 32, bf16 weights/activations, f32 accumulate",
+                   "network": f"{ce.CLOSURE_FEATURES} -> {net.depth} x {net.hidden} SiLU -> 32, bf16 weights/activations, f32 accumulate",
                    "l2": "flushed between timed steps (256 MiB write, outside the events)"},
         "plain": {"value": S / (ms_plain / 1e3), "unit": UNIT, "ms_per_step": ms_plain,
                   "mean_steps": float(op["steps"].double().mean())},
         "speedup_vs_plain": ms_plain / ms_clo,
+        "breakdown_ms": {"loose_run": ms_loose, "network_forward": None, "fallback_run": ms_fb,
+                         "rest (features, gate, merge)": None},
         "accepted_frac": acc / max(1, acc + fbk), "fallback_sims": fbk,
         "mean_steps_closure_path": float(steps_c[accepted].mean()) if bool(accepted.any()) else None,
         "gate": {"tol_energy": gate.tol_energy, "tol_momentum": gate.tol_momentum,
@@ -572,10 +589,63 @@ def run_closure(args):
                             "peak_source": "MEASURED_PEAKS.json bf16_tflops" if peaks else "fallback 1590"},
         "clocks": clk.summary(),
     }
+    line["breakdown_ms"]["network_forward"] = ms_fwd
+    line["breakdown_ms"]["rest (features, gate, merge)"] = ms_clo - ms_loose - ms_fwd - ms_fb
     print(json.dumps(line))
     clo.close()
     net.close()
     eng.close()
+    return 0
+
+
+def run_network(args):
+    """The closure network's serving forward alone (fused tcgen05 kernel):
+    `--sims` rows (default 1e7) of random BF16 features through 128 -> 4 x 256
+    SiLU -> 32 with random weights, event-timed, against the measured bf16
+    tensor-core peak."""
+    import importlib
+
+    import torch
+
+    from __graft_entry__ import load_package
+
+    ce = load_package()
+    cl = importlib.import_module("coulomb_explosion_b200.closure")
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    rows = cl.pad128(args.sims if args.sims != S_DEFAULT else 10_000_000)
+    net = cl.Network(max_batch=65536, seed=SEED)
+    g = torch.Generator(device=dev)
+    g.manual_seed(SEED)
+    x = torch.randn((rows, ce.CLOSURE_FEATURES), generator=g, device=dev).to(torch.bfloat16)
+    out = torch.empty((rows, ce.CLOSURE_OUTPUTS), dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    for _ in range(args.warmup):
+        net.forward(x, out, rows, stream)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(0) as clk:
+        for a, b in ev:
+            a.record()
+            net.forward(x, out, rows, stream)
+            b.record()
+        torch.cuda.synchronize()
+    net.check(stream)
+    ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
+    fl_row = 2 * (ce.CLOSURE_FEATURES * net.hidden + (net.depth - 1) * net.hidden * net.hidden + net.hidden * 32)
+    tflops = fl_row * rows / (ms / 1e3) / 1e12
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = peaks.get("bf16_tflops") or 1590.0
+    print(json.dumps({
+        "metric": "closure network forward (fused tcgen05 kernel)", "value": rows / (ms / 1e3), "unit": "rows/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "dtype": "bf16 in, f32 accumulate", "data": "synthetic",
+        "config": {"workload": f"{rows} rows, {ce.CLOSURE_FEATURES} -> {net.depth} x {net.hidden} SiLU -> 32",
+                   "flops_per_row": fl_row},
+        "roofline": {"bound": "tensor", "achieved": tflops, "peak": peak, "unit": "TFLOP/s", "frac": tflops / peak,
+                     "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback 1590"},
+        "clocks": clk.summary()}))
+    net.close()
     return 0
 
 
@@ -593,9 +663,10 @@ def main():
                     help="ch4 (the headline workload), c2h6 (10-atom C2H6-like), h2o (stiff H2O)")
     ap.add_argument("--cpu-budget", type=float, default=8.0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="fixed", choices=["fixed", "mixed", "precision", "closure"],
+    ap.add_argument("--workload", default="fixed", choices=["fixed", "mixed", "precision", "closure", "network"],
                     help="fixed: one molecule (--molecule); mixed: 2..10-atom population, one launch vs per size; "
-                         "closure: learned closure vs plain RK45 on the mixed population")
+                         "closure: learned closure vs plain RK45 on the mixed population; network: the closure "
+                         "network's fused forward alone")
     ap.add_argument("--train-sims", type=int, default=5_000_000, help="closure: training pairs")
     ap.add_argument("--epochs", type=int, default=20, help="closure: training epochs")
     ap.add_argument("--minibatch", type=int, default=8192, help="closure: rows per training step")
@@ -611,6 +682,8 @@ def main():
         return run_precision(args)
     if args.workload == "closure":
         return run_closure(args)
+    if args.workload == "network":
+        return run_network(args)
 
     import torch
 

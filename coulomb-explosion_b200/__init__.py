@@ -105,7 +105,7 @@ class CeClosureGate(C.Structure):
     _fields_ = [("tol_energy", C.c_float), ("tol_momentum", C.c_float), ("tol_correction", C.c_float)]
 
 
-CLOSURE_FEATURES = 96
+CLOSURE_FEATURES = 128
 CLOSURE_OUTPUTS = 32
 CE_SIM_BAD_INPUT = 4
 CE_SCHEDULE_ONE_LAUNCH = 0
@@ -173,6 +173,7 @@ _SIGNATURES = {
     "ce_mlp_set_params": ([C.c_void_p, C.c_void_p], C.c_int),
     "ce_mlp_get_params": ([C.c_void_p, C.c_void_p], C.c_int),
     "ce_mlp_forward": ([C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p], C.c_int),
+    "ce_mlp_forward_layered": ([C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p], C.c_int),
     "ce_mlp_gradients": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
                           C.c_void_p], C.c_int),
     "ce_mlp_train_step": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_float, C.c_void_p,

@@ -5,7 +5,7 @@ calibration and serving.
 The reference's only closure is the uniform velocity rescale at the stop
 (src/driver.cpp:38-42). Here every sim is integrated to a loose stop
 (PE <= 5% PE_0), the closed-form straight-line pair impulse to t -> infinity
-plus that rescale gives a base, and a BF16 MLP (96 -> 4 x 256 SiLU -> 32)
+plus that rescale gives a base, and a BF16 MLP (128 -> 4 x 256 SiLU -> 32)
 predicts the remaining correction in units of the base's RMS atom momentum.
 Training targets are the engine's own fully converged momenta on the same
 inputs. Device memory is held in torch tensors; every computation on the
@@ -44,7 +44,7 @@ def pad128(S: int) -> int:
 
 
 class Network:
-    """ce_mlp handle: in 96 -> hidden x depth (SiLU) -> 32."""
+    """ce_mlp handle: in 128 -> hidden x depth (SiLU) -> 32."""
 
     def __init__(self, device: int = 0, hidden: int = 256, depth: int = 4, max_batch: int = 65536, seed: int = 1):
         self.lib = load_library()
@@ -197,7 +197,7 @@ def closure_state(loose: dict) -> CeClosureState:
 
 def features(batch: DeviceBatch, loose: dict, p_true=None, weight_scale: float = 1.0, stream: int = 0,
              coulomb_k: float = 1.0) -> dict:
-    """ce_closure_features: BF16 features [pad128(S), 96], ballistic base
+    """ce_closure_features: BF16 features [pad128(S), 128], ballistic base
     [S, 10, 3], scale P [S] and, with p_true, targets/weights [pad128(S), 32]."""
     torch = _torch()
     lib = load_library()
@@ -223,8 +223,9 @@ def net_forward(net: Network, feats, stream: int = 0):
     torch = _torch()
     Sp = feats.shape[0]
     out = torch.empty((Sp, CLOSURE_OUTPUTS), dtype=torch.float32, device=feats.device)
-    for a in range(0, Sp, net.max_batch):
-        b = min(Sp, a + net.max_batch)
+    chunk = Sp if (net.hidden % 32 == 0 and net.depth + 1 <= 8) else net.max_batch  # fused kernel: one launch
+    for a in range(0, Sp, chunk):
+        b = min(Sp, a + chunk)
         net.forward(feats[a:b], out[a:b], b - a, stream)
     return out
 

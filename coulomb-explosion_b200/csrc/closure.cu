@@ -39,6 +39,9 @@ constexpr int kFeat = CE_CLOSURE_FEATURES;
 constexpr int kOut = CE_CLOSURE_OUTPUTS;
 constexpr double kMassUnit = 1822.888486209;  // m_e per amu (include/coulomb/units.hpp:11)
 constexpr float kLogMassScale = 1.0f / 3.5f;  // ln(32.06 amu / 1 amu) ~ 3.47
+constexpr int kPerAtom = 12;                  // features per atom
+constexpr float kRelRef = 1e-3f;              // typical RMS residual (units of P)
+constexpr float kRelEps = 2e-5f;              // floor of the relative weighting
 
 struct FeatArgs {
   uint64_t S, S_pad;
@@ -61,7 +64,7 @@ struct FeatArgs {
 };
 
 __device__ __forceinline__ void zero_row(const FeatArgs& A, uint64_t s) {
-  uint4* f = reinterpret_cast<uint4*>(A.feats + s * kFeat);  // 192 B row, 16-B aligned
+  uint4* f = reinterpret_cast<uint4*>(A.feats + s * kFeat);  // 256 B row, 16-B aligned
 #pragma unroll
   for (int c = 0; c < kFeat * 2 / 16; ++c) f[c] = make_uint4(0u, 0u, 0u, 0u);
   if (A.target) {
@@ -196,8 +199,9 @@ __global__ void __launch_bounds__(128) closure_features_kernel(const FeatArgs A)
     }
     A.p_scale[s] = P;
 
-    // Features: per atom (x - x_com)/L, p/P, q/3, ln(m/amu)/3.5, 1; then the
-    // remaining PE fraction at the stop and n/10; zeros to the padded width.
+    // Features: per atom (x - x_com)/L, p/P, (p_base - p)/P, q/3, ln(m/amu)/3.5,
+    // 1; then the remaining PE fraction at the stop and n/10; zeros to the
+    // padded width.
     const float iL = 1.0f / L, iP = 1.0f / P;
     __align__(16) bf16 f[kFeat];
 #pragma unroll
@@ -205,34 +209,47 @@ __global__ void __launch_bounds__(128) closure_features_kernel(const FeatArgs A)
       const bool on = i < n;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        f[9 * i + c] = __float2bfloat16_rn(on ? (x[i][c] - com[c]) * iL : 0.0f);
-        f[9 * i + 3 + c] = __float2bfloat16_rn(on ? p[i][c] * iP : 0.0f);
+        f[kPerAtom * i + c] = __float2bfloat16_rn(on ? (x[i][c] - com[c]) * iL : 0.0f);
+        f[kPerAtom * i + 3 + c] = __float2bfloat16_rn(on ? p[i][c] * iP : 0.0f);
+        f[kPerAtom * i + 6 + c] = __float2bfloat16_rn(on ? (dp[i][c] - p[i][c]) * iP : 0.0f);
       }
-      f[9 * i + 6] = __float2bfloat16_rn(on ? q[i] * (1.0f / 3.0f) : 0.0f);
-      f[9 * i + 7] = __float2bfloat16_rn(on ? static_cast<float>(log(ms[i] / kMassUnit)) * kLogMassScale : 0.0f);
-      f[9 * i + 8] = __float2bfloat16_rn(on ? 1.0f : 0.0f);
+      f[kPerAtom * i + 9] = __float2bfloat16_rn(on ? q[i] * (1.0f / 3.0f) : 0.0f);
+      f[kPerAtom * i + 10] =
+          __float2bfloat16_rn(on ? static_cast<float>(log(ms[i] / kMassUnit)) * kLogMassScale : 0.0f);
+      f[kPerAtom * i + 11] = __float2bfloat16_rn(on ? 1.0f : 0.0f);
     }
-    f[9 * kA] = __float2bfloat16_rn(static_cast<float>(A.pe_final[s] / e0) * 20.0f);
-    f[9 * kA + 1] = __float2bfloat16_rn(static_cast<float>(n) * 0.1f);
+    f[kPerAtom * kA] = __float2bfloat16_rn(static_cast<float>(A.pe_final[s] / e0) * 20.0f);
+    f[kPerAtom * kA + 1] = __float2bfloat16_rn(static_cast<float>(n) * 0.1f);
 #pragma unroll
-    for (int c = 9 * kA + 2; c < kFeat; ++c) f[c] = __float2bfloat16_rn(0.0f);
+    for (int c = kPerAtom * kA + 2; c < kFeat; ++c) f[c] = __float2bfloat16_rn(0.0f);
     uint4* fo = reinterpret_cast<uint4*>(A.feats + s * kFeat);
     const uint4* fi = reinterpret_cast<const uint4*>(f);
 #pragma unroll
     for (int c = 0; c < kFeat * 2 / 16; ++c) fo[c] = fi[c];
 
     if (A.target) {
+      // Targets (p_true - p_base)/P; weights w_scale / (3n) scaled by
+      // kRelRef / sqrt(rms^2 + kRelEps^2), rms = the RMS target of the sim, so
+      // the loss weighs each sim's relative rather than absolute residual.
       const float* pt = A.p_true + s * 3 * kA;
       float* t = A.target + s * kOut;
       float* w = A.weight + s * kOut;
-      const float wv = A.w_scale / static_cast<float>(3 * n);
+      float ss = 0.0f;
 #pragma unroll
       for (int i = 0; i < kA; ++i) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          t[3 * i + c] = i < n ? (pt[3 * i + c] - dp[i][c]) * iP : 0.0f;
-          w[3 * i + c] = i < n ? wv : 0.0f;
+          const float v = i < n ? (pt[3 * i + c] - dp[i][c]) * iP : 0.0f;
+          t[3 * i + c] = v;
+          ss += v * v;
         }
+      }
+      const float rms2 = ss / static_cast<float>(3 * n);
+      const float wv = A.w_scale / static_cast<float>(3 * n) * kRelRef * rsqrtf(rms2 + kRelEps * kRelEps);
+#pragma unroll
+      for (int i = 0; i < kA; ++i) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) w[3 * i + c] = i < n ? wv : 0.0f;
       }
       for (int c = 3 * kA; c < kOut; ++c) t[c] = w[c] = 0.0f;
     }
@@ -423,6 +440,7 @@ struct ce_closure {
   ce_engine* e = nullptr;
   ce_mlp* net = nullptr;
   uint64_t max_batch = 0;
+  bool fused = false;  // network runs as one fused forward launch
   uint64_t cap = 0;
   void* arena = nullptr;
   // loose-stop state
@@ -507,14 +525,15 @@ int ce_closure_apply(uint64_t S, const ce_mixed_batch* in, const ce_closure_stat
 int ce_closure_create(ce_closure** out, ce_engine* e, ce_mlp* net, uint64_t max_sims) {
   if (!out || !e || !net || max_sims == 0 || max_sims >= (1ull << 32)) return CE_ERR_INVALID;
   *out = nullptr;
-  int in_dim = 0, out_dim = 0;
+  int in_dim = 0, out_dim = 0, hidden = 0, depth = 0;
   uint64_t mb = 0;
-  if (ce_mlp_shape(net, &in_dim, nullptr, nullptr, &out_dim, &mb) != CE_OK || in_dim != kFeat || out_dim != kOut)
+  if (ce_mlp_shape(net, &in_dim, &hidden, &depth, &out_dim, &mb) != CE_OK || in_dim != kFeat || out_dim != kOut)
     return CE_ERR_INVALID;
   ce_closure* c = new ce_closure;
   c->e = e;
   c->net = net;
   c->max_batch = mb;
+  c->fused = hidden % 32 == 0 && depth + 1 <= 8;
   c->cap = max_sims;
   const uint64_t S = max_sims, Sp = pad128(max_sims);
   auto al = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
@@ -606,9 +625,10 @@ int ce_closure_serve(ce_closure* c, uint64_t S, const ce_mixed_batch* in, double
   rc = launch_features(S, in, coulomb_k, &st, nullptr, 0.0f, c->feats, c->pbase, c->pscale, nullptr, nullptr, s);
   if (rc != CE_OK) return cfail(c, rc, "features launch");
 
-  // 3. network correction, in chunks of at most max_batch rows
+  // 3. network correction: one fused launch over all rows when the network
+  // allows it, else chunks of at most max_batch rows
   const uint64_t Sp = pad128(S);
-  const uint64_t mb = c->max_batch;
+  const uint64_t mb = c->fused ? Sp : c->max_batch;
   for (uint64_t off = 0; off < Sp; off += mb) {
     const uint64_t B = Sp - off < mb ? Sp - off : mb;
     rc = ce_mlp_forward(c->net, c->feats + off * kFeat, B, c->out + off * kOut, stream);

@@ -95,7 +95,27 @@ __device__ __forceinline__ void stage(uint8_t* s, const bf16* G, int ld, int r0,
   }
 }
 
-__device__ __forceinline__ float sigmoidf_(float z) { return 1.0f / (1.0f + __expf(-z)); }
+// sigmoid(z) = (1 + tanh(z/2)) / 2 with the hardware tanh approximation
+// (tanh.approx.f32, max relative error ~2^-11, below the BF16 rounding of the
+// activations): one special-function op per element instead of exp + divide.
+__device__ __forceinline__ float tanh_approx(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float sigmoidf_(float z) { return fmaf(0.5f, tanh_approx(0.5f * z), 0.5f); }
+
+// Forward SiLU of a BF16 pre-activation in BF16 arithmetic:
+// y = z * (1/2 + tanh(z/2)/2) (tanh.approx.bf16). The fused serving kernel
+// evaluates the same operations on pairs (bf16x2), so both forwards agree bit
+// for bit.
+__device__ __forceinline__ bf16 silu_bf16(bf16 z) {
+  const bf16 half = __float2bfloat16(0.5f);
+  const bf16 h = __hmul(z, half);
+  uint16_t tb;
+  asm("tanh.approx.bf16 %0, %1;" : "=h"(tb) : "h"(__bfloat16_as_ushort(h)));
+  return __hmul(z, __hfma(__ushort_as_bfloat16(tb), half, half));
+}
 
 template <bool A_MN, bool B_MN>
 __global__ void __launch_bounds__(128) umma_gemm_kernel(const GemmArgs g) {
@@ -154,11 +174,9 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(const GemmArgs g) {
         const float acc = __uint_as_float(r[j]);
         switch (g.epi) {
           case kEpiFwdAct: {
-            const float z = acc + g.bias[n];
-            const bf16 zb = __float2bfloat16(z);
+            const bf16 zb = __float2bfloat16(acc + g.bias[n]);
             g.Zout[static_cast<size_t>(row) * g.ldz + n] = zb;
-            const float zr = __bfloat162float(zb);
-            g.Y[static_cast<size_t>(row) * g.ldy + n] = __float2bfloat16(zr * sigmoidf_(zr));
+            g.Y[static_cast<size_t>(row) * g.ldy + n] = silu_bf16(zb);
             break;
           }
           case kEpiFwdLinearF32:
@@ -231,6 +249,276 @@ __global__ void f32_to_bf16_kernel(const float* a, bf16* b, int n) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = __float2bfloat16(a[i]);
 }
 
+// ---- fused forward (serving) ----
+//
+// One persistent CTA per SM walks pairs of 128-row tiles through every layer,
+// with warp roles:
+//   warp 0  producer: one thread streams the weights, pre-packed in global
+//           memory in the tensor core's canonical operand layout (one
+//           contiguous block per 64-wide K slice), into a three-slot ring with
+//           1-D bulk copies (cp.async.bulk, completion counted on an mbarrier);
+//   warp 1  MMA issuer: one thread runs the (layer, tile) jobs in the order
+//           A0 B0 A1 B1 ..., each job's slices into its tile's accumulator
+//           (two 128 x 256 FP32 blocks, 512 TMEM columns);
+//   warps 4-7 / 8-11  epilogue of tile A / tile B: TMEM -> bias + SiLU ->
+//           BF16 -> the tile's activation operand in shared memory (the input
+//           of the next layer), or FP32 outputs after the last layer; they also
+//           load the next input tile.
+// So tile A's epilogue of layer l overlaps tile B's MMAs of layer l and vice
+// versa; activations never leave shared memory. All waits are bounded.
+constexpr int kFwdMaxLayers = 8;
+constexpr int kFwdThreads = 384;               // 12 warps
+constexpr int kFwdKmax = 256;                  // widest layer input held in shared memory
+constexpr int kFwdSboA = (kFwdKmax / 8) * 128; // 4096 B between row-adjacent core matrices
+constexpr int kFwdAct = kTM * kFwdKmax * 2;    // 64 KB activation operand per tile
+constexpr int kFwdW = kTNmax * kKC * 2;        // 32 KB per weight slice slot
+constexpr int kFwdSlots = 3;
+constexpr int kFwdSmem = 2 * kFwdAct + kFwdSlots * kFwdW + 256;
+constexpr uint32_t kFwdTmemCols = 512;
+
+struct FwdArgs {
+  const bf16* x;     // [rows][fan_in[0]]
+  const uint8_t* wpk;  // packed weight slices
+  const float* p;    // FP32 parameters (biases)
+  float* out;        // [rows][fan_out[L-1]]
+  int rows;
+  int layers;
+  int fan_in[kFwdMaxLayers], fan_out[kFwdMaxLayers], b_off[kFwdMaxLayers], w_off[kFwdMaxLayers];
+  int slice_off[kFwdMaxLayers][4];  // byte offset of slice (l, c) in wpk; slice size = fan_out * 128 B
+  int* err;
+};
+
+__device__ __forceinline__ void cp_async16(void* s, const void* g) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(umma::smem_addr(s)), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(umma::smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(umma::smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+// 1-D bulk copy global -> this CTA's shared memory, completion reported as
+// transaction bytes on `bar` (no multicast).
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   umma::smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(umma::smem_addr(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ uint32_t tanh_bf16x2(uint32_t x) {
+  uint32_t y;
+  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(y) : "r"(x));
+  return y;
+}
+
+// SiLU of two pre-activations, rounded like the training forward: z = BF16(acc
+// + b), then y = z * (1/2 + tanh(z/2)/2) in BF16x2 arithmetic.
+__device__ __forceinline__ uint32_t silu_pair(float a0, float a1, uint32_t* zpair) {
+  const __nv_bfloat162 z = __floats2bfloat162_rn(a0, a1);
+  const __nv_bfloat162 half = __floats2bfloat162_rn(0.5f, 0.5f);
+  const __nv_bfloat162 h = __hmul2(z, half);
+  const uint32_t hb = *reinterpret_cast<const uint32_t*>(&h);
+  const uint32_t tb = tanh_bf16x2(hb);
+  const __nv_bfloat162 t = *reinterpret_cast<const __nv_bfloat162*>(&tb);
+  const __nv_bfloat162 sg = __hfma2(t, half, half);
+  const __nv_bfloat162 y = __hmul2(z, sg);
+  if (zpair) *zpair = *reinterpret_cast<const uint32_t*>(&z);
+  return *reinterpret_cast<const uint32_t*>(&y);
+}
+
+// Packs W_l into per-slice canonical K-major blocks: slice (l, c) element
+// (n, k) at slice_off + (n/8)*1024 + (k/8)*128 + (n%8)*16 + (k%8)*2; K columns
+// past fan_in are zero.
+__global__ void pack_weights_kernel(const bf16* pb, const FwdArgs A, uint8_t* wpk) {
+  for (int l = 0; l < A.layers; ++l) {
+    const int N = A.fan_out[l], K = A.fan_in[l], nch = (K + kKC - 1) / kKC;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nch * N * 8; t += gridDim.x * blockDim.x) {
+      const int c = t / (N * 8), rem = t - c * N * 8, n = rem >> 3, g = rem & 7;
+      const int k = c * kKC + g * 8;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (k < K) v = *reinterpret_cast<const uint4*>(pb + A.w_off[l] + static_cast<size_t>(n) * K + k);
+      *reinterpret_cast<uint4*>(wpk + A.slice_off[l][c] + (n >> 3) * kSBO + g * kLBO + (n & 7) * 16) = v;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kFwdThreads, 1) mlp_forward_fused_kernel(const FwdArgs A) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t* act[2] = {smem, smem + kFwdAct};
+  uint8_t* ring = smem + 2 * kFwdAct;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * kFwdAct + kFwdSlots * kFwdW);
+  uint64_t* full = bars;              // [3] slice landed
+  uint64_t* empty = bars + 3;         // [3] slice consumed by the tensor core
+  uint64_t* acc_full = bars + 6;      // [2] tile's layer accumulated
+  uint64_t* act_ready = bars + 8;     // [2] tile's layer input written (128 arrivals)
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 10);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 11);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ntiles = A.rows / kTM;
+  const int npairs = (ntiles + 1) / 2;
+  if (tid == 0) {
+    for (int b = 0; b < 3; ++b) {
+      umma::mbar_init(&full[b], 1);
+      umma::mbar_init(&empty[b], 1);
+    }
+    for (int t = 0; t < 2; ++t) {
+      umma::mbar_init(&acc_full[t], 1);
+      umma::mbar_init(&act_ready[t], kTM);
+    }
+    *abort_flag = 0;
+  }
+  if (warp == 1) umma::tmem_alloc(tslot, kFwdTmemCols);
+  umma::tc_fence_before();
+  __syncthreads();
+  umma::tc_fence_after();
+  const uint32_t tmem = *tslot;
+  auto tiles_of = [&](int pair) { return 2 * pair + 1 < ntiles ? 2 : 1; };
+  auto wait = [&](uint64_t* bar, uint32_t parity) -> bool {
+    if (*abort_flag) return false;
+    if (umma::mbar_wait(bar, parity, A.err, 3)) return true;
+    *abort_flag = 1;
+    return false;
+  };
+
+  if (warp == 0) {
+    // ---- producer ----
+    if (lane == 0) {
+      uint32_t k = 0;
+      bool ok = true;
+      for (int pair = blockIdx.x; pair < npairs && ok; pair += gridDim.x) {
+        const int nt = tiles_of(pair);
+        for (int l = 0; l < A.layers && ok; ++l) {
+          const int nch = (A.fan_in[l] + kKC - 1) / kKC;
+          const uint32_t bytes = static_cast<uint32_t>(A.fan_out[l]) * (kKC * 2);
+          for (int t = 0; t < nt && ok; ++t)
+            for (int c = 0; c < nch; ++c, ++k) {
+              const uint32_t slot = k % kFwdSlots;
+              if (k >= kFwdSlots && !(ok = wait(&empty[slot], ((k / kFwdSlots) - 1) & 1u))) break;
+              mbar_expect_tx(&full[slot], bytes);
+              bulk_g2s(ring + slot * kFwdW, A.wpk + A.slice_off[l][c], bytes, &full[slot]);
+            }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ---- MMA issuer ----
+    if (lane == 0) {
+      uint32_t k = 0, ph_act[2] = {0u, 0u};
+      bool ok = true;
+      for (int pair = blockIdx.x; pair < npairs && ok; pair += gridDim.x) {
+        const int nt = tiles_of(pair);
+        for (int l = 0; l < A.layers && ok; ++l) {
+          const int N = A.fan_out[l], K = A.fan_in[l], nch = (K + kKC - 1) / kKC;
+          const uint32_t idesc = umma::instr_desc_bf16_f32(kTM, N, false, false);
+          for (int t = 0; t < nt && ok; ++t) {
+            if (!(ok = wait(&act_ready[t], ph_act[t]))) break;
+            ph_act[t] ^= 1u;
+            umma::tc_fence_after();
+            const uint32_t a0 = umma::smem_addr(act[t]);
+            for (int c = 0; c < nch; ++c, ++k) {
+              const uint32_t slot = k % kFwdSlots;
+              if (!(ok = wait(&full[slot], (k / kFwdSlots) & 1u))) break;
+              umma::tc_fence_after();
+              const uint32_t bsm = umma::smem_addr(ring + slot * kFwdW);
+              const int nks = min(kKC, K - c * kKC) / 16;
+              for (int ks = 0; ks < nks; ++ks) {
+                const uint64_t ad = umma::smem_desc(a0 + (c * (kKC / 8) + 2 * ks) * kLBO, kLBO, kFwdSboA);
+                const uint64_t bd = umma::smem_desc(bsm + ks * 2 * kLBO, kLBO, kSBO);
+                umma::mma_bf16(tmem + t * kTNmax, ad, bd, idesc, (c > 0 || ks > 0) ? 1u : 0u);
+              }
+              umma::mma_commit(&empty[slot]);
+            }
+            if (ok) umma::mma_commit(&acc_full[t]);
+          }
+        }
+      }
+    }
+  } else if (warp >= 4) {
+    // ---- epilogue warpgroups ----
+    const int t = (warp - 4) >> 2, quarter = warp & 3;
+    const int row = quarter * 32 + lane;
+    const uint32_t tbase = tmem + (static_cast<uint32_t>(quarter * 32) << 16) + t * kTNmax;
+    const int G = A.fan_in[0] / 8;
+    auto load_x = [&](int pair) {
+      const int m0 = (2 * pair + t) * kTM;
+      for (int i = row; i < kTM * G; i += kTM) {
+        const int r = i / G, g = i - r * G;
+        cp_async16(act[t] + (r >> 3) * kFwdSboA + g * kLBO + (r & 7) * 16,
+                   A.x + static_cast<size_t>(m0 + r) * A.fan_in[0] + g * 8);
+      }
+      cp_async_commit();
+      cp_async_wait_all();
+      umma::fence_async_smem();
+    };
+    uint32_t ph_acc = 0;
+    bool ok = true;
+    int pair = blockIdx.x;
+    if (pair < npairs && t < tiles_of(pair)) {
+      load_x(pair);
+      mbar_arrive(&act_ready[t]);
+    }
+    for (; pair < npairs && ok; pair += gridDim.x) {
+      if (t >= tiles_of(pair)) break;
+      const int m0 = (2 * pair + t) * kTM;
+      for (int l = 0; l < A.layers && ok; ++l) {
+        if (!(ok = wait(&acc_full[t], ph_acc))) break;
+        ph_acc ^= 1u;
+        umma::tc_fence_after();
+        const int N = A.fan_out[l];
+        const float* bias = A.p + A.b_off[l];
+        const bool last = l + 1 == A.layers;
+        for (int c0 = 0; c0 < N; c0 += 32) {
+          uint32_t r[32];
+          umma::tmem_ld16(tbase + static_cast<uint32_t>(c0), *reinterpret_cast<uint32_t(*)[16]>(r));
+          umma::tmem_ld16(tbase + static_cast<uint32_t>(c0 + 16), *reinterpret_cast<uint32_t(*)[16]>(r + 16));
+          umma::tmem_wait_ld();
+          if (!last) {
+            uint32_t y[16];
+#pragma unroll
+            for (int j = 0; j < 32; j += 2)
+              y[j / 2] = silu_pair(__uint_as_float(r[j]) + __ldg(bias + c0 + j),
+                                   __uint_as_float(r[j + 1]) + __ldg(bias + c0 + j + 1), nullptr);
+            uint8_t* dst = act[t] + (row >> 3) * kFwdSboA + (c0 / 8) * kLBO + (row & 7) * 16;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+              *reinterpret_cast<uint4*>(dst + q * kLBO) = make_uint4(y[4 * q], y[4 * q + 1], y[4 * q + 2], y[4 * q + 3]);
+          } else {
+            float* o = A.out + static_cast<size_t>(m0 + row) * N + c0;
+#pragma unroll
+            for (int j = 0; j < 32; j += 4)
+              if (c0 + j < N)
+                *reinterpret_cast<float4*>(o + j) = make_float4(
+                    __uint_as_float(r[j]) + __ldg(bias + c0 + j), __uint_as_float(r[j + 1]) + __ldg(bias + c0 + j + 1),
+                    __uint_as_float(r[j + 2]) + __ldg(bias + c0 + j + 2),
+                    __uint_as_float(r[j + 3]) + __ldg(bias + c0 + j + 3));
+          }
+        }
+        umma::tc_fence_before();
+        if (!last) {
+          umma::fence_async_smem();
+          mbar_arrive(&act_ready[t]);
+        } else {
+          const int np = pair + static_cast<int>(gridDim.x);
+          if (np < npairs && t < tiles_of(np)) {
+            load_x(np);
+            mbar_arrive(&act_ready[t]);
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (warp == 1) {
+    umma::tc_fence_after();
+    umma::tmem_dealloc(tmem, kFwdTmemCols);
+  }
+}
+
 }  // namespace mlp
 }  // namespace ce
 
@@ -255,6 +543,10 @@ struct ce_mlp {
   float* loss = nullptr;              // device scalar
   int* err = nullptr;                 // device error flag
   uint64_t step = 0;
+  // weights packed for the fused forward, refreshed when the parameters change
+  uint8_t* wpk = nullptr;
+  size_t wpk_bytes = 0;
+  uint64_t param_version = 1, packed_version = 0;
   std::string msg;
 };
 
@@ -390,6 +682,16 @@ int backward(ce_mlp* net, const bf16* x, const float* target, const float* w, ui
   return cudaGetLastError() == cudaSuccess ? CE_OK : set_err(net, CE_ERR_CUDA, "backward launch");
 }
 
+// The fused serving forward holds a 128-row tile of every layer's input in
+// shared memory (width <= 256) and splits each layer's columns over two warp
+// groups in 16-column TMEM loads (width a multiple of 32).
+bool fused_eligible(const ce_mlp* n) {
+  if (n->layers > ce::mlp::kFwdMaxLayers || n->in_dim > ce::mlp::kFwdKmax || n->in_dim % 8) return false;
+  for (int l = 0; l < n->layers; ++l)
+    if (n->fan_out[l] % 32 || n->fan_out[l] > ce::mlp::kTNmax) return false;
+  return n->n_params < (1ull << 31);
+}
+
 int check_err_flag(ce_mlp* net, cudaStream_t s) {
   int h = 0;
   if (cudaMemcpyAsync(&h, net->err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
@@ -477,6 +779,7 @@ void ce_mlp_destroy(ce_mlp* n) {
                   static_cast<void*>(n->err), static_cast<void*>(n->out), static_cast<void*>(n->dout),
                   static_cast<void*>(n->dA), static_cast<void*>(n->dB)})
     if (p) cudaFree(p);
+  if (n->wpk) cudaFree(n->wpk);
   for (bf16* z : n->Z) cudaFree(z);
   for (bf16* h : n->H) cudaFree(h);
   delete n;
@@ -491,6 +794,7 @@ int ce_mlp_set_params(ce_mlp* n, const float* host) {
   cudaSetDevice(n->device);
   if (cudaMemcpy(n->p, host, n->n_params * 4, cudaMemcpyHostToDevice) != cudaSuccess) return CE_ERR_CUDA;
   ce::mlp::f32_to_bf16_kernel<<<256, 256>>>(n->p, n->pb, static_cast<int>(n->n_params));
+  ++n->param_version;
   return cudaDeviceSynchronize() == cudaSuccess ? CE_OK : CE_ERR_CUDA;
 }
 
@@ -500,8 +804,9 @@ int ce_mlp_get_params(const ce_mlp* n, float* host) {
   return cudaMemcpy(host, n->p, n->n_params * 4, cudaMemcpyDeviceToHost) == cudaSuccess ? CE_OK : CE_ERR_CUDA;
 }
 
-int ce_mlp_forward(ce_mlp* n, const void* x, uint64_t B, float* out, void* stream) {
-  if (!n || !x || !out || B == 0 || B % 128 || B > n->max_batch) return set_err(n, CE_ERR_INVALID, "ce_mlp_forward: B must be a positive multiple of 128 up to max_batch");
+int ce_mlp_forward_layered(ce_mlp* n, const void* x, uint64_t B, float* out, void* stream) {
+  if (!n || !x || !out || B == 0 || B % 128 || B > n->max_batch)
+    return set_err(n, CE_ERR_INVALID, "ce_mlp_forward_layered: B must be a positive multiple of 128 up to max_batch");
   cudaSetDevice(n->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   int rc = forward(n, static_cast<const bf16*>(x), B, s);
@@ -509,6 +814,57 @@ int ce_mlp_forward(ce_mlp* n, const void* x, uint64_t B, float* out, void* strea
   if (cudaMemcpyAsync(out, n->out, B * n->out_dim * 4, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
     return set_err(n, CE_ERR_CUDA, "copy out");
   return CE_OK;
+}
+
+int ce_mlp_forward(ce_mlp* n, const void* x, uint64_t B, float* out, void* stream) {
+  if (!n || !x || !out || B == 0 || B % 128) return set_err(n, CE_ERR_INVALID, "ce_mlp_forward: B must be a positive multiple of 128");
+  if (!fused_eligible(n)) {
+    if (B > n->max_batch) return set_err(n, CE_ERR_INVALID, "ce_mlp_forward: B exceeds max_batch");
+    return ce_mlp_forward_layered(n, x, B, out, stream);
+  }
+  if (B > (1ull << 30)) return set_err(n, CE_ERR_INVALID, "ce_mlp_forward: B above 2^30 rows");
+  cudaSetDevice(n->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  using namespace ce::mlp;
+  FwdArgs a{};
+  a.x = static_cast<const bf16*>(x);
+  a.p = n->p;
+  a.out = out;
+  a.rows = static_cast<int>(B);
+  a.layers = n->layers;
+  size_t off = 0;
+  for (int l = 0; l < n->layers; ++l) {
+    a.fan_in[l] = n->fan_in[l];
+    a.fan_out[l] = n->fan_out[l];
+    a.w_off[l] = static_cast<int>(n->w_off[l]);
+    a.b_off[l] = static_cast<int>(n->b_off[l]);
+    for (int c = 0; c * kKC < n->fan_in[l]; ++c) {
+      a.slice_off[l][c] = static_cast<int>(off);
+      off += static_cast<size_t>(n->fan_out[l]) * kKC * 2;
+    }
+  }
+  a.err = n->err;
+  if (off > n->wpk_bytes) {
+    if (n->wpk) cudaFree(n->wpk);
+    n->wpk = nullptr;
+    n->wpk_bytes = 0;
+    if (cudaMalloc(&n->wpk, off) != cudaSuccess) return set_err(n, CE_ERR_CUDA, "cudaMalloc(packed weights)");
+    n->wpk_bytes = off;
+    n->packed_version = 0;
+  }
+  a.wpk = n->wpk;
+  if (n->packed_version != n->param_version) {
+    pack_weights_kernel<<<128, 256, 0, s>>>(n->pb, a, n->wpk);
+    n->packed_version = n->param_version;
+  }
+  if (cudaFuncSetAttribute(mlp_forward_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwdSmem) !=
+      cudaSuccess)
+    return set_err(n, CE_ERR_CUDA, "cudaFuncSetAttribute(fused forward)");
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, n->device);
+  const int pairs = static_cast<int>((B / kTM + 1) / 2);
+  mlp_forward_fused_kernel<<<pairs < sms ? pairs : sms, kFwdThreads, kFwdSmem, s>>>(a);
+  return cudaGetLastError() == cudaSuccess ? CE_OK : set_err(n, CE_ERR_CUDA, "fused forward launch");
 }
 
 int ce_mlp_gradients(ce_mlp* n, const void* x, const float* target, const float* weight, uint64_t B, float* loss,
@@ -538,6 +894,7 @@ int ce_mlp_train_step(ce_mlp* n, const void* x, const float* target, const float
   if (rc == CE_OK) rc = backward(n, static_cast<const bf16*>(x), target, weight, B, s);
   if (rc != CE_OK) return rc;
   ++n->step;
+  ++n->param_version;
   const float b1 = 0.9f, b2 = 0.999f;
   const float c1 = 1.0f - std::pow(b1, static_cast<float>(n->step));
   const float c2 = 1.0f - std::pow(b2, static_cast<float>(n->step));

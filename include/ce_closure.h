@@ -37,8 +37,15 @@ const char* ce_mlp_last_error(const ce_mlp* n);
 uint64_t ce_mlp_param_count(const ce_mlp* n);
 int ce_mlp_set_params(ce_mlp* n, const float* host);
 int ce_mlp_get_params(const ce_mlp* n, float* host);
-/* x: [B][in_dim] BF16 (device), out: [B][out_dim] FP32 (device). Async on stream. */
+/* Serving forward. x: [B][in_dim] BF16 (device), out: [B][out_dim] FP32
+ * (device); async on stream. When every layer is at most 256 wide and a
+ * multiple of 32, with at most 8 layers, one fused persistent kernel runs the
+ * whole network and B may be any multiple of 128 up to 2^30 (else B <=
+ * max_batch and the per-layer path below is used). Both paths round at the
+ * same points, so they agree bit for bit. */
 int ce_mlp_forward(ce_mlp* n, const void* x, uint64_t B, float* out, void* stream);
+/* The per-layer forward of the training path (B <= max_batch), for tests. */
+int ce_mlp_forward_layered(ce_mlp* n, const void* x, uint64_t B, float* out, void* stream);
 /* Loss = sum(weight * (out - target)^2) with weights summing to 1 over the batch
  * (target, weight: [B][out_dim] FP32, device). Synchronous: writes the loss and,
  * if grads_host is not NULL, the FP32 gradients in parameter layout. */
@@ -63,12 +70,13 @@ int ce_umma_gemm_f32(const void* A, int a_mn, const void* B, int b_mn, int M, in
 
 /* ---- the closure around the mixed-batch engine ---------------------------
  * Rows are the mixed layout of ce_gpu.h (10 atoms per sim). Per sim the
- * network sees CE_CLOSURE_FEATURES BF16 inputs: per atom i < 10 the 9 values
- * (x_i - x_com)/L (3), p_i/P (3), q_i/3, ln(m_i / amu)/3.5, 1 (zeros for the
- * padded atoms), then PE_stop/E_0 * 20, n/10 and zeros; L is the RMS distance
- * from the centre of mass and P the RMS atom momentum of the base. It predicts
- * CE_CLOSURE_OUTPUTS values, the first 3n being (p_inf - p_base)/P. */
-#define CE_CLOSURE_FEATURES 96
+ * network sees CE_CLOSURE_FEATURES BF16 inputs: per atom i < 10 the 12 values
+ * (x_i - x_com)/L (3), p_i/P (3), (p_base,i - p_i)/P (3), q_i/3,
+ * ln(m_i / amu)/3.5, 1 (zeros for the padded atoms), then PE_stop/E_0 * 20,
+ * n/10 and zeros; L is the RMS distance from the centre of mass, P the RMS
+ * atom momentum of the base p_base. It predicts CE_CLOSURE_OUTPUTS values, the
+ * first 3n being (p_inf - p_base)/P. */
+#define CE_CLOSURE_FEATURES 128
 #define CE_CLOSURE_OUTPUTS 32
 
 /* State at the loose stop, as ce_run_mixed_device writes it with
@@ -94,11 +102,12 @@ typedef struct ce_closure_gate {
 void ce_closure_default_gate(ce_closure_gate* g);
 
 /* Features, ballistic base and (if target != NULL) training targets for S sims
- * (device pointers, async on stream). feats [pad128(S)][96] BF16 (padded rows
+ * (device pointers, async on stream). feats [pad128(S)][128] BF16 (padded rows
  * zeroed); p_base [S][10][3]; p_scale [S] (0 for one-atom or unconverged sims,
  * NaN when the ballistic integral does not exist); target, weight
- * [pad128(S)][32] FP32 with target = (p_true - p_base)/P and weight =
- * weight_scale / (3n) on the 3n live components, zero elsewhere. */
+ * [pad128(S)][32] FP32 with target = (p_true - p_base)/P and, on the 3n live
+ * components (zero elsewhere), weight = weight_scale / (3n) * 1e-3 /
+ * sqrt(rms^2 + (2e-5)^2) where rms is the sim's RMS target: a relative loss. */
 int ce_closure_features(uint64_t S, const ce_mixed_batch* in, double coulomb_k, const ce_closure_state* st,
                         const float* p_true, float weight_scale, void* feats, float* p_base, float* p_scale,
                         float* target, float* weight, void* stream);
@@ -113,7 +122,7 @@ int ce_closure_apply(uint64_t S, const ce_mixed_batch* in, const ce_closure_stat
                      const float* p_base, const float* p_scale, const float* net_out, const ce_closure_gate* gate,
                      const ce_outputs* out, uint8_t* fallback, unsigned long long* counts, void* stream);
 
-/* Serving pipeline bound to one engine and one network (in_dim 96, out_dim 32):
+/* Serving pipeline bound to one engine and one network (in_dim 128, out_dim 32):
  * loose run (cfg with pe_stop_fraction = loose_pe_stop and no rescale) ->
  * features -> network -> gate -> plain run (cfg) of the sims sent back ->
  * merge. Device pointers, stream-ordered, no host synchronisation and no

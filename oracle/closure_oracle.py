@@ -8,8 +8,9 @@ A float64 numpy restatement of include/ce_closure.h for mixed rows of 10 atoms:
   I0 = 1/(|r|(|r||w| + r.w)), I1 = 1/(|w|(|r||w| + r.w)), rescaled to
   KE = E_0 (the reference's rescale, src/driver.cpp:38-42, applied to the
   ballistic state);
-* features: per atom (x - x_com)/L, p/P, q/3, ln(m/amu)/3.5, 1, then
-  PE_stop/E_0 * 20 and n/10 (BF16-rounded like the device);
+* features: per atom (x - x_com)/L, p/P, (p_base - p)/P, q/3, ln(m/amu)/3.5,
+  1, then PE_stop/E_0 * 20 and n/10 (BF16-rounded like the device);
+* training targets and the relative loss weights;
 * gate: |KE/E_0 - 1|, |sum p|/sum|p|, |correction|/|base|, then projection
   to zero net momentum (mass weighted) and rescale to E_0.
 """
@@ -64,21 +65,38 @@ def ballistic_base(n, mass, charge, x, p, e0, k=1.0):
 
 
 def features(n, mass, charge, x, p, e0, pe_final, k=1.0):
-    """(feats [S,96] float64 of BF16 values, p_base, P)."""
+    """(feats [S,128] float64 of BF16 values, p_base, P)."""
     pb, P, L, com = ballistic_base(n, mass, charge, x, p, e0, k)
     S = n.shape[0]
-    f = np.zeros((S, 96), np.float32)
+    f = np.zeros((S, 128), np.float32)
     for s in range(S):
         k_ = int(n[s])
         for i in range(k_):
-            f[s, 9 * i:9 * i + 3] = (x[s, i] - com[s]) / L[s]
-            f[s, 9 * i + 3:9 * i + 6] = p[s, i] / P[s]
-            f[s, 9 * i + 6] = charge[s, i] / 3.0
-            f[s, 9 * i + 7] = np.log(mass[s, i] / MASS_UNIT) / 3.5
-            f[s, 9 * i + 8] = 1.0
-        f[s, 90] = pe_final[s] / e0[s] * 20.0
-        f[s, 91] = k_ * 0.1
+            o = 12 * i
+            f[s, o:o + 3] = (x[s, i] - com[s]) / L[s]
+            f[s, o + 3:o + 6] = p[s, i] / P[s]
+            f[s, o + 6:o + 9] = (pb[s, i] - p[s, i]) / P[s]
+            f[s, o + 9] = charge[s, i] / 3.0
+            f[s, o + 10] = np.log(mass[s, i] / MASS_UNIT) / 3.5
+            f[s, o + 11] = 1.0
+        f[s, 120] = pe_final[s] / e0[s] * 20.0
+        f[s, 121] = k_ * 0.1
     return to_bf16(f), pb, P
+
+
+def targets(n, p_base, P, p_true, weight_scale=1.0):
+    """(target [S,32], weight [S,32]): (p_true - p_base)/P and the relative
+    loss weight weight_scale/(3n) * 1e-3 / sqrt(rms^2 + (2e-5)^2)."""
+    S = n.shape[0]
+    t = np.zeros((S, 32))
+    w = np.zeros((S, 32))
+    for s in range(S):
+        k_ = int(n[s])
+        v = ((p_true[s, :k_] - p_base[s, :k_]) / P[s]).reshape(-1)
+        t[s, :3 * k_] = v
+        rms2 = np.sum(v * v) / (3 * k_)
+        w[s, :3 * k_] = weight_scale / (3 * k_) * 1e-3 / np.sqrt(rms2 + 2e-5 ** 2)
+    return t, w
 
 
 def apply_gate(n, mass, e0, p_base, P, out, tol_e, tol_p, tol_c):

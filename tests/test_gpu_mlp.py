@@ -102,3 +102,49 @@ def test_network_gradients_match_oracle(ce):
         assert loss.value < 0.8 * first
     finally:
         lib.ce_mlp_destroy(h)
+
+
+def test_fused_forward_equals_layered_forward(ce):
+    """The serving network (128 -> 4 x 256 -> 32) through the fused persistent
+    kernel over 300 row tiles (two passes of the grid) equals the training
+    path's per-layer forward bit for bit, and the oracle within 1e-2."""
+    torch = pytest.importorskip("torch")
+    in_dim, hidden, depth, out_dim, B = 128, 256, 4, 32, 128 * 300
+    lib, h = make_net(ce, in_dim, hidden, depth, out_dim, B, seed=11)
+    try:
+        P = int(lib.ce_mlp_param_count(h))
+        params = np.zeros(P, np.float32)
+        assert lib.ce_mlp_get_params(h, params.ctypes.data) == 0
+        rng = np.random.default_rng(8)
+        params += rng.standard_normal(P).astype(np.float32) * 0.02
+        assert lib.ce_mlp_set_params(h, params.ctypes.data) == 0
+        x = mo.to_bf16(rng.standard_normal((B, in_dim)))
+        xd = bf16_tensor(torch, x)
+        fused = torch.full((B, out_dim), float("nan"), dtype=torch.float32, device="cuda")
+        layered = torch.zeros((B, out_dim), dtype=torch.float32, device="cuda")
+        for _ in range(2):  # a second call reuses the same kernel state
+            assert lib.ce_mlp_forward(h, xd.data_ptr(), B, fused.data_ptr(), None) == 0, lib.ce_mlp_last_error(h)
+        assert lib.ce_mlp_forward_layered(h, xd.data_ptr(), B, layered.data_ptr(), None) == 0
+        assert lib.ce_mlp_check(h, None) == 0
+        torch.cuda.synchronize()
+        assert torch.equal(fused, layered)
+        ref, _, _ = mo.forward(params, x[:512], in_dim, hidden, depth, out_dim, bf16=True)
+        got = fused[:512].cpu().numpy()
+        assert np.linalg.norm(got - ref) <= 1e-2 * np.linalg.norm(ref)
+    finally:
+        lib.ce_mlp_destroy(h)
+
+
+def test_forward_limits(ce):
+    torch = pytest.importorskip("torch")
+    # a width that is not a multiple of 32 takes the per-layer path, bounded by max_batch
+    lib, h = make_net(ce, 96, 48, 2, 32, 256)
+    try:
+        x = torch.zeros((512, 96), dtype=torch.bfloat16, device="cuda")
+        out = torch.zeros((512, 32), dtype=torch.float32, device="cuda")
+        assert lib.ce_mlp_forward(h, x.data_ptr(), 256, out.data_ptr(), None) == 0
+        assert lib.ce_mlp_forward(h, x.data_ptr(), 512, out.data_ptr(), None) == ce.CE_ERR_INVALID
+        assert lib.ce_mlp_forward(h, x.data_ptr(), 100, out.data_ptr(), None) == ce.CE_ERR_INVALID
+        assert lib.ce_mlp_check(h, None) == 0
+    finally:
+        lib.ce_mlp_destroy(h)
