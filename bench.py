@@ -598,6 +598,212 @@ def run_closure(args):
     return 0
 
 
+def run_stream(args):
+    """Config-5 production generation: `--total` (default 1e8) explosions of the
+    10-atom C2H6-like molecule (2 C q=+2, 8 H q=+1, radius 4.0, pairs >= 0.5) in
+    1e6-sim chunks. Per chunk, on a compute stream: Philox geometries on the
+    device, then the integration replayed from a CUDA graph captured once per
+    buffer slot; on a side stream: the chunk's momenta / KER / steps / status
+    copied into a pinned host ring (two slots) that the host consumes while the
+    next chunk computes. Plain RK45 and the learned closure (a network trained
+    on this molecule, held-out sims) run the same pipeline back to back; the
+    timed region is the whole stream, first geometry to last host byte."""
+    import ctypes
+    import importlib
+
+    import torch
+
+    from __graft_entry__ import load_package
+
+    ce = load_package()
+    cl = importlib.import_module("coulomb_explosion_b200.closure")
+    wl = importlib.import_module("coulomb_explosion_b200.workloads")
+    sp = importlib.import_module("coulomb_explosion_b200.sampling")
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_lib as ol
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    mol = wl.C2H6_LIKE
+    rtol, atol, pes = TIGHT
+    cfg = ce.RunConfig(rtol=rtol, atol=atol, pe_stop_fraction=pes, precision_mode=args.mode)
+    C_ = 1_000_000
+    total = (args.total // C_) * C_
+    seed = SEED + 5
+    eng = ce.Engine(0)
+    eng.reserve_mixed(C_)
+
+    # ---- network for this molecule, trained on held-out sims (counter range above the stream)
+    t0 = time.perf_counter()
+    mb = args.minibatch
+    tb = cl.sample_molecule_device(mol, args.train_sims, seed, first_sim=1 << 40)
+    torch.cuda.synchronize()
+    ts, loose_t, base_t, plain_t = cl.make_training_set(eng, tb, cfg, minibatch=mb)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    perm = torch.randperm(ts.S, generator=g, device=dev)
+    n_val = max(mb, ts.S // 50)
+    val_rows, train_rows = perm[:n_val], perm[n_val:]
+    train_rows = train_rows[ts.valid[train_rows]]
+    net = cl.Network(max_batch=65536, seed=seed)
+    rep = cl.train(net, ts, epochs=args.epochs, minibatch=mb, lr=args.lr, lr_final=args.lr * 1e-2, seed=seed,
+                   train_rows=train_rows)
+    net.scale_output_layer(1.0 / cl.TARGET_SCALE)
+    out_t = cl.net_forward(net, ts.feats)
+    stats = cl.gate_stats(tb, loose_t, base_t, out_t)
+    vmask = torch.zeros(ts.S, dtype=torch.bool, device=dev)
+    vmask[val_rows] = True
+    vmask &= ts.valid
+    gate = cl.calibrate_gate(stats, vmask, quantile=args.gate_quantile)
+    val_err = cl.rel_err(cl.predict(tb, base_t, out_t)[vmask], plain_t["momenta"][vmask]).float()
+    ana_err = cl.rel_err(base_t["p_base"][vmask], plain_t["momenta"][vmask]).float()
+    train_s = time.perf_counter() - t0
+    del ts, loose_t, base_t, plain_t, out_t, stats, tb
+    torch.cuda.empty_cache()
+
+    # ---- two buffer slots, pinned host ring
+    slots = []
+    for _ in range(2):
+        b = cl.sample_molecule_device(mol, C_, seed, first_sim=0)
+        d = {"batch": b, "cb": b.c(),
+             "momenta": torch.empty((C_, 10, 3), dtype=torch.float32, device=dev),
+             "ker": torch.empty(C_, dtype=torch.float64, device=dev),
+             "steps": torch.empty(C_, dtype=torch.int32, device=dev),
+             "status": torch.empty(C_, dtype=torch.uint8, device=dev)}
+        d["out"] = ce.CeOutputs(d["momenta"].data_ptr(), d["ker"].data_ptr(), d["steps"].data_ptr(),
+                                d["status"].data_ptr())
+        d["host"] = {k: torch.empty(d[k].shape, dtype=d[k].dtype, pin_memory=True)
+                     for k in ("momenta", "ker", "steps", "status")}
+        slots.append(d)
+    clo = cl.Closure(eng, net, C_)
+    compute = torch.cuda.Stream(device=dev)
+    side = torch.cuda.Stream(device=dev)
+    cs, ss = compute.cuda_stream, side.cuda_stream
+    bcfg = sp.ball_config(mol, seed)
+    lib = ce.load_library()
+    d2h_bytes = C_ * (120 + 8 + 4 + 1)
+
+    def capture(mode):
+        graphs = []
+        for d in slots:
+            # one eager call first: sizes engine scratch and packs the network weights outside the capture
+            if mode == "closure":
+                clo.serve(d["batch"], cfg, gate, d["out"], stream=cs, cbatch=d["cb"])
+            else:
+                eng.run_mixed_device(C_, d["cb"], cfg, d["out"], ce.CE_SCHEDULE_ONE_LAUNCH, cs)
+            torch.cuda.synchronize()
+            eng.graph_begin(cs)
+            if mode == "closure":
+                clo.serve(d["batch"], cfg, gate, d["out"], stream=cs, cbatch=d["cb"])
+            else:
+                eng.run_mixed_device(C_, d["cb"], cfg, d["out"], ce.CE_SCHEDULE_ONE_LAUNCH, cs)
+            graphs.append(eng.graph_end(cs))
+        return graphs
+
+    def stream_run(graphs, keep_first):
+        done_ev = [torch.cuda.Event() for _ in range(2)]
+        copied_ev = [torch.cuda.Event() for _ in range(2)]
+        first = None
+        ok_count = 0
+        nchunks = total // C_
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        start.record(compute)
+
+        def consume(i):
+            nonlocal first, ok_count
+            d = slots[i % 2]
+            copied_ev[i % 2].synchronize()
+            ok_count += int((d["host"]["status"].numpy() == 0).sum())
+            if keep_first and i == 0:
+                first = {k: v.clone() for k, v in d["host"].items()}
+
+        for i in range(nchunks):
+            d = slots[i % 2]
+            if i >= 2:
+                compute.wait_event(copied_ev[i % 2])
+            rc = lib.ce_sample_ball_device(10, i * C_, C_, ctypes.byref(bcfg), ctypes.c_void_p(d["batch"].pos.data_ptr()),
+                                           None, ctypes.c_void_p(cs))
+            assert rc == 0
+            graphs[i % 2].launch(cs)
+            done_ev[i % 2].record(compute)
+            side.wait_event(done_ev[i % 2])
+            with torch.cuda.stream(side):
+                for k in ("momenta", "ker", "steps", "status"):
+                    d["host"][k].copy_(d[k], non_blocking=True)
+            copied_ev[i % 2].record(side)
+            if i >= 1:
+                consume(i - 1)
+        consume(nchunks - 1)
+        stop.record(side)
+        torch.cuda.synchronize()
+        return start.elapsed_time(stop), ok_count, first
+
+    res = {}
+    firsts = {}
+    with ClockSampler(0) as clk:
+        for mode in ("plain", "closure"):
+            graphs = capture(mode)
+            stream_run(graphs, False)  # warm-up pass over the first chunks is the capture call; one full untimed pass
+            ms, okc, first = stream_run(graphs, True)
+            res[mode] = {"explosions_per_s": total / (ms / 1e3), "seconds": ms / 1e3, "status_ok_frac": okc / total}
+            firsts[mode] = first
+            for gph in graphs:
+                gph.close()
+    acc, fbk = clo.counts()
+
+    # accuracy on the first chunk: closure vs plain, both vs the FP64 oracle on a subset
+    pc = firsts["closure"]["momenta"].double()
+    pp = firsts["plain"]["momenta"].double()
+    okm = (firsts["closure"]["status"] == 0) & (firsts["plain"]["status"] == 0)
+    e_cp = cl.rel_err(pc[okm], pp[okm]).float()
+    n_sub = args.fp64_subset
+    sub = np.linspace(0, C_ - 1, n_sub).astype(np.int64)
+    x32 = np.zeros((n_sub, 10, 3), np.float32)
+    for j, i in enumerate(sub):
+        a_, _, _ = sp.sample_ball_host(mol, 1, seed, first_sim=int(i))
+        x32[j] = a_[0]
+    ref = ol.run_batch(x32.astype(np.float64), mol.masses_me, mol.charge_array, bits=64, rtol=1e-10, atol=1e-16,
+                       pe_stop=1e-11)
+    e64_c = ol.config_norm_error(pc.numpy()[sub], ref["momenta"])
+    e64_p = ol.config_norm_error(pp.numpy()[sub], ref["momenta"])
+
+    def dist_t(e):
+        return {"median": float(e.median()), "p99": float(torch.quantile(e[: 1 << 24], 0.99)), "max": float(e.max())}
+
+    def dist_n(e):
+        return {"median": float(np.median(e)), "p99": float(np.percentile(e, 99)), "max": float(e.max())}
+
+    line = {
+        "metric": METRIC + " [config 5: 1e8 C2H6-like N=10 explosions streamed in 1e6 chunks, closure vs plain]",
+        "value": res["closure"]["explosions_per_s"], "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": 1,
+        "ms_per_step": res["closure"]["seconds"] * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 integration, bf16/f32-accumulate network", "data": "synthetic",
+        "config": {"workload": f"{total} C2H6-like (2 C q=+2, 8 H q=+1, r 4.0, min pair 0.5) explosions, "
+                               f"{C_}-sim chunks, Philox geometries on device",
+                   "rtol": rtol, "atol": atol, "pe_stop": pes, "loose_pe_stop": cl.LOOSE_PE_STOP,
+                   "pipeline": "compute stream: sampler + CUDA-graph replay per chunk; side stream: D2H into a "
+                               "2-slot pinned host ring consumed by the host",
+                   "d2h_bytes_per_chunk": d2h_bytes},
+        "plain": res["plain"], "closure": res["closure"],
+        "speedup_vs_plain": res["closure"]["explosions_per_s"] / res["plain"]["explosions_per_s"],
+        "closure_last_chunk": {"accepted": acc, "fallback": fbk},
+        "gate": {"tol_energy": gate.tol_energy, "tol_momentum": gate.tol_momentum,
+                 "tol_correction": gate.tol_correction},
+        "rel_err_vs_plain_first_chunk": dist_t(e_cp),
+        "rel_err_vs_fp64": {"subset": n_sub, "closure": dist_n(e64_c), "plain": dist_n(e64_p),
+                            "fp64": "oracle f64, rtol 1e-10, atol 1e-16, pe_stop 1e-11"},
+        "training": {"sims": args.train_sims, "epochs": rep.epochs, "steps": rep.steps, "seconds_total": train_s,
+                     "validation_network": dist_t(val_err), "validation_analytic_only": dist_t(ana_err)},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+    clo.close()
+    net.close()
+    eng.close()
+    return 0
+
+
 def run_network(args):
     """The closure network's serving forward alone (fused tcgen05 kernel):
     `--sims` rows (default 1e7) of random BF16 features through 128 -> 4 x 256
@@ -663,16 +869,18 @@ def main():
                     help="ch4 (the headline workload), c2h6 (10-atom C2H6-like), h2o (stiff H2O)")
     ap.add_argument("--cpu-budget", type=float, default=8.0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="fixed", choices=["fixed", "mixed", "precision", "closure", "network"],
+    ap.add_argument("--workload", default="fixed", choices=["fixed", "mixed", "precision", "closure", "network", "stream"],
                     help="fixed: one molecule (--molecule); mixed: 2..10-atom population, one launch vs per size; "
                          "closure: learned closure vs plain RK45 on the mixed population; network: the closure "
-                         "network's fused forward alone")
+                         "network's fused forward alone; stream: 1e8 C2H6-like explosions streamed in 1e6 chunks, "
+                         "closure vs plain")
     ap.add_argument("--train-sims", type=int, default=5_000_000, help="closure: training pairs")
     ap.add_argument("--epochs", type=int, default=20, help="closure: training epochs")
     ap.add_argument("--minibatch", type=int, default=8192, help="closure: rows per training step")
     ap.add_argument("--lr", type=float, default=1e-3, help="closure: peak Adam learning rate")
     ap.add_argument("--gate-quantile", type=float, default=0.99, help="closure: gate bounds quantile")
     ap.add_argument("--fp64-subset", type=int, default=300, help="closure: sims checked against the FP64 oracle")
+    ap.add_argument("--total", type=int, default=100_000_000, help="stream: explosions in the whole stream")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -684,6 +892,8 @@ def main():
         return run_closure(args)
     if args.workload == "network":
         return run_network(args)
+    if args.workload == "stream":
+        return run_stream(args)
 
     import torch
 

@@ -157,6 +157,32 @@ def sample_mixed_device(S: int, seed: int, first_sim: int = 0, device: int = 0, 
     return DeviceBatch(n, m, q, x)
 
 
+def sample_molecule_device(mol, S: int, seed: int, first_sim: int = 0, device: int = 0, stream: int = 0,
+                           out: DeviceBatch | None = None) -> DeviceBatch:
+    """One molecule (n <= 10 atoms) in the padded mixed layout: positions from
+    the device Philox ball sampler, masses/charges repeated per row."""
+    from .sampling import ball_config
+
+    torch = _torch()
+    lib = load_library()
+    dev = torch.device("cuda", device)
+    n = mol.n
+    if out is None:
+        m = torch.ones((S, MAX_ATOMS), dtype=torch.float64, device=dev)
+        q = torch.zeros((S, MAX_ATOMS), dtype=torch.float64, device=dev)
+        m[:, :n] = torch.from_numpy(mol.masses_me).to(dev)
+        q[:, :n] = torch.from_numpy(mol.charge_array).to(dev)
+        out = DeviceBatch(torch.full((S,), n, dtype=torch.uint8, device=dev), m, q,
+                          torch.zeros((S, MAX_ATOMS, 3), dtype=torch.float32, device=dev))
+    if n != MAX_ATOMS:
+        raise ValueError("sample_molecule_device fills rows in place only for 10-atom molecules")
+    cfg = ball_config(mol, seed)
+    rc = lib.ce_sample_ball_device(n, int(first_sim), int(S), C.byref(cfg), _vp(out.pos), None, C.c_void_p(stream))
+    if rc != 0:
+        raise EngineError(rc, "ce_sample_ball_device failed")
+    return out
+
+
 def run_plain(engine: Engine, batch: DeviceBatch, cfg: RunConfig, stream: int = 0, coulomb_k: float = 1.0) -> dict:
     """Plain RK45 to cfg's stop, device outputs."""
     torch = _torch()
