@@ -409,7 +409,8 @@ def run_closure(args):
     # ---- training pairs
     t0 = time.perf_counter()
     tb = cl.sample_mixed_device(S_train, seed=seed)
-    ts, loose_t, base_t, plain_t = cl.make_training_set(eng, tb, cfg, minibatch=mb)
+    ts, loose_t, base_t, plain_t = cl.make_training_set(eng, tb, cfg, loose_pe_stop=args.loose_pe_stop,
+                                                         minibatch=mb)
     torch.cuda.synchronize()
     gen_s = time.perf_counter() - t0
     g = torch.Generator(device=dev)
@@ -432,8 +433,12 @@ def run_closure(args):
     vmask = torch.zeros(S_train, dtype=torch.bool, device=dev)
     vmask[val_rows] = True
     vmask &= ts.valid
-    gate = cl.calibrate_gate(stats, vmask, quantile=args.gate_quantile)
     p_net = cl.predict(tb, base_t, out_t)
+    if args.gate_target_err:
+        gate = cl.calibrate_gate_for_error(stats, cl.rel_err(p_net, plain_t["momenta"]), vmask, args.gate_target_err,
+                                           quantile=args.gate_quantile)
+    else:
+        gate = cl.calibrate_gate(stats, vmask, quantile=args.gate_quantile)
     p_ana = base_t["p_base"]
     pl = loose_t["momenta"].double()
     live = (torch.arange(10, device=dev)[None, :] < tb.n[:, None].long()).double()
@@ -491,12 +496,13 @@ def run_closure(args):
 
     with ClockSampler(0) as clk:
         ms_plain = timed(lambda: eng.run_mixed_device(S, batch_c, cfg, c_op, ce.CE_SCHEDULE_ONE_LAUNCH, stream.cuda_stream))
-        ms_clo = timed(lambda: clo.serve(sb, cfg, gate, c_oc, stream=stream.cuda_stream, cbatch=batch_c))
+        ms_clo = timed(lambda: clo.serve(sb, cfg, gate, c_oc, loose_pe_stop=args.loose_pe_stop,
+                                         stream=stream.cuda_stream, cbatch=batch_c))
     acc, fbk = clo.counts()
     fbf = clo.fallback_flags(S, stream.cuda_stream)
     torch.cuda.synchronize()
     # stage breakdown: the loose run alone, and the plain rerun of the sims the gate sent back
-    lcfg = ce.RunConfig(rtol=rtol, atol=atol, pe_stop_fraction=cl.LOOSE_PE_STOP, redistribute_energy=False,
+    lcfg = ce.RunConfig(rtol=rtol, atol=atol, pe_stop_fraction=args.loose_pe_stop, redistribute_energy=False,
                         precision_mode=args.mode)
     lo_m = torch.empty((S, 10, 3), dtype=torch.float32, device=dev)
     lo_x = torch.empty((S, 10, 3), dtype=torch.float32, device=dev)
@@ -564,7 +570,7 @@ def run_closure(args):
         "dtype": "f32 integration, bf16/f32-accumulate network", "data": "synthetic",
         "config": {"workload": f"closure serving of {S} held-out mixed sims per step (N ~ U{{2..10}}, species "
                                "U{H,C,N,O,S}, q ~ U{+1,+2,+3}, radius 2.0 N^(1/3), min pair 0.5, Philox on device)",
-                   "rtol": rtol, "atol": atol, "pe_stop": pes, "loose_pe_stop": cl.LOOSE_PE_STOP,
+                   "rtol": rtol, "atol": atol, "pe_stop": pes, "loose_pe_stop": args.loose_pe_stop,
                    "network": f"{ce.CLOSURE_FEATURES} -> {net.depth} x {net.hidden} SiLU -> 32, bf16 weights/activations, f32 accumulate",
                    "l2": "flushed between timed steps (256 MiB write, outside the events)"},
         "plain": {"value": S / (ms_plain / 1e3), "unit": UNIT, "ms_per_step": ms_plain,
@@ -575,7 +581,10 @@ def run_closure(args):
         "accepted_frac": acc / max(1, acc + fbk), "fallback_sims": fbk,
         "mean_steps_closure_path": float(steps_c[accepted].mean()) if bool(accepted.any()) else None,
         "gate": {"tol_energy": gate.tol_energy, "tol_momentum": gate.tol_momentum,
-                 "tol_correction": gate.tol_correction, "calibration": f"{args.gate_quantile} quantile on validation"},
+                 "tol_correction": gate.tol_correction,
+                 "calibration": (f"correction bound for max validation error <= {args.gate_target_err}, "
+                                 f"energy/momentum at the {args.gate_quantile} quantile") if args.gate_target_err
+                 else f"{args.gate_quantile} quantile on validation"},
         "rel_err_vs_plain": {"all": dist(e_all), "accepted": dist(e_acc)},
         "rel_err_vs_fp64": {"subset": int(n_sub), "closure_all": d_np(e64_c), "closure_accepted": d_np(e64_c[acc_np]),
                             "plain": d_np(e64_p), "fp64": "oracle f64, rtol 1e-10, atol 1e-16, pe_stop 1e-11"},
@@ -638,7 +647,8 @@ def run_stream(args):
     mb = args.minibatch
     tb = cl.sample_molecule_device(mol, args.train_sims, seed, first_sim=1 << 40)
     torch.cuda.synchronize()
-    ts, loose_t, base_t, plain_t = cl.make_training_set(eng, tb, cfg, minibatch=mb)
+    ts, loose_t, base_t, plain_t = cl.make_training_set(eng, tb, cfg, loose_pe_stop=args.loose_pe_stop,
+                                                         minibatch=mb)
     g = torch.Generator(device=dev)
     g.manual_seed(seed)
     perm = torch.randperm(ts.S, generator=g, device=dev)
@@ -655,7 +665,11 @@ def run_stream(args):
     vmask[val_rows] = True
     vmask &= ts.valid
     gate = cl.calibrate_gate(stats, vmask, quantile=args.gate_quantile)
-    val_err = cl.rel_err(cl.predict(tb, base_t, out_t)[vmask], plain_t["momenta"][vmask]).float()
+    p_net_t = cl.predict(tb, base_t, out_t)
+    if args.gate_target_err:
+        gate = cl.calibrate_gate_for_error(stats, cl.rel_err(p_net_t, plain_t["momenta"]), vmask, args.gate_target_err,
+                                           quantile=args.gate_quantile)
+    val_err = cl.rel_err(p_net_t[vmask], plain_t["momenta"][vmask]).float()
     ana_err = cl.rel_err(base_t["p_base"][vmask], plain_t["momenta"][vmask]).float()
     train_s = time.perf_counter() - t0
     del ts, loose_t, base_t, plain_t, out_t, stats, tb
@@ -688,13 +702,13 @@ def run_stream(args):
         for d in slots:
             # one eager call first: sizes engine scratch and packs the network weights outside the capture
             if mode == "closure":
-                clo.serve(d["batch"], cfg, gate, d["out"], stream=cs, cbatch=d["cb"])
+                clo.serve(d["batch"], cfg, gate, d["out"], loose_pe_stop=args.loose_pe_stop, stream=cs, cbatch=d["cb"])
             else:
                 eng.run_mixed_device(C_, d["cb"], cfg, d["out"], ce.CE_SCHEDULE_ONE_LAUNCH, cs)
             torch.cuda.synchronize()
             eng.graph_begin(cs)
             if mode == "closure":
-                clo.serve(d["batch"], cfg, gate, d["out"], stream=cs, cbatch=d["cb"])
+                clo.serve(d["batch"], cfg, gate, d["out"], loose_pe_stop=args.loose_pe_stop, stream=cs, cbatch=d["cb"])
             else:
                 eng.run_mixed_device(C_, d["cb"], cfg, d["out"], ce.CE_SCHEDULE_ONE_LAUNCH, cs)
             graphs.append(eng.graph_end(cs))
@@ -781,7 +795,7 @@ def run_stream(args):
         "vs_baseline": None, "dtype": "f32 integration, bf16/f32-accumulate network", "data": "synthetic",
         "config": {"workload": f"{total} C2H6-like (2 C q=+2, 8 H q=+1, r 4.0, min pair 0.5) explosions, "
                                f"{C_}-sim chunks, Philox geometries on device",
-                   "rtol": rtol, "atol": atol, "pe_stop": pes, "loose_pe_stop": cl.LOOSE_PE_STOP,
+                   "rtol": rtol, "atol": atol, "pe_stop": pes, "loose_pe_stop": args.loose_pe_stop,
                    "pipeline": "compute stream: sampler + CUDA-graph replay per chunk; side stream: D2H into a "
                                "2-slot pinned host ring consumed by the host",
                    "d2h_bytes_per_chunk": d2h_bytes},
@@ -881,6 +895,11 @@ def main():
     ap.add_argument("--gate-quantile", type=float, default=0.99, help="closure: gate bounds quantile")
     ap.add_argument("--fp64-subset", type=int, default=300, help="closure: sims checked against the FP64 oracle")
     ap.add_argument("--total", type=int, default=100_000_000, help="stream: explosions in the whole stream")
+    ap.add_argument("--gate-target-err", type=float, default=0.0,
+                    help="closure/stream: calibrate the gate so accepted validation sims stay within this relative "
+                         "error (0: quantile bounds only)")
+    ap.add_argument("--loose-pe-stop", type=float, default=0.05,
+                    help="closure/stream: potential-energy fraction at which integration hands over to the closure")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

@@ -368,6 +368,25 @@ def calibrate_gate(stats: dict, valid, quantile: float = 0.99) -> CeClosureGate:
     return CeClosureGate(*q)
 
 
+def calibrate_gate_for_error(stats: dict, err, valid, target: float, quantile: float = 0.99) -> CeClosureGate:
+    """Energy and momentum bounds at `quantile` of the validation sims; the
+    correction bound is the largest for which every validation sim that passes
+    all three bounds has error <= target (err: per-sim error of the network's
+    prediction against converged momenta)."""
+    torch = _torch()
+    g = calibrate_gate(stats, valid, quantile)
+    ok = valid & (stats["rho"] <= g.tol_energy) & (stats["mu"] <= g.tol_momentum)
+    c = stats["corr"][ok].double()
+    e = err[ok].double()
+    if c.numel() == 0:
+        return CeClosureGate(g.tol_energy, g.tol_momentum, 0.0)
+    order = torch.argsort(c)
+    bad = torch.cummax(e[order], dim=0).values > target
+    first_bad = int(torch.nonzero(bad)[0].item()) if bool(bad.any()) else c.numel()
+    tol_c = float(c[order[first_bad - 1]].item()) if first_bad > 0 else 0.0
+    return CeClosureGate(g.tol_energy, g.tol_momentum, tol_c)
+
+
 class Closure:
     """ce_closure handle: serving pipeline bound to an engine and a network."""
 

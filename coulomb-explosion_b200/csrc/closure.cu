@@ -15,8 +15,9 @@
 //        I1 = int_0^inf t |r + w t|^-3 dt = 1 / (|w| (|r||w| + r.w)),
 //      with r_ij = x_i - x_j and w_ij = v_i - v_j at the stop;
 //   2. the reference's energy rescale applied to that base (KE = E_0);
-//   3. the network's correction, predicted in units of the base's RMS atom
-//      momentum.
+//   3. the network's correction, predicted in units of Q, the RMS per-atom
+//      size of the analytic step (so the network works at the same relative
+//      scale at any loose stop).
 // Every sim whose corrected momenta break energy or momentum conservation by
 // more than the gate's bounds, or whose correction is implausibly large, is
 // integrated again by plain RK45 from its initial geometry.
@@ -40,8 +41,8 @@ constexpr int kOut = CE_CLOSURE_OUTPUTS;
 constexpr double kMassUnit = 1822.888486209;  // m_e per amu (include/coulomb/units.hpp:11)
 constexpr float kLogMassScale = 1.0f / 3.5f;  // ln(32.06 amu / 1 amu) ~ 3.47
 constexpr int kPerAtom = 12;                  // features per atom
-constexpr float kRelRef = 1e-3f;              // typical RMS residual (units of P)
-constexpr float kRelEps = 2e-5f;              // floor of the relative weighting
+constexpr float kRelRef = 1e-2f;              // typical RMS residual (units of Q)
+constexpr float kRelEps = 1e-4f;              // floor of the relative weighting (units of Q)
 
 struct FeatArgs {
   uint64_t S, S_pad;
@@ -183,9 +184,20 @@ __global__ void __launch_bounds__(128) closure_features_kernel(const FeatArgs A)
         }
       }
     }
+    double q2 = 0.0;
+#pragma unroll
+    for (int i = 0; i < kA; ++i) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const double d = static_cast<double>(dp[i][c]) - p[i][c];
+        q2 += d * d;
+      }
+    }
     const float P = static_cast<float>(sqrt(p2 / n));
+    const float Q = static_cast<float>(sqrt(q2 / n));  // RMS per-atom size of the analytic step p -> p_base
     const float L = static_cast<float>(sqrt(r2 / n));
-    if (bad || !(ke > 0.0) || !isfinite(sc) || !(P > 0.0f) || !isfinite(P) || !(L > 0.0f)) {
+    if (bad || !(ke > 0.0) || !isfinite(sc) || !(P > 0.0f) || !isfinite(P) || !(Q > 0.0f) || !isfinite(Q) ||
+        !(L > 0.0f)) {
       zero_row(A, s);
       for (int c = 0; c < 3 * kA; ++c) A.p_base[s * 3 * kA + c] = 0.0f;
       A.p_scale[s] = __int_as_float(0x7fc00000);  // NaN: the gate sends the sim to plain integration
@@ -197,7 +209,7 @@ __global__ void __launch_bounds__(128) closure_features_kernel(const FeatArgs A)
 #pragma unroll
       for (int c = 0; c < 3; ++c) pb[3 * i + c] = dp[i][c];
     }
-    A.p_scale[s] = P;
+    A.p_scale[s] = Q;
 
     // Features: per atom (x - x_com)/L, p/P, (p_base - p)/P, q/3, ln(m/amu)/3.5,
     // 1; then the remaining PE fraction at the stop and n/10; zeros to the
@@ -228,9 +240,10 @@ __global__ void __launch_bounds__(128) closure_features_kernel(const FeatArgs A)
     for (int c = 0; c < kFeat * 2 / 16; ++c) fo[c] = fi[c];
 
     if (A.target) {
-      // Targets (p_true - p_base)/P; weights w_scale / (3n) scaled by
+      // Targets (p_true - p_base)/Q; weights w_scale / (3n) scaled by
       // kRelRef / sqrt(rms^2 + kRelEps^2), rms = the RMS target of the sim, so
       // the loss weighs each sim's relative rather than absolute residual.
+      const float iQ = 1.0f / Q;
       const float* pt = A.p_true + s * 3 * kA;
       float* t = A.target + s * kOut;
       float* w = A.weight + s * kOut;
@@ -239,7 +252,7 @@ __global__ void __launch_bounds__(128) closure_features_kernel(const FeatArgs A)
       for (int i = 0; i < kA; ++i) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          const float v = i < n ? (pt[3 * i + c] - dp[i][c]) * iP : 0.0f;
+          const float v = i < n ? (pt[3 * i + c] - dp[i][c]) * iQ : 0.0f;
           t[3 * i + c] = v;
           ss += v * v;
         }

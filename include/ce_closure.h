@@ -75,7 +75,8 @@ int ce_umma_gemm_f32(const void* A, int a_mn, const void* B, int b_mn, int M, in
  * ln(m_i / amu)/3.5, 1 (zeros for the padded atoms), then PE_stop/E_0 * 20,
  * n/10 and zeros; L is the RMS distance from the centre of mass, P the RMS
  * atom momentum of the base p_base. It predicts CE_CLOSURE_OUTPUTS values, the
- * first 3n being (p_inf - p_base)/P. */
+ * first 3n being (p_inf - p_base)/Q, Q = RMS over atoms of |p_base,i - p_i|
+ * (the size of the analytic step). */
 #define CE_CLOSURE_FEATURES 128
 #define CE_CLOSURE_OUTPUTS 32
 
@@ -89,11 +90,11 @@ typedef struct ce_closure_state {
   const uint8_t* status;   /* [S] CE_SIM_* of the loose run */
 } ce_closure_state;
 
-/* Bounds a sim's corrected momenta p = p_base + P * out must meet to be
+/* Bounds a sim's corrected momenta p = p_base + Q * out must meet to be
  * accepted (else it is integrated again by plain RK45):
  *   |KE(p)/E_0 - 1|            <= tol_energy      (energy conservation)
  *   |sum_i p_i| / sum_i |p_i|   <= tol_momentum    (momentum conservation)
- *   |P * out| / |p_base|        <= tol_correction  (size of the learned step) */
+ *   |Q * out| / |p_base|        <= tol_correction  (size of the learned step) */
 typedef struct ce_closure_gate {
   float tol_energy;
   float tol_momentum;
@@ -103,11 +104,11 @@ void ce_closure_default_gate(ce_closure_gate* g);
 
 /* Features, ballistic base and (if target != NULL) training targets for S sims
  * (device pointers, async on stream). feats [pad128(S)][128] BF16 (padded rows
- * zeroed); p_base [S][10][3]; p_scale [S] (0 for one-atom or unconverged sims,
- * NaN when the ballistic integral does not exist); target, weight
- * [pad128(S)][32] FP32 with target = (p_true - p_base)/P and, on the 3n live
- * components (zero elsewhere), weight = weight_scale / (3n) * 1e-3 /
- * sqrt(rms^2 + (2e-5)^2) where rms is the sim's RMS target: a relative loss. */
+ * zeroed); p_base [S][10][3]; p_scale [S] = Q (0 for one-atom or unconverged
+ * sims, NaN when the ballistic integral does not exist); target, weight
+ * [pad128(S)][32] FP32 with target = (p_true - p_base)/Q and, on the 3n live
+ * components (zero elsewhere), weight = weight_scale / (3n) * 1e-2 /
+ * sqrt(rms^2 + (1e-4)^2) where rms is the sim's RMS target: a relative loss. */
 int ce_closure_features(uint64_t S, const ce_mixed_batch* in, double coulomb_k, const ce_closure_state* st,
                         const float* p_true, float weight_scale, void* feats, float* p_base, float* p_scale,
                         float* target, float* weight, void* stream);

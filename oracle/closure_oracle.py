@@ -9,7 +9,8 @@ A float64 numpy restatement of include/ce_closure.h for mixed rows of 10 atoms:
   KE = E_0 (the reference's rescale, src/driver.cpp:38-42, applied to the
   ballistic state);
 * features: per atom (x - x_com)/L, p/P, (p_base - p)/P, q/3, ln(m/amu)/3.5,
-  1, then PE_stop/E_0 * 20 and n/10 (BF16-rounded like the device);
+  1, then PE_stop/E_0 * 20 and n/10 (BF16-rounded like the device); the
+  network output is in units of Q, the RMS per-atom size of p_base - p;
 * training targets and the relative loss weights;
 * gate: |KE/E_0 - 1|, |sum p|/sum|p|, |correction|/|base|, then projection
   to zero net momentum (mass weighted) and rescale to E_0.
@@ -34,12 +35,14 @@ def pair_impulse(r, w):
 
 
 def ballistic_base(n, mass, charge, x, p, e0, k=1.0):
-    """(p_base [S,10,3], P [S], L [S], com [S,3]) in float64."""
+    """(p_base [S,10,3], P [S], L [S], com [S,3], Q [S]) in float64; Q is the
+    RMS per-atom size of the analytic step |p_base - p|."""
     S = n.shape[0]
     pb = np.zeros((S, A, 3))
     P = np.zeros(S)
     L = np.zeros(S)
     com = np.zeros((S, 3))
+    Q = np.zeros(S)
     for s in range(S):
         k_ = int(n[s])
         m = mass[s, :k_].astype(np.float64)
@@ -58,15 +61,16 @@ def ballistic_base(n, mass, charge, x, p, e0, k=1.0):
         b2 = b2 * np.sqrt(e0[s] / ke)
         pb[s, :k_] = b2
         P[s] = np.sqrt(np.sum(b2 * b2) / k_)
+        Q[s] = np.sqrt(np.sum((b2 - ps) ** 2) / k_)
         c0 = (m[:, None] * xs).sum(0) / m.sum()
         com[s] = c0
         L[s] = np.sqrt(np.sum((xs - c0) ** 2) / k_)
-    return pb, P, L, com
+    return pb, P, L, com, Q
 
 
 def features(n, mass, charge, x, p, e0, pe_final, k=1.0):
-    """(feats [S,128] float64 of BF16 values, p_base, P)."""
-    pb, P, L, com = ballistic_base(n, mass, charge, x, p, e0, k)
+    """(feats [S,128] float64 of BF16 values, p_base, Q)."""
+    pb, P, L, com, Q = ballistic_base(n, mass, charge, x, p, e0, k)
     S = n.shape[0]
     f = np.zeros((S, 128), np.float32)
     for s in range(S):
@@ -81,25 +85,25 @@ def features(n, mass, charge, x, p, e0, pe_final, k=1.0):
             f[s, o + 11] = 1.0
         f[s, 120] = pe_final[s] / e0[s] * 20.0
         f[s, 121] = k_ * 0.1
-    return to_bf16(f), pb, P
+    return to_bf16(f), pb, Q
 
 
-def targets(n, p_base, P, p_true, weight_scale=1.0):
-    """(target [S,32], weight [S,32]): (p_true - p_base)/P and the relative
-    loss weight weight_scale/(3n) * 1e-3 / sqrt(rms^2 + (2e-5)^2)."""
+def targets(n, p_base, Q, p_true, weight_scale=1.0):
+    """(target [S,32], weight [S,32]): (p_true - p_base)/Q and the relative
+    loss weight weight_scale/(3n) * 1e-2 / sqrt(rms^2 + (1e-4)^2)."""
     S = n.shape[0]
     t = np.zeros((S, 32))
     w = np.zeros((S, 32))
     for s in range(S):
         k_ = int(n[s])
-        v = ((p_true[s, :k_] - p_base[s, :k_]) / P[s]).reshape(-1)
+        v = ((p_true[s, :k_] - p_base[s, :k_]) / Q[s]).reshape(-1)
         t[s, :3 * k_] = v
         rms2 = np.sum(v * v) / (3 * k_)
-        w[s, :3 * k_] = weight_scale / (3 * k_) * 1e-3 / np.sqrt(rms2 + 2e-5 ** 2)
+        w[s, :3 * k_] = weight_scale / (3 * k_) * 1e-2 / np.sqrt(rms2 + 1e-4 ** 2)
     return t, w
 
 
-def apply_gate(n, mass, e0, p_base, P, out, tol_e, tol_p, tol_c):
+def apply_gate(n, mass, e0, p_base, Q, out, tol_e, tol_p, tol_c):
     """(accepted [S] bool, momenta [S,10,3] for accepted sims, rho, mu, corr)."""
     S = n.shape[0]
     acc = np.zeros(S, bool)
@@ -110,7 +114,7 @@ def apply_gate(n, mass, e0, p_base, P, out, tol_e, tol_p, tol_c):
     for s in range(S):
         k_ = int(n[s])
         m = mass[s, :k_]
-        d = P[s] * out[s, :3 * k_].reshape(k_, 3)
+        d = Q[s] * out[s, :3 * k_].reshape(k_, 3)
         pp = p_base[s, :k_] + d
         ke = 0.5 * np.sum(np.sum(pp * pp, 1) / m)
         rho[s] = abs(ke / e0[s] - 1.0)

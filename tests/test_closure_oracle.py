@@ -51,7 +51,7 @@ def test_ballistic_base_conserves_and_converges(wl):
             k = int(n[s])
             x, p, st = ol.run_state(k, m[s, :k], q[s, :k], pos[s, :k], rtol=1e-10, atol=1e-16, pe_stop=pes)
             xs[s, :k], ps[s, :k], e0[s] = x, p, st.e0
-        pb, P, L, _ = co.ballistic_base(n, m, q, xs, ps, e0)
+        pb, P, L, _, Q = co.ballistic_base(n, m, q, xs, ps, e0)
         for s in range(40):
             k = int(n[s])
             assert np.linalg.norm(pb[s, :k].sum(0)) < 2e-5 * np.abs(pb[s, :k]).max()  # f32 loose state

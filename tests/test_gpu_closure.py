@@ -1,8 +1,8 @@
 """Learned closure (include/ce_closure.h) on the GPU.
 
 * features and ballistic base against the float64 oracle
-  (oracle/closure_oracle.py): base and scale within 3e-5 relative (FP32 pair
-  sums), features within one BF16 rounding step;
+  (oracle/closure_oracle.py): base within 3e-5 relative (FP32 pair sums), the
+  output scale Q within 2e-4, features within one BF16 rounding step;
 * gate and projection against the oracle on a random network output;
 * serving: a gate that accepts nothing reproduces plain RK45 bit for bit, a
   gate that accepts everything leaves no sim behind, one-atom and invalid
@@ -57,9 +57,9 @@ def test_features_match_oracle(ce, engine, cl):
     n, m, q = _np(b.n)[ok], _np(b.mass)[ok], _np(b.charge)[ok]
     x, p = _np(loose["positions"])[ok], _np(loose["momenta"])[ok]
     e0, pef = _np(loose["e0"])[ok], _np(loose["pe_final"])[ok]
-    f_ref, pb_ref, P_ref = co.features(n, m, q, x, p, e0, pef)
-    P = _np(d["p_scale"])[ok]
-    np.testing.assert_allclose(P, P_ref, rtol=3e-5)
+    f_ref, pb_ref, Q_ref = co.features(n, m, q, x, p, e0, pef)
+    Q = _np(d["p_scale"])[ok]
+    np.testing.assert_allclose(Q, Q_ref, rtol=2e-4)
     pb = _np(d["p_base"])[ok]
     err = np.linalg.norm((pb - pb_ref).reshape(len(n), -1), axis=1) / np.linalg.norm(pb_ref.reshape(len(n), -1), axis=1)
     assert err.max() < 3e-5
@@ -69,10 +69,11 @@ def test_features_match_oracle(ce, engine, cl):
     # padded rows of the feature matrix are zero
     assert float(d["feats"][600:].float().abs().sum()) == 0.0
     # training targets and relative weights (targets inherit the FP32 base error)
-    t_ref, w_ref = co.targets(n, pb_ref, P_ref, _np(plain["momenta"])[ok].astype(np.float64), 0.5)
+    t_ref, w_ref = co.targets(n, pb_ref, Q_ref, _np(plain["momenta"])[ok].astype(np.float64), 0.5)
     t = _np(d["target"])[:600][ok]
     w = _np(d["weight"])[:600][ok]
-    assert np.abs(t - t_ref).max() < 1e-4
+    P_ref = np.sqrt((pb_ref ** 2).sum(axis=(1, 2)) / n)
+    assert np.all(np.abs(t - t_ref).max(axis=1) < 3e-5 * P_ref / Q_ref)
     np.testing.assert_allclose(w, w_ref, rtol=0.15, atol=0)
     assert float(d["weight"][600:].abs().sum()) == 0.0
     # loose stop: remaining PE at most 5% (and not far below) of PE_0
@@ -88,7 +89,10 @@ def test_gate_and_projection_match_oracle(ce, engine, cl):
     d = cl.features(b, loose)
     g = torch.Generator(device="cuda")
     g.manual_seed(3)
-    out = torch.randn((512, 32), generator=g, device="cuda") * 2e-3
+    # corrections of ~2e-3 of the base momenta (the output is in units of Q)
+    P = torch.sqrt((d["p_base"].double() ** 2).sum(dim=(1, 2)) / b.n.double().clamp(min=1))
+    ratio = torch.nan_to_num(P / d["p_scale"].double(), nan=0.0, posinf=0.0).float()
+    out = torch.randn((512, 32), generator=g, device="cuda") * 2e-3 * ratio[:, None]
     out[::2] *= 0.1  # even rows pass the bounds below, odd rows mostly fail them
     gate = ce.CeClosureGate(1e-3, 1e-3, 3e-3)
     mom = torch.full((512, 10, 3), -7.0, device="cuda")
