@@ -883,7 +883,8 @@ def main():
                     help="ch4 (the headline workload), c2h6 (10-atom C2H6-like), h2o (stiff H2O)")
     ap.add_argument("--cpu-budget", type=float, default=8.0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="fixed", choices=["fixed", "mixed", "precision", "closure", "network", "stream"],
+    ap.add_argument("--workload", default="fixed",
+                    choices=["fixed", "mixed", "precision", "closure", "network", "stream"],
                     help="fixed: one molecule (--molecule); mixed: 2..10-atom population, one launch vs per size; "
                          "closure: learned closure vs plain RK45 on the mixed population; network: the closure "
                          "network's fused forward alone; stream: 1e8 C2H6-like explosions streamed in 1e6 chunks, "
@@ -1057,13 +1058,15 @@ def main():
                    "sample": f"{r_all[1]} CH4 sims of the step on {r_all[2]} threads (reference scalar f32 engine)",
                    "single_core_value": r_one[0] if r_one else None}
 
+    # DRAM traffic of one integration launch, from the committed ncu summary of
+    # this workload (dram__bytes_read.sum + dram__bytes_write.sum).
     traffic = None
-    tp = ROOT / "profiles" / "traffic_rk45_fixed_ch4.json"
-    if tp.exists():
-        try:
-            traffic = json.loads(tp.read_text()).get("bytes_per_launch_full")
-        except Exception:
-            traffic = None
+    tp = ROOT / "profiles" / f"rk45_atom_{args.molecule}_1e6.md"
+    if tp.exists() and S == S_DEFAULT and args.molecule == "ch4":
+        import re
+
+        m = re.search(r"traffic_bytes_per_launch:\s*([0-9]+)", tp.read_text())
+        traffic = int(m.group(1)) if m else None
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -260,14 +260,14 @@ __global__ void f32_to_bf16_kernel(const float* a, bf16* b, int n) {
 //   warp 1  MMA issuer: one thread runs the (layer, tile) jobs in the order
 //           A0 B0 A1 B1 ..., each job's slices into its tile's accumulator
 //           (two 128 x 256 FP32 blocks, 512 TMEM columns);
-//   warps 4-7 / 8-11  epilogue of tile A / tile B: TMEM -> bias + SiLU ->
+//   warps 2-9 / 10-17  epilogue of tile A / tile B: TMEM -> bias + SiLU ->
 //           BF16 -> the tile's activation operand in shared memory (the input
 //           of the next layer), or FP32 outputs after the last layer; they also
 //           load the next input tile.
 // So tile A's epilogue of layer l overlaps tile B's MMAs of layer l and vice
 // versa; activations never leave shared memory. All waits are bounded.
 constexpr int kFwdMaxLayers = 8;
-constexpr int kFwdThreads = 384;               // 12 warps
+constexpr int kFwdThreads = 576;               // 18 warps: producer, MMA issuer, 2 x 8 epilogue
 constexpr int kFwdKmax = 256;                  // widest layer input held in shared memory
 constexpr int kFwdSboA = (kFwdKmax / 8) * 128; // 4096 B between row-adjacent core matrices
 constexpr int kFwdAct = kTM * kFwdKmax * 2;    // 64 KB activation operand per tile
@@ -355,7 +355,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) mlp_forward_fused_kernel(const
   uint64_t* full = bars;              // [3] slice landed
   uint64_t* empty = bars + 3;         // [3] slice consumed by the tensor core
   uint64_t* acc_full = bars + 6;      // [2] tile's layer accumulated
-  uint64_t* act_ready = bars + 8;     // [2] tile's layer input written (128 arrivals)
+  uint64_t* act_ready = bars + 8;     // [2] tile's layer input written (256 arrivals)
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 10);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 11);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -368,7 +368,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) mlp_forward_fused_kernel(const
     }
     for (int t = 0; t < 2; ++t) {
       umma::mbar_init(&acc_full[t], 1);
-      umma::mbar_init(&act_ready[t], kTM);
+      umma::mbar_init(&act_ready[t], 2 * kTM);  // the tile's 8 epilogue warps
     }
     *abort_flag = 0;
   }
@@ -438,15 +438,16 @@ __global__ void __launch_bounds__(kFwdThreads, 1) mlp_forward_fused_kernel(const
         }
       }
     }
-  } else if (warp >= 4) {
-    // ---- epilogue warpgroups ----
-    const int t = (warp - 4) >> 2, quarter = warp & 3;
+  } else {
+    // ---- epilogue: warps 2-9 tile A, 10-17 tile B; each warp one lane quarter
+    // (warp % 4, the TMEM lanes it may read) and one half of the columns ----
+    const int ew = warp - 2, t = ew >> 3, half = (ew & 7) >> 2, quarter = warp & 3;
     const int row = quarter * 32 + lane;
     const uint32_t tbase = tmem + (static_cast<uint32_t>(quarter * 32) << 16) + t * kTNmax;
     const int G = A.fan_in[0] / 8;
     auto load_x = [&](int pair) {
       const int m0 = (2 * pair + t) * kTM;
-      for (int i = row; i < kTM * G; i += kTM) {
+      for (int i = half * kTM + row; i < kTM * G; i += 2 * kTM) {
         const int r = i / G, g = i - r * G;
         cp_async16(act[t] + (r >> 3) * kFwdSboA + g * kLBO + (r & 7) * 16,
                    A.x + static_cast<size_t>(m0 + r) * A.fan_in[0] + g * 8);
@@ -466,36 +467,38 @@ __global__ void __launch_bounds__(kFwdThreads, 1) mlp_forward_fused_kernel(const
       if (t >= tiles_of(pair)) break;
       const int m0 = (2 * pair + t) * kTM;
       for (int l = 0; l < A.layers && ok; ++l) {
+        const int N = A.fan_out[l], cols = N / 2, cbeg = half * cols;
+        const float* bias = A.p + A.b_off[l];
+        const bool last = l + 1 == A.layers;
+        // this warp's first 16 biases, one per lane, fetched before the wait
+        float bnext = lane < 16 ? __ldg(bias + cbeg + lane) : 0.0f;
         if (!(ok = wait(&acc_full[t], ph_acc))) break;
         ph_acc ^= 1u;
         umma::tc_fence_after();
-        const int N = A.fan_out[l];
-        const float* bias = A.p + A.b_off[l];
-        const bool last = l + 1 == A.layers;
-        for (int c0 = 0; c0 < N; c0 += 32) {
-          uint32_t r[32];
-          umma::tmem_ld16(tbase + static_cast<uint32_t>(c0), *reinterpret_cast<uint32_t(*)[16]>(r));
-          umma::tmem_ld16(tbase + static_cast<uint32_t>(c0 + 16), *reinterpret_cast<uint32_t(*)[16]>(r + 16));
+        for (int c0 = cbeg; c0 < cbeg + cols; c0 += 16) {
+          uint32_t r[16];
+          umma::tmem_ld16(tbase + static_cast<uint32_t>(c0), r);
+          const float bl = bnext;  // lane j holds bias[c0 + j]
+          if (c0 + 16 < cbeg + cols) bnext = lane < 16 ? __ldg(bias + c0 + 16 + lane) : 0.0f;
           umma::tmem_wait_ld();
+          float b[16];
+#pragma unroll
+          for (int j = 0; j < 16; ++j) b[j] = __shfl_sync(0xffffffffu, bl, j);
           if (!last) {
-            uint32_t y[16];
+            uint32_t y[8];
 #pragma unroll
-            for (int j = 0; j < 32; j += 2)
-              y[j / 2] = silu_pair(__uint_as_float(r[j]) + __ldg(bias + c0 + j),
-                                   __uint_as_float(r[j + 1]) + __ldg(bias + c0 + j + 1), nullptr);
+            for (int j = 0; j < 16; j += 2)
+              y[j / 2] = silu_pair(__uint_as_float(r[j]) + b[j], __uint_as_float(r[j + 1]) + b[j + 1], nullptr);
             uint8_t* dst = act[t] + (row >> 3) * kFwdSboA + (c0 / 8) * kLBO + (row & 7) * 16;
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-              *reinterpret_cast<uint4*>(dst + q * kLBO) = make_uint4(y[4 * q], y[4 * q + 1], y[4 * q + 2], y[4 * q + 3]);
+            *reinterpret_cast<uint4*>(dst) = make_uint4(y[0], y[1], y[2], y[3]);
+            *reinterpret_cast<uint4*>(dst + kLBO) = make_uint4(y[4], y[5], y[6], y[7]);
           } else {
             float* o = A.out + static_cast<size_t>(m0 + row) * N + c0;
 #pragma unroll
-            for (int j = 0; j < 32; j += 4)
-              if (c0 + j < N)
-                *reinterpret_cast<float4*>(o + j) = make_float4(
-                    __uint_as_float(r[j]) + __ldg(bias + c0 + j), __uint_as_float(r[j + 1]) + __ldg(bias + c0 + j + 1),
-                    __uint_as_float(r[j + 2]) + __ldg(bias + c0 + j + 2),
-                    __uint_as_float(r[j + 3]) + __ldg(bias + c0 + j + 3));
+            for (int j = 0; j < 16; j += 4)
+              *reinterpret_cast<float4*>(o + j) =
+                  make_float4(__uint_as_float(r[j]) + b[j], __uint_as_float(r[j + 1]) + b[j + 1],
+                              __uint_as_float(r[j + 2]) + b[j + 2], __uint_as_float(r[j + 3]) + b[j + 3]);
           }
         }
         umma::tc_fence_before();
