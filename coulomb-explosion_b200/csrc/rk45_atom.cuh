@@ -9,10 +9,10 @@
 //
 // Per force evaluation a lane publishes (x, y, z) to its slot of a per-warp
 // shared-memory buffer (three rotating buffers, one __syncwarp per evaluation)
-// and reads its N-1 partners with 16-byte loads; the partner set is fixed per
-// lane, so there is no self pair, and the lane's pair constants k q_i q_j sit in
-// registers. The pair term is computed on both sides instead of using Newton's
-// third law. Sums over a simulation (error norm, potential, kinetic energy,
+// and reads its partners with 16-byte loads; the partner set is fixed per lane,
+// so there is no self pair, and the lane's pair constants k q_i q_j sit in
+// registers. Each pair term is evaluated by one lane of the pair and handed to
+// the other with shuffles (Newton's third law, see lane_force). Sums over a simulation (error norm, potential, kinetic energy,
 // Hairer norms) are gathered with N shuffles in a fixed order, so every lane of
 // a group holds the bit-identical value and takes the same accept/reject and
 // stop decisions.
@@ -95,22 +95,33 @@ struct AtomLane {
   unsigned long long sim;
 };
 
-// One force evaluation for every lane of the warp: publish xs, read the N-1
-// partners, accumulate a_i and (optionally) this lane's half of the pair
-// potential. `which` (0..2) selects one of three 32-slot buffers; consecutive
-// calls always use different buffers, so a lane never overwrites a slot that a
-// slower lane is still reading from the previous evaluation.
+// One force evaluation for every lane of the warp: publish xs, read partners,
+// accumulate a_i and (optionally) this lane's share of the potential. `which`
+// (0..2) selects one of three 32-slot buffers; consecutive calls always use
+// different buffers, so a lane never overwrites a slot that a slower lane is
+// still reading from the previous evaluation.
+//
+// Newton's third law across lanes: partner d of lane i is atom i+1+d (mod N).
+// Lane i evaluates the pair terms f_d = k q_i q_j r / |r|^3 (r = x_i - x_j) for
+// d < H = (N-1)/2 only, adds them to its own acceleration, and receives -f from
+// the lane that evaluated its pair as that lane's d-th term (lane i-1-d) with
+// one shuffle per component. For even N the opposite atom (d = N/2 - 1) pairs
+// two lanes symmetrically; both evaluate it, each taking half of its potential.
+// Every pair's potential is counted once: the group sum of pe_part is PE.
 template <int N, typename Acc>
 __device__ __forceinline__ void lane_force(float4* __restrict__ buf, int which, int slot, const int (&nbr)[N - 1],
-                                           const float (&pcv)[N - 1], const float (&xs)[3], const AtomConsts& ac,
-                                           bool want_pe, float (&a)[3], Acc& pe_half) {
+                                           const int (&recv)[N - 1], const float (&pcv)[N - 1], const float (&xs)[3],
+                                           const AtomConsts& ac, bool want_pe, float (&a)[3], Acc& pe_part) {
+  constexpr int H = (N - 1) / 2;
+  constexpr bool kOpp = (N % 2) == 0;
   float4* b = buf + which * 32;
   b[slot] = make_float4(xs[0], xs[1], xs[2], 0.0f);
   __syncwarp();
   float ax = 0.0f, ay = 0.0f, az = 0.0f;
+  float fx[H > 0 ? H : 1], fy[H > 0 ? H : 1], fz[H > 0 ? H : 1];
   Acc pe = Acc(0);
 #pragma unroll
-  for (int d = 0; d < N - 1; ++d) {
+  for (int d = 0; d < H; ++d) {
     const float4 o = b[nbr[d]];
     const float rx = xs[0] - o.x;
     const float ry = xs[1] - o.y;
@@ -119,15 +130,39 @@ __device__ __forceinline__ void lane_force(float4* __restrict__ buf, int which, 
     const float rinv = rsqrtf(d2);
     const float u = pcv[d] * rinv;  // k q_i q_j / r
     if (want_pe) pe += static_cast<Acc>(u);
-    const float s = u * (rinv * rinv);
-    ax = fmaf(rx, s, ax);
-    ay = fmaf(ry, s, ay);
-    az = fmaf(rz, s, az);
+    const float sc = u * (rinv * rinv);
+    fx[d] = rx * sc;
+    fy[d] = ry * sc;
+    fz[d] = rz * sc;
+    ax += fx[d];
+    ay += fy[d];
+    az += fz[d];
+  }
+  if (kOpp) {
+    constexpr int d = N / 2 - 1;
+    const float4 o = b[nbr[d]];
+    const float rx = xs[0] - o.x;
+    const float ry = xs[1] - o.y;
+    const float rz = xs[2] - o.z;
+    const float d2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+    const float rinv = rsqrtf(d2);
+    const float u = pcv[d] * rinv;
+    if (want_pe) pe += static_cast<Acc>(0.5f * u);
+    const float sc = u * (rinv * rinv);
+    ax = fmaf(rx, sc, ax);
+    ay = fmaf(ry, sc, ay);
+    az = fmaf(rz, sc, az);
+  }
+#pragma unroll
+  for (int d = 0; d < H; ++d) {
+    ax -= __shfl_sync(0xffffffffu, fx[d], recv[d]);
+    ay -= __shfl_sync(0xffffffffu, fy[d], recv[d]);
+    az -= __shfl_sync(0xffffffffu, fz[d], recv[d]);
   }
   a[0] = ax * ac.inv_m;
   a[1] = ay * ac.inv_m;
   a[2] = az * ac.inv_m;
-  pe_half = pe;
+  pe_part = pe;
 }
 
 // FP64 finalize, executed by every lane of the warp (the reductions are full-warp
@@ -187,6 +222,7 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
   const int base = has_atom ? g * N : lane;
   const bool leader = has_atom && ai == 0;
   int nbr[N - 1];
+  int recv[N - 1];  // lane that evaluates this lane's pair as its d-th term
   int pidx[N - 1];  // partner atom index j for each d
 #pragma unroll
   for (int d = 0; d < N - 1; ++d) {
@@ -194,6 +230,9 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
     if (j >= N) j -= N;
     pidx[d] = j;
     nbr[d] = has_atom ? base + j : lane;
+    int r = ai - 1 - d;
+    if (r < 0) r += N;
+    recv[d] = has_atom ? base + r : lane;
   }
   AtomConsts ac;
   float pcv[N - 1];
@@ -276,8 +315,8 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
       }
       float a0[3];
       Acc peh;
-      lane_force<N, Acc>(buf, 2, lane, nbr, pcv, s.x, ac, true, a0, peh);  // stages use buffers 1, 0, 1, ...
-      const Acc pe0 = gsum<N>(peh, base) * Acc(0.5);
+      lane_force<N, Acc>(buf, 2, lane, nbr, recv, pcv, s.x, ac, true, a0, peh);  // stages use buffers 1, 0, 1, ...
+      const Acc pe0 = gsum<N>(peh, base);
       // Hairer norms from rest (sv = atol, probe accelerations = k1).
       float d0p = 0.0f, d1p = 0.0f;
 #pragma unroll
@@ -353,7 +392,7 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
           xs[c] = s.x[c] + inc;
         }
       }
-      lane_force<N, Acc>(buf, si & 1, lane, nbr, pcv, xs, ac, si == 6, a, pe_half);
+      lane_force<N, Acc>(buf, si & 1, lane, nbr, recv, pcv, xs, ac, si == 6, a, pe_half);
       if (si <= 5) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) s.k[si][c] = a[c];
@@ -389,7 +428,7 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
       errp = fmaf(rv, rv, errp);
     }
     const float err_sq = gsum<N>(errp, base);
-    const Acc pe_new = gsum<N>(pe_half, base) * Acc(0.5);
+    const Acc pe_new = gsum<N>(pe_half, base);
     int fin_st = -1;
     if (active) {
       const float en = sqrtf(err_sq * (1.0f / static_cast<float>(6 * N)));
