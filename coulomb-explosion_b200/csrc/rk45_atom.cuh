@@ -80,14 +80,36 @@ __device__ __forceinline__ T gsum(T v, int base) {
   return s;
 }
 
+// A lane's 3-vector as an (x, y) pair plus z, so component-wise arithmetic
+// runs on the packed FP32x2 instructions (one FFMA2 / FADD2 / FMUL2 for x and
+// y). Every packed operation rounds each element exactly like its scalar
+// counterpart (a - b is evaluated as fma(-1, b, a), which is exact), so the
+// results equal the scalar formulation bit for bit.
+struct V3 {
+  float2 xy;
+  float z;
+  __device__ __forceinline__ float get(int c) const { return c == 0 ? xy.x : (c == 1 ? xy.y : z); }
+};
+__device__ __forceinline__ float2 bcast(float s) { return make_float2(s, s); }
+__device__ __forceinline__ V3 v3_zero() { return {make_float2(0.0f, 0.0f), 0.0f}; }
+// s * a + c
+__device__ __forceinline__ V3 v3_fma(float s, const V3& a, const V3& c) {
+  return {__ffma2_rn(bcast(s), a.xy, c.xy), fmaf(s, a.z, c.z)};
+}
+__device__ __forceinline__ V3 v3_mul(float s, const V3& a) { return {__fmul2_rn(bcast(s), a.xy), s * a.z}; }
+__device__ __forceinline__ V3 v3_add(const V3& a, const V3& b) { return {__fadd2_rn(a.xy, b.xy), a.z + b.z}; }
+__device__ __forceinline__ V3 v3_sub(const V3& a, const V3& b) {
+  return {__ffma2_rn(bcast(-1.0f), b.xy, a.xy), a.z - b.z};
+}
+
 template <int N, int MODE>
 struct AtomLane {
   static constexpr bool kKahan = (MODE & CE_PREC_KAHAN) != 0;
   static constexpr bool kF64 = (MODE & CE_PREC_FP64) != 0;
   using Acc = typename std::conditional<kF64, double, float>::type;
-  float x[3], v[3];
-  float k[6][3];
-  float cx[3], cv[3];
+  V3 x, v;
+  V3 k[6];
+  V3 cx, cv;
   float h;
   Acc t, e0, pe_stop;
   uint32_t steps, rejects, rej_in_step;
@@ -110,58 +132,55 @@ struct AtomLane {
 // Every pair's potential is counted once: the group sum of pe_part is PE.
 template <int N, typename Acc>
 __device__ __forceinline__ void lane_force(float4* __restrict__ buf, int which, int slot, const int (&nbr)[N - 1],
-                                           const int (&recv)[N - 1], const float (&pcv)[N - 1], const float (&xs)[3],
-                                           const AtomConsts& ac, bool want_pe, float (&a)[3], Acc& pe_part) {
+                                           const int (&recv)[N - 1], const float (&pcv)[N - 1], const V3& xs,
+                                           const AtomConsts& ac, bool want_pe, V3& a, Acc& pe_part) {
   constexpr int H = (N - 1) / 2;
   constexpr bool kOpp = (N % 2) == 0;
   float4* b = buf + which * 32;
-  b[slot] = make_float4(xs[0], xs[1], xs[2], 0.0f);
+  b[slot] = make_float4(xs.xy.x, xs.xy.y, xs.z, 0.0f);
   __syncwarp();
-  float ax = 0.0f, ay = 0.0f, az = 0.0f;
-  float fx[H > 0 ? H : 1], fy[H > 0 ? H : 1], fz[H > 0 ? H : 1];
+  float2 axy = make_float2(0.0f, 0.0f);
+  float az = 0.0f;
+  float2 fxy[H > 0 ? H : 1];
+  float fz[H > 0 ? H : 1];
   Acc pe = Acc(0);
 #pragma unroll
   for (int d = 0; d < H; ++d) {
     const float4 o = b[nbr[d]];
-    const float rx = xs[0] - o.x;
-    const float ry = xs[1] - o.y;
-    const float rz = xs[2] - o.z;
-    const float d2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+    const float2 rxy = __ffma2_rn(bcast(-1.0f), make_float2(o.x, o.y), xs.xy);
+    const float rz = xs.z - o.z;
+    const float d2 = fmaf(rxy.x, rxy.x, fmaf(rxy.y, rxy.y, rz * rz));
     const float rinv = rsqrtf(d2);
     const float u = pcv[d] * rinv;  // k q_i q_j / r
     if (want_pe) pe += static_cast<Acc>(u);
     const float sc = u * (rinv * rinv);
-    fx[d] = rx * sc;
-    fy[d] = ry * sc;
+    fxy[d] = __fmul2_rn(rxy, bcast(sc));
     fz[d] = rz * sc;
-    ax += fx[d];
-    ay += fy[d];
+    axy = __fadd2_rn(axy, fxy[d]);
     az += fz[d];
   }
   if (kOpp) {
     constexpr int d = N / 2 - 1;
     const float4 o = b[nbr[d]];
-    const float rx = xs[0] - o.x;
-    const float ry = xs[1] - o.y;
-    const float rz = xs[2] - o.z;
-    const float d2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+    const float2 rxy = __ffma2_rn(bcast(-1.0f), make_float2(o.x, o.y), xs.xy);
+    const float rz = xs.z - o.z;
+    const float d2 = fmaf(rxy.x, rxy.x, fmaf(rxy.y, rxy.y, rz * rz));
     const float rinv = rsqrtf(d2);
     const float u = pcv[d] * rinv;
     if (want_pe) pe += static_cast<Acc>(0.5f * u);
     const float sc = u * (rinv * rinv);
-    ax = fmaf(rx, sc, ax);
-    ay = fmaf(ry, sc, ay);
+    axy = __ffma2_rn(rxy, bcast(sc), axy);
     az = fmaf(rz, sc, az);
   }
 #pragma unroll
   for (int d = 0; d < H; ++d) {
-    ax -= __shfl_sync(0xffffffffu, fx[d], recv[d]);
-    ay -= __shfl_sync(0xffffffffu, fy[d], recv[d]);
+    const float gx = __shfl_sync(0xffffffffu, fxy[d].x, recv[d]);
+    const float gy = __shfl_sync(0xffffffffu, fxy[d].y, recv[d]);
+    axy = __ffma2_rn(bcast(-1.0f), make_float2(gx, gy), axy);
     az -= __shfl_sync(0xffffffffu, fz[d], recv[d]);
   }
-  a[0] = ax * ac.inv_m;
-  a[1] = ay * ac.inv_m;
-  a[2] = az * ac.inv_m;
+  a.xy = __fmul2_rn(axy, bcast(ac.inv_m));
+  a.z = az * ac.inv_m;
   pe_part = pe;
 }
 
@@ -171,7 +190,7 @@ __device__ __forceinline__ void lane_force(float4* __restrict__ buf, int which, 
 template <int N, int MODE, int STRIDE>
 __device__ __forceinline__ void atom_finalize(const AtomLane<N, MODE>& s, int status, double pe_final,
                                               const AtomConsts& ac, int ai, int base, const RunParams& P) {
-  const double vx = s.v[0], vy = s.v[1], vz = s.v[2];
+  const double vx = s.v.xy.x, vy = s.v.xy.y, vz = s.v.z;
   const double ke = gsum<N>(0.5 * ac.mass * (vx * vx + vy * vy + vz * vz), base);
   const int fin = gsum<N>((isfinite(vx) && isfinite(vy) && isfinite(vz)) ? 0 : 1, base);
   if (status == CE_SIM_OK && fin != 0) status = CE_SIM_NONFINITE;
@@ -186,9 +205,9 @@ __device__ __forceinline__ void atom_finalize(const AtomLane<N, MODE>& s, int st
   dst[2] = static_cast<float>(pz);
   if (P.positions) {
     float* xp = P.positions + s.sim * (3ull * STRIDE) + 3 * ai;
-    xp[0] = s.x[0];
-    xp[1] = s.x[1];
-    xp[2] = s.x[2];
+    xp[0] = s.x.xy.x;
+    xp[1] = s.x.xy.y;
+    xp[2] = s.x.z;
   }
   if (ai == 0 && P.e0) P.e0[s.sim] = static_cast<double>(s.e0);
   if (ai == 0) {
@@ -248,12 +267,9 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
     for (int d = 0; d < N - 1; ++d) pcv[d] = 0.0f;
   }
   L s;
+  s.x = s.v = s.cx = s.cv = v3_zero();
 #pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    s.x[c] = s.v[c] = s.cx[c] = s.cv[c] = 0.0f;
-#pragma unroll
-    for (int l = 0; l < 6; ++l) s.k[l][c] = 0.0f;
-  }
+  for (int l = 0; l < 6; ++l) s.k[l] = v3_zero();
   s.h = 0.0f;
   s.t = s.e0 = s.pe_stop = Acc(0);
   s.steps = s.rejects = s.rej_in_step = 0u;
@@ -288,12 +304,8 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
       int fin_st = -1;
       if (fresh) {
         const float* src = P.pos + s.sim * (3ull * STRIDE) + 3 * ai;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          s.x[c] = __ldg(src + c);
-          s.v[c] = 0.0f;
-          s.cx[c] = s.cv[c] = 0.0f;
-        }
+        s.x = {make_float2(__ldg(src), __ldg(src + 1)), __ldg(src + 2)};
+        s.v = s.cx = s.cv = v3_zero();
       }
       if (MIXED) {
         // This sim's constants: pair constants (k q_i) q_j formed in double and
@@ -313,7 +325,7 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
           ac.inv_m = static_cast<float>(1.0 / mi);
         }
       }
-      float a0[3];
+      V3 a0;
       Acc peh;
       lane_force<N, Acc>(buf, 2, lane, nbr, recv, pcv, s.x, ac, true, a0, peh);  // stages use buffers 1, 0, 1, ...
       const Acc pe0 = gsum<N>(peh, base);
@@ -321,9 +333,9 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
       float d0p = 0.0f, d1p = 0.0f;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const float sx = P.atol + P.rtol * fabsf(s.x[c]);
-        const float r0 = s.x[c] / sx;
-        const float r1 = a0[c] / P.atol;
+        const float sx = P.atol + P.rtol * fabsf(s.x.get(c));
+        const float r0 = s.x.get(c) / sx;
+        const float r1 = a0.get(c) / P.atol;
         d0p += r0 * r0;
         d1p += r1 * r1;
       }
@@ -334,14 +346,13 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
       float d2p = 0.0f;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const float sx = P.atol + P.rtol * fabsf(s.x[c]);
-        const float r = (a0[c] * h0) / sx;
+        const float sx = P.atol + P.rtol * fabsf(s.x.get(c));
+        const float r = (a0.get(c) * h0) / sx;
         d2p += r * r;
       }
       const float d2 = sqrtf(gsum<N>(d2p, base) / denom) / h0;
       if (fresh) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) s.k[0][c] = a0[c];
+        s.k[0] = a0;
         const float h1 = (static_cast<double>(d1) <= 1e-15 && static_cast<double>(d2) <= 1e-15)
                              ? fmaxf(1e-6f, h0 * 1e-3f)
                              : powf(0.01f / fmaxf(d1, d2), 0.2f);
@@ -373,57 +384,51 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
 
     // ---- one DP5(4) attempt, all lanes ----
     const float hh = (P.max_dt < s.h) ? P.max_dt : s.h;
-    float xs[3], a[3];
-    float cxn[3] = {0.0f, 0.0f, 0.0f};
+    V3 xs, a;
+    V3 cxn = v3_zero();
     Acc pe_half = Acc(0);
 #pragma unroll
     for (int si = 1; si <= 6; ++si) {
+      V3 sum = v3_zero();
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        float sum = 0.0f;
-#pragma unroll
-        for (int l = 0; l + 1 < si; ++l) sum = fmaf(c_abar[si + 1][l + 1], s.k[l][c], sum);
-        const float inc = hh * fmaf(hh, sum, c_c[si + 1] * s.v[c]);
-        if (L::kKahan && si == 6) {
-          const float y = inc - s.cx[c];
-          xs[c] = s.x[c] + y;
-          cxn[c] = (xs[c] - s.x[c]) - y;
-        } else {
-          xs[c] = s.x[c] + inc;
-        }
+      for (int l = 0; l + 1 < si; ++l) sum = v3_fma(c_abar[si + 1][l + 1], s.k[l], sum);
+      const V3 inc = v3_mul(hh, v3_fma(hh, sum, v3_mul(c_c[si + 1], s.v)));
+      if (L::kKahan && si == 6) {
+        const V3 y = v3_sub(inc, s.cx);
+        xs = v3_add(s.x, y);
+        cxn = v3_sub(v3_sub(xs, s.x), y);
+      } else {
+        xs = v3_add(s.x, inc);
       }
       lane_force<N, Acc>(buf, si & 1, lane, nbr, recv, pcv, xs, ac, si == 6, a, pe_half);
-      if (si <= 5) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) s.k[si][c] = a[c];
-      }
+      if (si <= 5) s.k[si] = a;
     }
     // Stage 7 done: xs = x_new, a = k7. Velocity update and error estimate.
-    float vn[3], cvn[3] = {0.0f, 0.0f, 0.0f};
+    V3 sv = v3_zero(), se = v3_zero(), sev = v3_zero();
+#pragma unroll
+    for (int l = 0; l < 6; ++l) {
+      if (l != 1) sv = v3_fma(c_b[l + 1], s.k[l], sv);
+      se = v3_fma(c_ebar[l + 1], s.k[l], se);
+      if (l != 1) sev = v3_fma(c_e[l + 1], s.k[l], sev);
+    }
+    const V3 incv = v3_mul(hh, sv);
+    V3 vn, cvn = v3_zero();
+    if (L::kKahan) {
+      const V3 y = v3_sub(incv, s.cv);
+      vn = v3_add(s.v, y);
+      cvn = v3_sub(v3_sub(vn, s.v), y);
+    } else {
+      vn = v3_add(s.v, incv);
+    }
+    const V3 ex = v3_mul(hh * hh, se);
+    const V3 ev = v3_mul(hh, v3_fma(c_e[7], a, sev));
     float errp = 0.0f;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      float sv = 0.0f, se = 0.0f, sev = 0.0f;
-#pragma unroll
-      for (int l = 0; l < 6; ++l) {
-        if (l != 1) sv = fmaf(c_b[l + 1], s.k[l][c], sv);
-        se = fmaf(c_ebar[l + 1], s.k[l][c], se);
-        if (l != 1) sev = fmaf(c_e[l + 1], s.k[l][c], sev);
-      }
-      const float incv = hh * sv;
-      if (L::kKahan) {
-        const float y = incv - s.cv[c];
-        vn[c] = s.v[c] + y;
-        cvn[c] = (vn[c] - s.v[c]) - y;
-      } else {
-        vn[c] = s.v[c] + incv;
-      }
-      const float ex = (hh * hh) * se;
-      const float ev = hh * fmaf(c_e[7], a[c], sev);
-      const float scx = fmaf(P.rtol, fmaxf(fabsf(s.x[c]), fabsf(xs[c])), P.atol);
-      const float scv = fmaf(P.rtol, fmaxf(fabsf(s.v[c]), fabsf(vn[c])), P.atol);
-      const float rx = __fdividef(ex, scx);
-      const float rv = __fdividef(ev, scv);
+      const float scx = fmaf(P.rtol, fmaxf(fabsf(s.x.get(c)), fabsf(xs.get(c))), P.atol);
+      const float scv = fmaf(P.rtol, fmaxf(fabsf(s.v.get(c)), fabsf(vn.get(c))), P.atol);
+      const float rx = __fdividef(ex.get(c), scx);
+      const float rv = __fdividef(ev.get(c), scv);
       errp = fmaf(rx, rx, errp);
       errp = fmaf(rv, rv, errp);
     }
@@ -433,15 +438,12 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
     if (active) {
       const float en = sqrtf(err_sq * (1.0f / static_cast<float>(6 * N)));
       if (en <= 1.0f) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          s.x[c] = xs[c];
-          s.v[c] = vn[c];
-          s.k[0][c] = a[c];
-          if (L::kKahan) {
-            s.cx[c] = cxn[c];
-            s.cv[c] = cvn[c];
-          }
+        s.x = xs;
+        s.v = vn;
+        s.k[0] = a;
+        if (L::kKahan) {
+          s.cx = cxn;
+          s.cv = cvn;
         }
         float factor = (en == 0.0f) ? kMaxFactor : fminf(kMaxFactor, kSafety * __powf(en, kExponent));
         if (s.rej_once) factor = fminf(factor, 1.0f);
