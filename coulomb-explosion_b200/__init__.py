@@ -128,6 +128,10 @@ _SIGNATURES = {
         [C.c_void_p, C.c_uint64, C.c_void_p, C.POINTER(CeRunConfig), C.POINTER(CeOutputs), C.c_void_p],
         C.c_int,
     ),
+    "ce_run_verlet_device": (
+        [C.c_void_p, C.c_uint64, C.c_void_p, C.POINTER(CeRunConfig), C.POINTER(CeOutputs), C.c_void_p],
+        C.c_int,
+    ),
     "ce_last_launch_count": ([C.c_void_p], C.c_int),
     "ce_probe_fp32_peak": ([C.c_int, C.POINTER(C.c_double)], C.c_int),
     "ce_reserve_mixed": ([C.c_void_p, C.c_uint64], C.c_int),
@@ -356,6 +360,12 @@ class Engine:
         c = cfg.to_c()
         self._check(self.lib.ce_run_device(self.h, int(S), C.c_void_p(pos_ptr), C.byref(c), C.byref(out),
                                            C.c_void_p(stream)))
+
+    def run_verlet_device(self, S: int, pos_ptr: int, cfg: RunConfig, out: CeOutputs, stream: int = 0):
+        """Velocity Verlet with the fixed step cfg.max_dt (ce_run_verlet_device)."""
+        c = cfg.to_c()
+        self._check(self.lib.ce_run_verlet_device(self.h, int(S), C.c_void_p(pos_ptr), C.byref(c), C.byref(out),
+                                                  C.c_void_p(stream)))
 
     def last_launch_count(self) -> int:
         return int(self.lib.ce_last_launch_count(self.h))

@@ -29,7 +29,7 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-ftz=true", "-Xcompiler", "
 # (object name, source, extra flags)
 UNITS = [("ce_gpu.o", "ce_gpu.cu", []), ("probe.o", "probe.cu", []), ("noalloc.o", "noalloc.cu", []),
          ("mixed.o", "mixed.cu", []), ("sampler.o", "sampler.cu", ["-Xcompiler", "-ffp-contract=off"]),
-         ("mlp.o", "mlp.cu", []), ("closure.o", "closure.cu", [])] + [
+         ("mlp.o", "mlp.cu", []), ("closure.o", "closure.cu", []), ("verlet.o", "verlet.cu", [])] + [
     (f"kernels_fixed_m{m}.o", "kernels_fixed.cu", [f"-DCE_MODE={m}"]) for m in range(4)
 ] + [(f"kernels_atom_m{m}.o", "kernels_atom.cu", [f"-DCE_MODE={m}"]) for m in range(4)]
 

@@ -108,6 +108,7 @@ int ce_set_molecule(ce_engine* e, int n, const double* mass_me, const double* ch
     m.inv_m[i] = static_cast<float>(1.0 / mass_me[i]);
     m.q[i] = static_cast<float>(charge[i]);
     m.kq[i] = static_cast<float>(coulomb_k * charge[i]);
+    m.k = static_cast<float>(coulomb_k);
     for (int j = 0; j < n; ++j)
       m.pc[i * n + j] = static_cast<float>(coulomb_k * charge[i] * charge[j]);
   }

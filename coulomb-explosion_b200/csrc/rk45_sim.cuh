@@ -31,6 +31,7 @@ struct FixedMol {
   double mass[CE_MAX_ATOMS];              // m_i (double, FP64 finalize)
   float q[CE_MAX_ATOMS];                  // q_i (lane-per-atom layout: pair constant q_i * (k q_j))
   float kq[CE_MAX_ATOMS];                 // k q_i
+  float k;                                // Coulomb constant narrowed to float (the reference's Real k_)
 };
 
 struct RunParams {

@@ -140,6 +140,17 @@ int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
 int ce_run_device(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
                   const ce_outputs* out, void* stream);
 
+/* The Velocity Verlet strategy (IntegratorKind::VelocityVerlet,
+ * src/integrators.cpp:14-47) under the same convergence driver
+ * (src/driver.cpp:7-46) for the engine's molecule: fixed step dt =
+ * cfg->max_dt, stop at PE <= pe_stop_fraction * PE_0 or max_steps, then the
+ * energy rescale. IEEE FP32 in the reference's operation order, so results equal
+ * the reference's scalar f32 engine bit for bit. rtol / atol are unused and
+ * precision_mode must be 0. Device pointers, async on stream; outputs as
+ * ce_run_device (rejects, positions and e0 are not written). */
+int ce_run_verlet_device(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
+                         const ce_outputs* out, void* stream);
+
 /* Number of kernel launches the last ce_run / ce_run_device issued. */
 int ce_last_launch_count(const ce_engine* e);
 

@@ -48,6 +48,8 @@ typedef struct ce_oracle_cfg {
   uint64_t max_steps;      /* RunConfig::max_steps (driver.hpp:162)               */
   int redistribute_energy; /* RunConfig::redistribute_energy (driver.hpp:155)     */
   int mode;                /* 0 = reference semantics; bits CE_ORACLE_KAHAN|FP64  */
+  int integrator;          /* 0 = DP5(4); 1 = Velocity Verlet with the fixed step
+                              max_dt (src/integrators.cpp:14-47; mode must be 0)   */
 } ce_oracle_cfg;
 
 typedef struct ce_oracle_stats {

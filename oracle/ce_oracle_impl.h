@@ -272,6 +272,33 @@ static REAL SFX(step)(SFX(dp45) * d, const SFX(mol) * m, REAL (*x)[3], REAL (*v)
   }
 }
 
+/* VelocityVerlet::step, src/integrators.cpp:16-39: x += v dt + a (0.5 dt dt);
+ * a' = a(x); v += (a + a') (0.5 dt); the acceleration is carried between steps. */
+typedef struct SFX(vv) {
+  int have_accel;
+  REAL a[CE_ORACLE_NMAX][3];
+} SFX(vv);
+
+static REAL SFX(vv_step)(SFX(vv) * w, const SFX(mol) * m, REAL (*x)[3], REAL (*v)[3], REAL dt) {
+  const int n = m->n;
+  REAL na[CE_ORACLE_NMAX][3];
+  if (!w->have_accel) {
+    SFX(accel)(m, x, w->a);
+    w->have_accel = 1;
+  }
+  const REAL h2 = (REAL)0.5 * dt * dt;
+  for (int i = 0; i < n; ++i)
+    for (int c = 0; c < 3; ++c) x[i][c] += v[i][c] * dt + w->a[i][c] * h2;
+  SFX(accel)(m, x, na);
+  const REAL hd = (REAL)0.5 * dt;
+  for (int i = 0; i < n; ++i)
+    for (int c = 0; c < 3; ++c) {
+      v[i][c] += (w->a[i][c] + na[i][c]) * hd;
+      w->a[i][c] = na[i][c];
+    }
+  return dt;
+}
+
 static int SFX(all_finite)(int n, REAL (*v)[3]) {
   for (int i = 0; i < n; ++i)
     for (int c = 0; c < 3; ++c)
@@ -311,6 +338,10 @@ static int SFX(run)(int n, const double* mass, const double* charge, double coul
   int status = CE_ORACLE_OK;
   int converged = 0;
 
+  const int verlet = cfg->integrator == 1;
+  SFX(vv) w;
+  memset(&w, 0, sizeof w);
+  if (verlet && cfg->mode != 0) return -1;
   if (!fp64) {
     /* Reference semantics, all in Real. */
     const REAL pe0 = SFX(pe)(&m, x);
@@ -324,7 +355,7 @@ static int SFX(run)(int n, const double* mass, const double* charge, double coul
         converged = 0;
         break;
       }
-      const REAL dt = SFX(step)(&d, &m, x, v, max_dt);
+      const REAL dt = verlet ? SFX(vv_step)(&w, &m, x, v, max_dt) : SFX(step)(&d, &m, x, v, max_dt);
       if (dt < (REAL)0) {
         status = CE_ORACLE_REJECT_LIMIT;
         break;

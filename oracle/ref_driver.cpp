@@ -77,10 +77,12 @@ double ref_pe(int n, const double* x, const double* charge, double k) {
 // One run_to_convergence per sim over [0, S), split across `threads` host
 // threads (<= 0: hardware_concurrency). status: 0 ok, 1 integrator threw,
 // 2 max_steps, 3 non-finite momenta (bench_precision_sweep.cpp:80-85).
-void ref_run_batch(int n, const double* mass, const double* charge, double k, uint64_t S,
-                   const double* pos, double rtol, double atol, double pe_stop, double max_dt,
-                   uint64_t max_steps, int redistribute, double* p_out, uint32_t* steps,
-                   uint8_t* status, double* t_final, int threads) {
+// kind: 0 = IntegratorKind::RK45, 1 = IntegratorKind::VelocityVerlet (fixed step max_dt).
+void ref_run_batch_kind(int kind, int n, const double* mass, const double* charge, double k, uint64_t S,
+                        const double* pos, double rtol, double atol, double pe_stop, double max_dt,
+                        uint64_t max_steps, int redistribute, double* p_out, uint32_t* steps,
+                        uint8_t* status, double* t_final, int threads) {
+  const IntegratorKind ikind = kind == 1 ? IntegratorKind::VelocityVerlet : IntegratorKind::RK45;
   const Molecule mol = make_mol(n, mass, charge);
   const CoulombForce force(static_cast<Real>(k));
   RunConfig cfg;
@@ -98,7 +100,7 @@ void ref_run_batch(int n, const double* mass, const double* charge, double k, ui
       const uint64_t s1 = std::min<uint64_t>(S, s0 + 64);
       for (uint64_t s = s0; s < s1; ++s) {
         State st = make_state(n, pos + s * static_cast<uint64_t>(n) * 3);
-        auto integ = make_integrator(IntegratorKind::RK45, opts);
+        auto integ = make_integrator(ikind, opts);
         uint8_t code = 0;
         RunResult rr;
         try {
@@ -141,6 +143,14 @@ void ref_run_batch(int n, const double* mass, const double* charge, double k, ui
 // UniformSphereSampler::sample `count` times (sampler.cpp:28-57) into
 // pos_out[count][n][3]. Returns 0, -1 on std::runtime_error (infeasible),
 // -2 on std::invalid_argument (bad options).
+void ref_run_batch(int n, const double* mass, const double* charge, double k, uint64_t S,
+                   const double* pos, double rtol, double atol, double pe_stop, double max_dt,
+                   uint64_t max_steps, int redistribute, double* p_out, uint32_t* steps,
+                   uint8_t* status, double* t_final, int threads) {
+  ref_run_batch_kind(0, n, mass, charge, k, S, pos, rtol, atol, pe_stop, max_dt, max_steps, redistribute, p_out,
+                     steps, status, t_final, threads);
+}
+
 int ref_sample(double radius, double min_sep, uint64_t max_attempts, uint64_t seed, int n,
                uint64_t count, double* pos_out) {
   try {

@@ -30,6 +30,7 @@ class OracleCfg(C.Structure):
         ("max_steps", C.c_uint64),
         ("redistribute_energy", C.c_int),
         ("mode", C.c_int),
+        ("integrator", C.c_int),
     ]
 
 
@@ -93,6 +94,7 @@ def ref(bits: int) -> C.CDLL:
         vp = C.c_void_p
         lib.ref_run_batch.argtypes = [C.c_int, vp, vp, C.c_double, C.c_uint64, vp, C.c_double, C.c_double,
                                       C.c_double, C.c_double, C.c_uint64, C.c_int, vp, vp, vp, vp, C.c_int]
+        lib.ref_run_batch_kind.argtypes = [C.c_int] + lib.ref_run_batch.argtypes
         lib.ref_accel.argtypes = [C.c_int, vp, vp, vp, C.c_double, vp]
         lib.ref_pe.argtypes = [C.c_int, vp, vp, C.c_double]
         lib.ref_pe.restype = C.c_double
@@ -103,8 +105,9 @@ def ref(bits: int) -> C.CDLL:
     return _refs[bits]
 
 
-def cfg(rtol=1e-8, atol=1e-16, pe_stop=1e-9, max_dt=1e12, max_steps=1_000_000, redistribute=True, mode=0):
-    return OracleCfg(rtol, atol, pe_stop, max_dt, max_steps, 1 if redistribute else 0, mode)
+def cfg(rtol=1e-8, atol=1e-16, pe_stop=1e-9, max_dt=1e12, max_steps=1_000_000, redistribute=True, mode=0,
+        integrator=0):
+    return OracleCfg(rtol, atol, pe_stop, max_dt, max_steps, 1 if redistribute else 0, mode, integrator)
 
 
 def run_batch(pos, mass, charge, *, bits=32, k=1.0, threads=0, **kw):
@@ -142,17 +145,18 @@ def run_batch_mixed(n_per, mass, charge, pos, *, bits=32, k=1.0, threads=0, **kw
 
 
 def ref_run_batch(pos, mass, charge, *, bits=32, k=1.0, rtol=1e-8, atol=1e-16, pe_stop=1e-9, max_dt=1e12,
-                  max_steps=1_000_000, redistribute=True, threads=0):
-    """The reference scalar engine (run_to_convergence per sim) over pos [S, N, 3]."""
+                  max_steps=1_000_000, redistribute=True, threads=0, integrator=0):
+    """The reference scalar engine (run_to_convergence per sim) over pos [S, N, 3];
+    integrator 0 = RK45, 1 = Velocity Verlet with the fixed step max_dt."""
     pos = np.ascontiguousarray(pos, dtype=np.float64)
     mass = np.ascontiguousarray(mass, dtype=np.float64)
     charge = np.ascontiguousarray(charge, dtype=np.float64)
     S, n, _ = pos.shape
     out = dict(momenta=np.zeros((S, n, 3)), steps=np.zeros(S, np.uint32), status=np.zeros(S, np.uint8),
                t_final=np.zeros(S))
-    ref(bits).ref_run_batch(n, _p(mass), _p(charge), k, S, _p(pos), rtol, atol, pe_stop, max_dt, max_steps,
-                            1 if redistribute else 0, _p(out["momenta"]), _p(out["steps"]), _p(out["status"]),
-                            _p(out["t_final"]), int(threads))
+    ref(bits).ref_run_batch_kind(int(integrator), n, _p(mass), _p(charge), k, S, _p(pos), rtol, atol, pe_stop,
+                                 max_dt, max_steps, 1 if redistribute else 0, _p(out["momenta"]), _p(out["steps"]),
+                                 _p(out["status"]), _p(out["t_final"]), int(threads))
     return out
 
 
