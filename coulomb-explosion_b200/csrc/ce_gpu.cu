@@ -80,6 +80,14 @@ void ce_destroy(ce_engine* e) {
   if (!e) return;
   cudaSetDevice(e->device);
   if (e->stream) cudaStreamSynchronize(e->stream);
+  for (cudaStream_t x : {e->s_in, e->s_out})
+    if (x) {
+      cudaStreamSynchronize(x);
+      cudaStreamDestroy(x);
+    }
+  for (int i = 0; i < 2; ++i)
+    for (cudaEvent_t ev : {e->ev_loaded[i], e->ev_computed[i], e->ev_copied[i]})
+      if (ev) cudaEventDestroy(ev);
   if (e->d_arena) cudaFree(e->d_arena);
   if (e->d_mixed) cudaFree(e->d_mixed);
   if (e->d_cursor) cudaFree(e->d_cursor);
@@ -187,6 +195,10 @@ int ce_run_device(ce_engine* e, uint64_t S, const float* pos, const ce_run_confi
   return CE_OK;
 }
 
+// Host-buffer path, pipelined: the batch is cut into chunks that alternate
+// between two device slots; chunk k's positions go up on a copy-in stream while
+// chunk k-1 integrates on the engine stream and chunk k-2's results come down on
+// a copy-out stream. With pinned host buffers the copies overlap the kernels.
 int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
            const ce_outputs* out) {
   if (!e) return CE_ERR_INVALID;
@@ -196,18 +208,35 @@ int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
   if (S == 0) return CE_OK;
   if (!pos || !out || !out->momenta)
     return ce::fail(e, CE_ERR_INVALID, "ce_run: pos and out->momenta are required");
+  if (S > (1ull << 40)) return ce::fail(e, CE_ERR_INVALID, "ce_run: S too large");
   cudaError_t st = cudaSetDevice(e->device);
   if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaSetDevice");
+  if (!e->s_in) {
+    if ((st = cudaStreamCreateWithFlags(&e->s_in, cudaStreamNonBlocking)) != cudaSuccess ||
+        (st = cudaStreamCreateWithFlags(&e->s_out, cudaStreamNonBlocking)) != cudaSuccess)
+      return ce::cuda_fail(e, st, "cudaStreamCreate(copy streams)");
+    for (int i = 0; i < 2; ++i)
+      if ((st = cudaEventCreateWithFlags(&e->ev_loaded[i], cudaEventDisableTiming)) != cudaSuccess ||
+          (st = cudaEventCreateWithFlags(&e->ev_computed[i], cudaEventDisableTiming)) != cudaSuccess ||
+          (st = cudaEventCreateWithFlags(&e->ev_copied[i], cudaEventDisableTiming)) != cudaSuccess)
+        return ce::cuda_fail(e, st, "cudaEventCreate");
+  }
 
+  // chunking: one chunk below 2^18 sims, else up to 8 chunks of at least 2^17
+  constexpr uint64_t kMinChunk = 1ull << 17;
+  const uint64_t nchunks = S < 2 * kMinChunk ? 1 : std::min<uint64_t>(8, S / kMinChunk);
+  const uint64_t C = (S + nchunks - 1) / nchunks;
   const size_t n3 = static_cast<size_t>(e->n) * 3;
   auto al = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
-  const size_t b_pos = al(S * n3 * sizeof(float));
-  const size_t b_mom = al(S * n3 * sizeof(float));
-  const size_t b_d = al(S * sizeof(double));
-  const size_t b_u = al(S * sizeof(uint32_t));
-  const size_t b_s = al(S);
-  const size_t total = b_pos + 2 * b_mom + 5 * b_d + 2 * b_u + b_s;
+  const size_t b_pos = al(C * n3 * sizeof(float));
+  const size_t b_d = al(C * sizeof(double));
+  const size_t b_u = al(C * sizeof(uint32_t));
+  const size_t b_s = al(C);
+  const size_t slot_bytes = 3 * b_pos + 5 * b_d + 2 * b_u + b_s;  // pos, momenta, positions out, ...
+  const int nslots = nchunks > 1 ? 2 : 1;
+  const size_t total = slot_bytes * nslots;
   if (total > e->arena_bytes) {
+    cudaDeviceSynchronize();
     if (e->d_arena) cudaFree(e->d_arena);
     e->d_arena = nullptr;
     e->arena_bytes = 0;
@@ -215,55 +244,82 @@ int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
     if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMalloc(arena)");
     e->arena_bytes = total;
   }
-  char* base = static_cast<char*>(e->d_arena);
-  float* d_pos = reinterpret_cast<float*>(base);
-  base += b_pos;
-  ce_outputs d{};
-  d.momenta = reinterpret_cast<float*>(base);
-  base += b_mom;
-  float* d_xout = reinterpret_cast<float*>(base);
-  base += b_mom;
-  double* dd[5];
-  for (int i = 0; i < 5; ++i) {
-    dd[i] = reinterpret_cast<double*>(base);
-    base += b_d;
+  struct Slot {
+    float* pos;
+    ce_outputs d;
+  } slots[2];
+  for (int k = 0; k < nslots; ++k) {
+    char* b = static_cast<char*>(e->d_arena) + k * slot_bytes;
+    Slot& sl = slots[k];
+    sl.pos = reinterpret_cast<float*>(b);
+    b += b_pos;
+    sl.d = ce_outputs{};
+    sl.d.momenta = reinterpret_cast<float*>(b);
+    b += b_pos;
+    float* xo = reinterpret_cast<float*>(b);
+    b += b_pos;
+    double* dd[5];
+    for (int i = 0; i < 5; ++i, b += b_d) dd[i] = reinterpret_cast<double*>(b);
+    uint32_t* du[2];
+    for (int i = 0; i < 2; ++i, b += b_u) du[i] = reinterpret_cast<uint32_t*>(b);
+    sl.d.ker = out->ker ? dd[0] : nullptr;
+    sl.d.t_final = out->t_final ? dd[1] : nullptr;
+    sl.d.pe_final = out->pe_final ? dd[2] : nullptr;
+    sl.d.ke_before = out->ke_before ? dd[3] : nullptr;
+    sl.d.e0 = out->e0 ? dd[4] : nullptr;
+    sl.d.positions = out->positions ? xo : nullptr;
+    sl.d.steps = out->steps ? du[0] : nullptr;
+    sl.d.rejects = out->rejects ? du[1] : nullptr;
+    sl.d.status = out->status ? reinterpret_cast<uint8_t*>(b) : nullptr;
   }
-  uint32_t* du[2];
-  for (int i = 0; i < 2; ++i) {
-    du[i] = reinterpret_cast<uint32_t*>(base);
-    base += b_u;
-  }
-  uint8_t* d_status = reinterpret_cast<uint8_t*>(base);
-  d.ker = out->ker ? dd[0] : nullptr;
-  d.t_final = out->t_final ? dd[1] : nullptr;
-  d.pe_final = out->pe_final ? dd[2] : nullptr;
-  d.ke_before = out->ke_before ? dd[3] : nullptr;
-  d.e0 = out->e0 ? dd[4] : nullptr;
-  d.positions = out->positions ? d_xout : nullptr;
-  d.steps = out->steps ? du[0] : nullptr;
-  d.rejects = out->rejects ? du[1] : nullptr;
-  d.status = out->status ? d_status : nullptr;
 
-  st = cudaMemcpyAsync(d_pos, pos, S * n3 * sizeof(float), cudaMemcpyHostToDevice, e->stream);
-  if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMemcpyAsync(pos H2D)");
-  rc = ce_run_device(e, S, d_pos, cfg, &d, e->stream);
-  if (rc != CE_OK) return rc;
-  struct Copy {
-    void* dst;
-    const void* src;
-    size_t bytes;
-  } copies[] = {
-      {out->momenta, d.momenta, S * n3 * sizeof(float)}, {out->ker, d.ker, S * sizeof(double)},
-      {out->t_final, d.t_final, S * sizeof(double)},    {out->pe_final, d.pe_final, S * sizeof(double)},
-      {out->ke_before, d.ke_before, S * sizeof(double)}, {out->steps, d.steps, S * sizeof(uint32_t)},
-      {out->rejects, d.rejects, S * sizeof(uint32_t)},  {out->status, d.status, S},
-      {out->positions, d.positions, S * n3 * sizeof(float)}, {out->e0, d.e0, S * sizeof(double)}};
-  for (const Copy& c : copies) {
-    if (!c.dst) continue;
-    st = cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, e->stream);
-    if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMemcpyAsync(D2H)");
+  int launches = 0;
+  for (uint64_t k = 0; k < nchunks; ++k) {
+    const uint64_t s0 = k * C;
+    if (s0 >= S) break;
+    const uint64_t Sk = std::min<uint64_t>(C, S - s0);
+    const int sl = static_cast<int>(k % nslots);
+    Slot& slot = slots[sl];
+    // positions up once the slot's previous chunk has been integrated
+    if (k >= 2 && (st = cudaStreamWaitEvent(e->s_in, e->ev_computed[sl], 0)) != cudaSuccess)
+      return ce::cuda_fail(e, st, "cudaStreamWaitEvent");
+    st = cudaMemcpyAsync(slot.pos, pos + s0 * n3, Sk * n3 * sizeof(float), cudaMemcpyHostToDevice, e->s_in);
+    if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMemcpyAsync(pos H2D)");
+    cudaEventRecord(e->ev_loaded[sl], e->s_in);
+    // integrate once the positions are in and the slot's previous results are out
+    cudaStreamWaitEvent(e->stream, e->ev_loaded[sl], 0);
+    if (k >= 2) cudaStreamWaitEvent(e->stream, e->ev_copied[sl], 0);
+    rc = ce_run_device(e, Sk, slot.pos, cfg, &slot.d, e->stream);
+    if (rc != CE_OK) return rc;
+    launches += e->last_launches;
+    cudaEventRecord(e->ev_computed[sl], e->stream);
+    // results down
+    cudaStreamWaitEvent(e->s_out, e->ev_computed[sl], 0);
+    struct Copy {
+      void* dst;
+      const void* src;
+      size_t bytes;
+    } copies[] = {
+        {out->momenta ? out->momenta + s0 * n3 : nullptr, slot.d.momenta, Sk * n3 * sizeof(float)},
+        {out->ker ? out->ker + s0 : nullptr, slot.d.ker, Sk * sizeof(double)},
+        {out->t_final ? out->t_final + s0 : nullptr, slot.d.t_final, Sk * sizeof(double)},
+        {out->pe_final ? out->pe_final + s0 : nullptr, slot.d.pe_final, Sk * sizeof(double)},
+        {out->ke_before ? out->ke_before + s0 : nullptr, slot.d.ke_before, Sk * sizeof(double)},
+        {out->steps ? out->steps + s0 : nullptr, slot.d.steps, Sk * sizeof(uint32_t)},
+        {out->rejects ? out->rejects + s0 : nullptr, slot.d.rejects, Sk * sizeof(uint32_t)},
+        {out->status ? out->status + s0 : nullptr, slot.d.status, Sk},
+        {out->positions ? out->positions + s0 * n3 : nullptr, slot.d.positions, Sk * n3 * sizeof(float)},
+        {out->e0 ? out->e0 + s0 : nullptr, slot.d.e0, Sk * sizeof(double)}};
+    for (const Copy& c : copies) {
+      if (!c.dst) continue;
+      st = cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, e->s_out);
+      if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMemcpyAsync(D2H)");
+    }
+    cudaEventRecord(e->ev_copied[sl], e->s_out);
   }
-  st = cudaStreamSynchronize(e->stream);
+  e->last_launches = launches;
+  st = cudaStreamSynchronize(e->s_out);
+  if (st == cudaSuccess) st = cudaStreamSynchronize(e->stream);
   if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaStreamSynchronize");
   return CE_OK;
 }
