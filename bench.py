@@ -892,7 +892,7 @@ def main():
                          "network's fused forward alone; stream: 1e8 C2H6-like explosions streamed in 1e6 chunks, "
                          "closure vs plain")
     ap.add_argument("--train-sims", type=int, default=5_000_000, help="closure: training pairs")
-    ap.add_argument("--epochs", type=int, default=20, help="closure: training epochs")
+    ap.add_argument("--epochs", type=int, default=40, help="closure: training epochs")
     ap.add_argument("--minibatch", type=int, default=8192, help="closure: rows per training step")
     ap.add_argument("--lr", type=float, default=1e-3, help="closure: peak Adam learning rate")
     ap.add_argument("--gate-quantile", type=float, default=0.99, help="closure: gate bounds quantile")
