@@ -64,208 +64,228 @@ struct FeatArgs {
   float* weight;   // optional [S_pad][kOut]
 };
 
-__device__ __forceinline__ void zero_row(const FeatArgs& A, uint64_t s) {
-  uint4* f = reinterpret_cast<uint4*>(A.feats + s * kFeat);  // 256 B row, 16-B aligned
-#pragma unroll
-  for (int c = 0; c < kFeat * 2 / 16; ++c) f[c] = make_uint4(0u, 0u, 0u, 0u);
-  if (A.target) {
-    float4* t = reinterpret_cast<float4*>(A.target + s * kOut);
-    float4* w = reinterpret_cast<float4*>(A.weight + s * kOut);
-#pragma unroll
-    for (int c = 0; c < kOut / 4; ++c) {
-      t[c] = make_float4(0.f, 0.f, 0.f, 0.f);
-      w[c] = make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-  }
-}
+// Features kernel: a block owns a tile of 128 consecutive sims, one per
+// thread; the tile's feature rows and base momenta leave through shared memory
+// with coalesced stores (a per-thread row write would touch one line per lane).
+constexpr int kFT = 128;                 // sims per tile (= threads per block)
+constexpr int kFRow = kFeat + 8;         // padded bf16 feature row in shared memory (272 B)
+constexpr size_t kFeatSmem = static_cast<size_t>(kFT) * (3 * kA * 4) + static_cast<size_t>(kFT) * kFRow * 2;
 
-__global__ void __launch_bounds__(128) closure_features_kernel(const FeatArgs A) {
-  for (uint64_t s = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; s < A.S_pad;
-       s += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-    if (s >= A.S) {
-      zero_row(A, s);
-      continue;
-    }
-    const int n = A.n_atoms[s];
-    const bool ok = n >= 2 && n <= kA && A.status[s] == CE_SIM_OK;
-    if (!ok) {
-      zero_row(A, s);
-      for (int c = 0; c < 3 * kA; ++c) A.p_base[s * 3 * kA + c] = 0.0f;
-      A.p_scale[s] = 0.0f;
-      continue;
-    }
-    const double* ms = A.mass + s * kA;
-    const double* qs = A.charge + s * kA;
+__global__ void __launch_bounds__(kFT, 4) closure_features_kernel(const FeatArgs A) {
+  extern __shared__ __align__(16) uint8_t fsm[];
+  float* spb = reinterpret_cast<float*>(fsm);              // [kFT][30]
+  bf16* sf = reinterpret_cast<bf16*>(spb + kFT * 3 * kA);  // [kFT][kFRow]
+  const int tid = threadIdx.x;
+  for (uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * kFT; t0 < A.S_pad;
+       t0 += static_cast<uint64_t>(gridDim.x) * kFT) {
+    const int rows = t0 < A.S ? static_cast<int>(A.S - t0 < kFT ? A.S - t0 : kFT) : 0;
+    const uint64_t s = t0 + tid;
+    float* pb = spb + tid * 3 * kA;
+    bf16* f = sf + tid * kFRow;
     const float* xs = A.x + s * 3 * kA;
     const float* ps = A.p + s * 3 * kA;
-    float x[kA][3], p[kA][3], im[kA], q[kA];
-    double msum = 0.0, cx = 0.0, cy = 0.0, cz = 0.0;
+    const double* ms = A.mass + s * kA;
+    const double* qs = A.charge + s * kA;
+    const int n = tid < rows ? A.n_atoms[s] : 0;
+    bool ok = tid < rows && n >= 2 && n <= kA && A.status[s] == CE_SIM_OK;
+    float scale_out = 0.0f;
+    float x[kA][3], p[kA][3], im[kA], q[kA], dp[kA][3];
+    float com[3] = {0.0f, 0.0f, 0.0f};
+    float P = 0.0f, Q = 0.0f, L = 0.0f;
+    double e0 = 1.0;
+    if (ok) {
+      double msum = 0.0, cx = 0.0, cy = 0.0, cz = 0.0;
 #pragma unroll
-    for (int i = 0; i < kA; ++i) {
-      const bool on = i < n;
-      const double mi = on ? ms[i] : 1.0;
-      im[i] = on ? static_cast<float>(1.0 / mi) : 0.0f;
-      q[i] = on ? static_cast<float>(qs[i]) : 0.0f;
+      for (int i = 0; i < kA; ++i) {
+        const bool on = i < n;
+        const double mi = on ? ms[i] : 1.0;
+        im[i] = on ? static_cast<float>(1.0 / mi) : 0.0f;
+        q[i] = on ? static_cast<float>(qs[i]) : 0.0f;
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        x[i][c] = on ? xs[3 * i + c] : 0.0f;
-        p[i][c] = on ? ps[3 * i + c] : 0.0f;
+        for (int c = 0; c < 3; ++c) {
+          x[i][c] = on ? xs[3 * i + c] : 0.0f;
+          p[i][c] = on ? ps[3 * i + c] : 0.0f;
+        }
+        if (on) {
+          msum += mi;
+          cx += mi * x[i][0];
+          cy += mi * x[i][1];
+          cz += mi * x[i][2];
+        }
       }
-      if (on) {
-        msum += mi;
-        cx += mi * x[i][0];
-        cy += mi * x[i][1];
-        cz += mi * x[i][2];
-      }
-    }
-    const float com[3] = {static_cast<float>(cx / msum), static_cast<float>(cy / msum), static_cast<float>(cz / msum)};
+      com[0] = static_cast<float>(cx / msum);
+      com[1] = static_cast<float>(cy / msum);
+      com[2] = static_cast<float>(cz / msum);
 
-    // Ballistic pair impulses from the stop to t -> infinity.
-    float dp[kA][3];
+      // Ballistic pair impulses from the stop to t -> infinity.
 #pragma unroll
-    for (int i = 0; i < kA; ++i) dp[i][0] = dp[i][1] = dp[i][2] = 0.0f;
-    bool bad = false;
-    const float kf = static_cast<float>(A.k);
+      for (int i = 0; i < kA; ++i) dp[i][0] = dp[i][1] = dp[i][2] = 0.0f;
+      bool bad = false;
+      const float kf = static_cast<float>(A.k);
 #pragma unroll
-    for (int i = 0; i < kA; ++i) {
+      for (int i = 0; i < kA; ++i) {
 #pragma unroll
-      for (int j = i + 1; j < kA; ++j) {
-        if (j < n) {
-          const float rx = x[i][0] - x[j][0], ry = x[i][1] - x[j][1], rz = x[i][2] - x[j][2];
-          const float wx = p[i][0] * im[i] - p[j][0] * im[j];
-          const float wy = p[i][1] * im[i] - p[j][1] * im[j];
-          const float wz = p[i][2] * im[i] - p[j][2] * im[j];
-          const float a = wx * wx + wy * wy + wz * wz;
-          const float b = rx * wx + ry * wy + rz * wz;
-          const float c = rx * rx + ry * ry + rz * rz;
-          const float sa = sqrtf(a), sc = sqrtf(c), sac = sa * sc;
-          float g;
-          if (b >= 0.0f) {
-            g = sac + b;
-          } else {  // approaching pair: |r|^2|w|^2 - (r.w)^2 = |r x w|^2 avoids the cancellation
-            const float ux = ry * wz - rz * wy, uy = rz * wx - rx * wz, uz = rx * wy - ry * wx;
-            g = (ux * ux + uy * uy + uz * uz) / (sac - b);
+        for (int j = i + 1; j < kA; ++j) {
+          if (j < n) {
+            const float rx = x[i][0] - x[j][0], ry = x[i][1] - x[j][1], rz = x[i][2] - x[j][2];
+            const float wx = p[i][0] * im[i] - p[j][0] * im[j];
+            const float wy = p[i][1] * im[i] - p[j][1] * im[j];
+            const float wz = p[i][2] * im[i] - p[j][2] * im[j];
+            const float a = wx * wx + wy * wy + wz * wz;
+            const float b = rx * wx + ry * wy + rz * wz;
+            const float c = rx * rx + ry * ry + rz * rz;
+            // approximate reciprocal square roots / reciprocal (a few ulp; the
+            // features are rounded to BF16 and the base is checked to 3e-5)
+            const float rsa = rsqrtf(a), rsc = rsqrtf(c);
+            const float sac = (a * rsa) * (c * rsc);
+            float g;
+            if (b >= 0.0f) {
+              g = sac + b;
+            } else {  // approaching pair: |r|^2|w|^2 - (r.w)^2 = |r x w|^2 avoids the cancellation
+              const float ux = ry * wz - rz * wy, uy = rz * wx - rx * wz, uz = rx * wy - ry * wx;
+              g = __fdividef(ux * ux + uy * uy + uz * uz, sac - b);
+            }
+            const float ig = __fdividef(1.0f, g);
+            const float I0 = ig * rsc, I1 = ig * rsa;
+            if (!(g > 0.0f) || !isfinite(I0) || !isfinite(I1)) bad = true;
+            const float fpair = kf * q[i] * q[j];
+            const float tx = fpair * (rx * I0 + wx * I1), ty = fpair * (ry * I0 + wy * I1),
+                        tz = fpair * (rz * I0 + wz * I1);
+            dp[i][0] += tx;
+            dp[i][1] += ty;
+            dp[i][2] += tz;
+            dp[j][0] -= tx;
+            dp[j][1] -= ty;
+            dp[j][2] -= tz;
           }
-          const float I0 = 1.0f / (sc * g), I1 = 1.0f / (sa * g);
-          if (!(g > 0.0f) || !isfinite(I0) || !isfinite(I1)) bad = true;
-          const float f = kf * q[i] * q[j];
-          const float tx = f * (rx * I0 + wx * I1), ty = f * (ry * I0 + wy * I1), tz = f * (rz * I0 + wz * I1);
-          dp[i][0] += tx;
-          dp[i][1] += ty;
-          dp[i][2] += tz;
-          dp[j][0] -= tx;
-          dp[j][1] -= ty;
-          dp[j][2] -= tz;
         }
       }
-    }
-    // Base = (p + dp) rescaled to KE = E_0 (src/driver.cpp:38-42 on the ballistic state).
-    double ke = 0.0;
-#pragma unroll
-    for (int i = 0; i < kA; ++i) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        dp[i][c] += p[i][c];
-        ke += 0.5 * static_cast<double>(dp[i][c]) * dp[i][c] * im[i];
-      }
-    }
-    const double e0 = A.e0[s];
-    const float sc = static_cast<float>(sqrt(e0 / ke));
-    double p2 = 0.0, r2 = 0.0;
-#pragma unroll
-    for (int i = 0; i < kA; ++i) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        dp[i][c] *= sc;
-        p2 += static_cast<double>(dp[i][c]) * dp[i][c];
-        if (i < n) {
-          const double d = x[i][c] - com[c];
-          r2 += d * d;
-        }
-      }
-    }
-    double q2 = 0.0;
-#pragma unroll
-    for (int i = 0; i < kA; ++i) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const double d = static_cast<double>(dp[i][c]) - p[i][c];
-        q2 += d * d;
-      }
-    }
-    const float P = static_cast<float>(sqrt(p2 / n));
-    const float Q = static_cast<float>(sqrt(q2 / n));  // RMS per-atom size of the analytic step p -> p_base
-    const float L = static_cast<float>(sqrt(r2 / n));
-    if (bad || !(ke > 0.0) || !isfinite(sc) || !(P > 0.0f) || !isfinite(P) || !(Q > 0.0f) || !isfinite(Q) ||
-        !(L > 0.0f)) {
-      zero_row(A, s);
-      for (int c = 0; c < 3 * kA; ++c) A.p_base[s * 3 * kA + c] = 0.0f;
-      A.p_scale[s] = __int_as_float(0x7fc00000);  // NaN: the gate sends the sim to plain integration
-      continue;
-    }
-    float* pb = A.p_base + s * 3 * kA;
-#pragma unroll
-    for (int i = 0; i < kA; ++i) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) pb[3 * i + c] = dp[i][c];
-    }
-    A.p_scale[s] = Q;
-
-    // Features: per atom (x - x_com)/L, p/P, (p_base - p)/P, q/3, ln(m/amu)/3.5,
-    // 1; then the remaining PE fraction at the stop and n/10; zeros to the
-    // padded width.
-    const float iL = 1.0f / L, iP = 1.0f / P;
-    __align__(16) bf16 f[kFeat];
-#pragma unroll
-    for (int i = 0; i < kA; ++i) {
-      const bool on = i < n;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        f[kPerAtom * i + c] = __float2bfloat16_rn(on ? (x[i][c] - com[c]) * iL : 0.0f);
-        f[kPerAtom * i + 3 + c] = __float2bfloat16_rn(on ? p[i][c] * iP : 0.0f);
-        f[kPerAtom * i + 6 + c] = __float2bfloat16_rn(on ? (dp[i][c] - p[i][c]) * iP : 0.0f);
-      }
-      f[kPerAtom * i + 9] = __float2bfloat16_rn(on ? q[i] * (1.0f / 3.0f) : 0.0f);
-      f[kPerAtom * i + 10] =
-          __float2bfloat16_rn(on ? static_cast<float>(log(ms[i] / kMassUnit)) * kLogMassScale : 0.0f);
-      f[kPerAtom * i + 11] = __float2bfloat16_rn(on ? 1.0f : 0.0f);
-    }
-    f[kPerAtom * kA] = __float2bfloat16_rn(static_cast<float>(A.pe_final[s] / e0) * 20.0f);
-    f[kPerAtom * kA + 1] = __float2bfloat16_rn(static_cast<float>(n) * 0.1f);
-#pragma unroll
-    for (int c = kPerAtom * kA + 2; c < kFeat; ++c) f[c] = __float2bfloat16_rn(0.0f);
-    uint4* fo = reinterpret_cast<uint4*>(A.feats + s * kFeat);
-    const uint4* fi = reinterpret_cast<const uint4*>(f);
-#pragma unroll
-    for (int c = 0; c < kFeat * 2 / 16; ++c) fo[c] = fi[c];
-
-    if (A.target) {
-      // Targets (p_true - p_base)/Q; weights w_scale / (3n) scaled by
-      // kRelRef / sqrt(rms^2 + kRelEps^2), rms = the RMS target of the sim, so
-      // the loss weighs each sim's relative rather than absolute residual.
-      const float iQ = 1.0f / Q;
-      const float* pt = A.p_true + s * 3 * kA;
-      float* t = A.target + s * kOut;
-      float* w = A.weight + s * kOut;
-      float ss = 0.0f;
+      // Base = (p + dp) rescaled to KE = E_0 (src/driver.cpp:38-42 on the ballistic state).
+      double ke = 0.0;
 #pragma unroll
       for (int i = 0; i < kA; ++i) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          const float v = i < n ? (pt[3 * i + c] - dp[i][c]) * iQ : 0.0f;
-          t[3 * i + c] = v;
-          ss += v * v;
+          dp[i][c] += p[i][c];
+          ke += 0.5 * static_cast<double>(dp[i][c]) * dp[i][c] * im[i];
         }
       }
-      const float rms2 = ss / static_cast<float>(3 * n);
-      const float wv = A.w_scale / static_cast<float>(3 * n) * kRelRef * rsqrtf(rms2 + kRelEps * kRelEps);
+      e0 = A.e0[s];
+      const float scl = static_cast<float>(sqrt(e0 / ke));
+      double p2 = 0.0, r2 = 0.0, q2 = 0.0;
 #pragma unroll
       for (int i = 0; i < kA; ++i) {
 #pragma unroll
-        for (int c = 0; c < 3; ++c) w[3 * i + c] = i < n ? wv : 0.0f;
+        for (int c = 0; c < 3; ++c) {
+          dp[i][c] *= scl;
+          p2 += static_cast<double>(dp[i][c]) * dp[i][c];
+          const double d = static_cast<double>(dp[i][c]) - p[i][c];
+          q2 += d * d;
+          if (i < n) {
+            const double dx = x[i][c] - com[c];
+            r2 += dx * dx;
+          }
+        }
       }
-      for (int c = 3 * kA; c < kOut; ++c) t[c] = w[c] = 0.0f;
+      P = static_cast<float>(sqrt(p2 / n));
+      Q = static_cast<float>(sqrt(q2 / n));  // RMS per-atom size of the analytic step p -> p_base
+      L = static_cast<float>(sqrt(r2 / n));
+      if (bad || !(ke > 0.0) || !isfinite(scl) || !(P > 0.0f) || !isfinite(P) || !(Q > 0.0f) || !isfinite(Q) ||
+          !(L > 0.0f)) {
+        ok = false;
+        scale_out = __int_as_float(0x7fc00000);  // NaN: the gate sends the sim to plain integration
+      } else {
+        scale_out = Q;
+      }
     }
+    if (tid < rows) A.p_scale[s] = scale_out;
+    if (ok) {
+#pragma unroll
+      for (int i = 0; i < kA; ++i) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) pb[3 * i + c] = dp[i][c];
+      }
+      // Features: per atom (x - x_com)/L, p/P, (p_base - p)/P, q/3,
+      // ln(m/amu)/3.5, 1; then the remaining PE fraction at the stop and n/10;
+      // zeros to the padded width.
+      const float iL = 1.0f / L, iP = 1.0f / P;
+#pragma unroll
+      for (int i = 0; i < kA; ++i) {
+        const bool on = i < n;
+        __nv_bfloat162* f2 = reinterpret_cast<__nv_bfloat162*>(f + kPerAtom * i);
+        const float v0 = on ? (x[i][0] - com[0]) * iL : 0.0f, v1 = on ? (x[i][1] - com[1]) * iL : 0.0f;
+        const float v2 = on ? (x[i][2] - com[2]) * iL : 0.0f, v3 = on ? p[i][0] * iP : 0.0f;
+        const float v4 = on ? p[i][1] * iP : 0.0f, v5 = on ? p[i][2] * iP : 0.0f;
+        const float v6 = on ? (dp[i][0] - p[i][0]) * iP : 0.0f, v7 = on ? (dp[i][1] - p[i][1]) * iP : 0.0f;
+        const float v8 = on ? (dp[i][2] - p[i][2]) * iP : 0.0f, v9 = on ? q[i] * (1.0f / 3.0f) : 0.0f;
+        const float v10 = on ? logf(static_cast<float>(ms[i] / kMassUnit)) * kLogMassScale : 0.0f;
+        const float v11 = on ? 1.0f : 0.0f;
+        f2[0] = __floats2bfloat162_rn(v0, v1);
+        f2[1] = __floats2bfloat162_rn(v2, v3);
+        f2[2] = __floats2bfloat162_rn(v4, v5);
+        f2[3] = __floats2bfloat162_rn(v6, v7);
+        f2[4] = __floats2bfloat162_rn(v8, v9);
+        f2[5] = __floats2bfloat162_rn(v10, v11);
+      }
+      __nv_bfloat162* g2 = reinterpret_cast<__nv_bfloat162*>(f + kPerAtom * kA);
+      g2[0] = __floats2bfloat162_rn(static_cast<float>(A.pe_final[s] / e0) * 20.0f, static_cast<float>(n) * 0.1f);
+#pragma unroll
+      for (int c = 1; c < (kFeat - kPerAtom * kA) / 2; ++c) g2[c] = __floats2bfloat162_rn(0.0f, 0.0f);
+
+      if (A.target) {
+        // Targets (p_true - p_base)/Q; weights w_scale / (3n) scaled by
+        // kRelRef / sqrt(rms^2 + kRelEps^2), rms = the RMS target of the sim, so
+        // the loss weighs each sim's relative rather than absolute residual.
+        const float iQ = 1.0f / Q;
+        const float* pt = A.p_true + s * 3 * kA;
+        float* t = A.target + s * kOut;
+        float* w = A.weight + s * kOut;
+        float ss = 0.0f;
+#pragma unroll
+        for (int i = 0; i < kA; ++i) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const float v = i < n ? (pt[3 * i + c] - dp[i][c]) * iQ : 0.0f;
+            t[3 * i + c] = v;
+            ss += v * v;
+          }
+        }
+        const float rms2 = ss / static_cast<float>(3 * n);
+        const float wv = A.w_scale / static_cast<float>(3 * n) * kRelRef * rsqrtf(rms2 + kRelEps * kRelEps);
+#pragma unroll
+        for (int i = 0; i < kA; ++i) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) w[3 * i + c] = i < n ? wv : 0.0f;
+        }
+        for (int c = 3 * kA; c < kOut; ++c) t[c] = w[c] = 0.0f;
+      }
+    } else {
+      for (int c = 0; c < 3 * kA; ++c) pb[c] = 0.0f;
+      uint4* fz = reinterpret_cast<uint4*>(f);
+#pragma unroll
+      for (int c = 0; c < kFeat * 2 / 16; ++c) fz[c] = make_uint4(0u, 0u, 0u, 0u);
+      if (A.target && s < A.S_pad) {
+        float4* t = reinterpret_cast<float4*>(A.target + s * kOut);
+        float4* w = reinterpret_cast<float4*>(A.weight + s * kOut);
+#pragma unroll
+        for (int c = 0; c < kOut / 4; ++c) {
+          t[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+          w[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+      }
+    }
+    __syncthreads();
+    // coalesced stores of the tile: feature rows (all 128, padded rows zero) and base momenta
+    {
+      uint4* fo = reinterpret_cast<uint4*>(A.feats + t0 * kFeat);
+      constexpr int kPerRow = kFeat * 2 / 16;  // uint4 per feature row
+      for (int u = tid; u < kFT * kPerRow; u += kFT) {
+        const int r = u / kPerRow, j = u - r * kPerRow;
+        fo[u] = *reinterpret_cast<const uint4*>(sf + r * kFRow + j * 8);
+      }
+      for (int k = tid; k < rows * 3 * kA; k += kFT) A.p_base[t0 * 3 * kA + k] = spb[k];
+    }
+    __syncthreads();
   }
 }
 
@@ -443,7 +463,14 @@ int launch_features(uint64_t S, const ce_mixed_batch* in, double k, const ce_clo
   A.weight = weight;
   int dev = 0;
   cudaGetDevice(&dev);
-  closure_features_kernel<<<grid_for(A.S_pad, dev), 128, 0, s>>>(A);
+  if (cudaFuncSetAttribute(closure_features_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(kFeatSmem)) != cudaSuccess)
+    return CE_ERR_CUDA;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const uint64_t tiles = A.S_pad / kFT;
+  const uint64_t cap = static_cast<uint64_t>(sms) * 4;
+  closure_features_kernel<<<static_cast<unsigned>(tiles < cap ? tiles : cap), kFT, kFeatSmem, s>>>(A);
   return cudaGetLastError() == cudaSuccess ? CE_OK : CE_ERR_CUDA;
 }
 
@@ -659,7 +686,7 @@ int ce_closure_serve(ce_closure* c, uint64_t S, const ce_mixed_batch* in, double
   fo.ker = c->fb_ker;
   fo.steps = c->fb_steps;
   fo.status = c->fb_st;
-  rc = ce_run_mixed_device(c->e, S, &fbin, coulomb_k, cfg, &fo, sched, stream);
+  rc = ce::run_mixed_device(c->e, S, &fbin, coulomb_k, cfg, &fo, sched, stream, /*skip_empty=*/true);
   if (rc != CE_OK) return cfail(c, rc, std::string("fallback run: ") + ce_last_error(c->e));
   MergeArgs M{S, c->fb, c->fb_m, c->fb_ker, c->fb_steps, c->fb_st, out->momenta, out->ker, out->steps, out->status};
   closure_merge_kernel<<<grid_for(S, c->e->device), 128, 0, s>>>(M);

@@ -116,6 +116,12 @@ inline MixedKernelFn select_mixed_kernel(int n, int mode) {
   }
 }
 
+// ce_run_mixed_device with one extra switch: skip_empty leaves rows with
+// n_atoms == 0 untouched instead of writing CE_SIM_BAD_INPUT outputs (the
+// closure's plain rerun of the sims its gate sent back). Defined in mixed.cu.
+int run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coulomb_k, const ce_run_config* cfg,
+                     const ce_outputs* out, int schedule, void* stream, bool skip_empty);
+
 // Dynamic shared memory of a lane-per-atom block.
 inline size_t atom_smem_bytes(int block) {
   return static_cast<size_t>(block / 32) * kAtomBufSlots * sizeof(float4);

@@ -95,7 +95,7 @@ __global__ void bucket_scatter_kernel(const uint8_t* __restrict__ n_per, uint64_
     __syncthreads();
     if (bin >= 2) {
       perm[off[bin] + b[bin] + r] = static_cast<uint32_t>(i);
-    } else if (bin >= 0) {
+    } else if (bin >= 0 && !(P.skip_empty && n_per[i] == 0)) {
       float* m = P.momenta + i * (3ull * ce::kMixedStride);
       for (int c = 0; c < 3 * ce::kMixedStride; ++c) m[c] = 0.0f;
       if (P.ker) P.ker[i] = 0.0;
@@ -166,6 +166,15 @@ int ce_reserve_mixed(ce_engine* e, uint64_t S) {
 
 int ce_run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coulomb_k,
                         const ce_run_config* cfg, const ce_outputs* out, int schedule, void* stream) {
+  return ce::run_mixed_device(e, S, in, coulomb_k, cfg, out, schedule, stream, false);
+}
+
+}  // extern "C"
+
+namespace ce {
+
+int run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coulomb_k, const ce_run_config* cfg,
+                     const ce_outputs* out, int schedule, void* stream, bool skip_empty) {
   if (!e) return CE_ERR_INVALID;
   e->last_launches = 0;
   int rc = check_mixed_args(e, S, in, coulomb_k, cfg, out);
@@ -187,6 +196,7 @@ int ce_run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, doub
 
   ce::RunParams P{};
   ce::fill_run_params(P, cfg, out, t.refill_threshold);
+  P.skip_empty = skip_empty ? 1 : 0;
   P.pos = in->pos;
   P.cursor = nullptr;
   P.S = S;
@@ -238,6 +248,10 @@ int ce_run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, doub
   e->last_launches = launches;
   return CE_OK;
 }
+
+}  // namespace ce
+
+extern "C" {
 
 int ce_run_mixed(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coulomb_k, const ce_run_config* cfg,
                  const ce_outputs* out) {

@@ -54,6 +54,7 @@ struct RunParams {
   uint32_t max_steps;
   int32_t redistribute;
   int32_t refill_threshold;
+  int32_t skip_empty;  // mixed batches: rows with n_atoms == 0 are left untouched (no outputs written)
 };
 
 template <int N, int MODE>
