@@ -71,6 +71,204 @@ constexpr int kFT = 128;                 // sims per tile (= threads per block)
 constexpr int kFRow = kFeat + 8;         // padded bf16 feature row in shared memory (272 B)
 constexpr size_t kFeatSmem = static_cast<size_t>(kFT) * (3 * kA * 4) + static_cast<size_t>(kFT) * kFRow * 2;
 
+// One sim's base momenta (into pb, 30 floats), features (into f, kFeat BF16),
+// scale (p_scale[s]) and, for training, targets and weights. live = the row is a
+// real sim (else zeros).
+__device__ __forceinline__ void feat_one(const FeatArgs& A, uint64_t s, bool live, float* pb, bf16* f) {
+  const float* xs = A.x + s * 3 * kA;
+  const float* ps = A.p + s * 3 * kA;
+  const double* ms = A.mass + s * kA;
+  const double* qs = A.charge + s * kA;
+  const int n = live ? A.n_atoms[s] : 0;
+  bool ok = live && n >= 2 && n <= kA && A.status[s] == CE_SIM_OK;
+  float scale_out = 0.0f;
+  float x[kA][3], p[kA][3], im[kA], q[kA], dp[kA][3];
+  float com[3] = {0.0f, 0.0f, 0.0f};
+  float P = 0.0f, Q = 0.0f, L = 0.0f;
+  double e0 = 1.0;
+  if (ok) {
+    double msum = 0.0, cx = 0.0, cy = 0.0, cz = 0.0;
+#pragma unroll
+    for (int i = 0; i < kA; ++i) {
+      const bool on = i < n;
+      const double mi = on ? ms[i] : 1.0;
+      im[i] = on ? static_cast<float>(1.0 / mi) : 0.0f;
+      q[i] = on ? static_cast<float>(qs[i]) : 0.0f;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        x[i][c] = on ? xs[3 * i + c] : 0.0f;
+        p[i][c] = on ? ps[3 * i + c] : 0.0f;
+      }
+      if (on) {
+        msum += mi;
+        cx += mi * x[i][0];
+        cy += mi * x[i][1];
+        cz += mi * x[i][2];
+      }
+    }
+    com[0] = static_cast<float>(cx / msum);
+    com[1] = static_cast<float>(cy / msum);
+    com[2] = static_cast<float>(cz / msum);
+
+    // Ballistic pair impulses from the stop to t -> infinity.
+#pragma unroll
+    for (int i = 0; i < kA; ++i) dp[i][0] = dp[i][1] = dp[i][2] = 0.0f;
+    bool bad = false;
+    const float kf = static_cast<float>(A.k);
+#pragma unroll
+    for (int i = 0; i < kA; ++i) {
+#pragma unroll
+      for (int j = i + 1; j < kA; ++j) {
+        if (j < n) {
+          const float rx = x[i][0] - x[j][0], ry = x[i][1] - x[j][1], rz = x[i][2] - x[j][2];
+          const float wx = p[i][0] * im[i] - p[j][0] * im[j];
+          const float wy = p[i][1] * im[i] - p[j][1] * im[j];
+          const float wz = p[i][2] * im[i] - p[j][2] * im[j];
+          const float a = wx * wx + wy * wy + wz * wz;
+          const float b = rx * wx + ry * wy + rz * wz;
+          const float c = rx * rx + ry * ry + rz * rz;
+          // approximate reciprocal square roots / reciprocal (a few ulp; the
+          // features are rounded to BF16 and the base is checked to 3e-5)
+          const float rsa = rsqrtf(a), rsc = rsqrtf(c);
+          const float sac = (a * rsa) * (c * rsc);
+          float g;
+          if (b >= 0.0f) {
+            g = sac + b;
+          } else {  // approaching pair: |r|^2|w|^2 - (r.w)^2 = |r x w|^2 avoids the cancellation
+            const float ux = ry * wz - rz * wy, uy = rz * wx - rx * wz, uz = rx * wy - ry * wx;
+            g = __fdividef(ux * ux + uy * uy + uz * uz, sac - b);
+          }
+          const float ig = __fdividef(1.0f, g);
+          const float I0 = ig * rsc, I1 = ig * rsa;
+          if (!(g > 0.0f) || !isfinite(I0) || !isfinite(I1)) bad = true;
+          const float fpair = kf * q[i] * q[j];
+          const float tx = fpair * (rx * I0 + wx * I1), ty = fpair * (ry * I0 + wy * I1),
+                      tz = fpair * (rz * I0 + wz * I1);
+          dp[i][0] += tx;
+          dp[i][1] += ty;
+          dp[i][2] += tz;
+          dp[j][0] -= tx;
+          dp[j][1] -= ty;
+          dp[j][2] -= tz;
+        }
+      }
+    }
+    // Base = (p + dp) rescaled to KE = E_0 (src/driver.cpp:38-42 on the ballistic state).
+    double ke = 0.0;
+#pragma unroll
+    for (int i = 0; i < kA; ++i) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        dp[i][c] += p[i][c];
+        ke += 0.5 * static_cast<double>(dp[i][c]) * dp[i][c] * im[i];
+      }
+    }
+    e0 = A.e0[s];
+    const float scl = static_cast<float>(sqrt(e0 / ke));
+    double p2 = 0.0, r2 = 0.0, q2 = 0.0;
+#pragma unroll
+    for (int i = 0; i < kA; ++i) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        dp[i][c] *= scl;
+        p2 += static_cast<double>(dp[i][c]) * dp[i][c];
+        const double d = static_cast<double>(dp[i][c]) - p[i][c];
+        q2 += d * d;
+        if (i < n) {
+          const double dx = x[i][c] - com[c];
+          r2 += dx * dx;
+        }
+      }
+    }
+    P = static_cast<float>(sqrt(p2 / n));
+    Q = static_cast<float>(sqrt(q2 / n));  // RMS per-atom size of the analytic step p -> p_base
+    L = static_cast<float>(sqrt(r2 / n));
+    if (bad || !(ke > 0.0) || !isfinite(scl) || !(P > 0.0f) || !isfinite(P) || !(Q > 0.0f) || !isfinite(Q) ||
+        !(L > 0.0f)) {
+      ok = false;
+      scale_out = __int_as_float(0x7fc00000);  // NaN: the gate sends the sim to plain integration
+    } else {
+      scale_out = Q;
+    }
+  }
+  if (live) A.p_scale[s] = scale_out;
+  if (ok) {
+#pragma unroll
+    for (int i = 0; i < kA; ++i) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) pb[3 * i + c] = dp[i][c];
+    }
+    // Features: per atom (x - x_com)/L, p/P, (p_base - p)/P, q/3,
+    // ln(m/amu)/3.5, 1; then the remaining PE fraction at the stop and n/10;
+    // zeros to the padded width.
+    const float iL = 1.0f / L, iP = 1.0f / P;
+#pragma unroll
+    for (int i = 0; i < kA; ++i) {
+      const bool on = i < n;
+      __nv_bfloat162* f2 = reinterpret_cast<__nv_bfloat162*>(f + kPerAtom * i);
+      const float v0 = on ? (x[i][0] - com[0]) * iL : 0.0f, v1 = on ? (x[i][1] - com[1]) * iL : 0.0f;
+      const float v2 = on ? (x[i][2] - com[2]) * iL : 0.0f, v3 = on ? p[i][0] * iP : 0.0f;
+      const float v4 = on ? p[i][1] * iP : 0.0f, v5 = on ? p[i][2] * iP : 0.0f;
+      const float v6 = on ? (dp[i][0] - p[i][0]) * iP : 0.0f, v7 = on ? (dp[i][1] - p[i][1]) * iP : 0.0f;
+      const float v8 = on ? (dp[i][2] - p[i][2]) * iP : 0.0f, v9 = on ? q[i] * (1.0f / 3.0f) : 0.0f;
+      const float v10 = on ? logf(static_cast<float>(ms[i] / kMassUnit)) * kLogMassScale : 0.0f;
+      const float v11 = on ? 1.0f : 0.0f;
+      f2[0] = __floats2bfloat162_rn(v0, v1);
+      f2[1] = __floats2bfloat162_rn(v2, v3);
+      f2[2] = __floats2bfloat162_rn(v4, v5);
+      f2[3] = __floats2bfloat162_rn(v6, v7);
+      f2[4] = __floats2bfloat162_rn(v8, v9);
+      f2[5] = __floats2bfloat162_rn(v10, v11);
+    }
+    __nv_bfloat162* g2 = reinterpret_cast<__nv_bfloat162*>(f + kPerAtom * kA);
+    g2[0] = __floats2bfloat162_rn(static_cast<float>(A.pe_final[s] / e0) * 20.0f, static_cast<float>(n) * 0.1f);
+#pragma unroll
+    for (int c = 1; c < (kFeat - kPerAtom * kA) / 2; ++c) g2[c] = __floats2bfloat162_rn(0.0f, 0.0f);
+
+    if (A.target) {
+      // Targets (p_true - p_base)/Q; weights w_scale / (3n) scaled by
+      // kRelRef / sqrt(rms^2 + kRelEps^2), rms = the RMS target of the sim, so
+      // the loss weighs each sim's relative rather than absolute residual.
+      const float iQ = 1.0f / Q;
+      const float* pt = A.p_true + s * 3 * kA;
+      float* t = A.target + s * kOut;
+      float* w = A.weight + s * kOut;
+      float ss = 0.0f;
+#pragma unroll
+      for (int i = 0; i < kA; ++i) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float v = i < n ? (pt[3 * i + c] - dp[i][c]) * iQ : 0.0f;
+          t[3 * i + c] = v;
+          ss += v * v;
+        }
+      }
+      const float rms2 = ss / static_cast<float>(3 * n);
+      const float wv = A.w_scale / static_cast<float>(3 * n) * kRelRef * rsqrtf(rms2 + kRelEps * kRelEps);
+#pragma unroll
+      for (int i = 0; i < kA; ++i) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) w[3 * i + c] = i < n ? wv : 0.0f;
+      }
+      for (int c = 3 * kA; c < kOut; ++c) t[c] = w[c] = 0.0f;
+    }
+  } else {
+    for (int c = 0; c < 3 * kA; ++c) pb[c] = 0.0f;
+    uint4* fz = reinterpret_cast<uint4*>(f);
+#pragma unroll
+    for (int c = 0; c < kFeat * 2 / 16; ++c) fz[c] = make_uint4(0u, 0u, 0u, 0u);
+    if (A.target && s < A.S_pad) {
+      float4* t = reinterpret_cast<float4*>(A.target + s * kOut);
+      float4* w = reinterpret_cast<float4*>(A.weight + s * kOut);
+#pragma unroll
+      for (int c = 0; c < kOut / 4; ++c) {
+        t[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+        w[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kFT, 4) closure_features_kernel(const FeatArgs A) {
   extern __shared__ __align__(16) uint8_t fsm[];
   float* spb = reinterpret_cast<float*>(fsm);              // [kFT][30]
@@ -79,201 +277,7 @@ __global__ void __launch_bounds__(kFT, 4) closure_features_kernel(const FeatArgs
   for (uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * kFT; t0 < A.S_pad;
        t0 += static_cast<uint64_t>(gridDim.x) * kFT) {
     const int rows = t0 < A.S ? static_cast<int>(A.S - t0 < kFT ? A.S - t0 : kFT) : 0;
-    const uint64_t s = t0 + tid;
-    float* pb = spb + tid * 3 * kA;
-    bf16* f = sf + tid * kFRow;
-    const float* xs = A.x + s * 3 * kA;
-    const float* ps = A.p + s * 3 * kA;
-    const double* ms = A.mass + s * kA;
-    const double* qs = A.charge + s * kA;
-    const int n = tid < rows ? A.n_atoms[s] : 0;
-    bool ok = tid < rows && n >= 2 && n <= kA && A.status[s] == CE_SIM_OK;
-    float scale_out = 0.0f;
-    float x[kA][3], p[kA][3], im[kA], q[kA], dp[kA][3];
-    float com[3] = {0.0f, 0.0f, 0.0f};
-    float P = 0.0f, Q = 0.0f, L = 0.0f;
-    double e0 = 1.0;
-    if (ok) {
-      double msum = 0.0, cx = 0.0, cy = 0.0, cz = 0.0;
-#pragma unroll
-      for (int i = 0; i < kA; ++i) {
-        const bool on = i < n;
-        const double mi = on ? ms[i] : 1.0;
-        im[i] = on ? static_cast<float>(1.0 / mi) : 0.0f;
-        q[i] = on ? static_cast<float>(qs[i]) : 0.0f;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          x[i][c] = on ? xs[3 * i + c] : 0.0f;
-          p[i][c] = on ? ps[3 * i + c] : 0.0f;
-        }
-        if (on) {
-          msum += mi;
-          cx += mi * x[i][0];
-          cy += mi * x[i][1];
-          cz += mi * x[i][2];
-        }
-      }
-      com[0] = static_cast<float>(cx / msum);
-      com[1] = static_cast<float>(cy / msum);
-      com[2] = static_cast<float>(cz / msum);
-
-      // Ballistic pair impulses from the stop to t -> infinity.
-#pragma unroll
-      for (int i = 0; i < kA; ++i) dp[i][0] = dp[i][1] = dp[i][2] = 0.0f;
-      bool bad = false;
-      const float kf = static_cast<float>(A.k);
-#pragma unroll
-      for (int i = 0; i < kA; ++i) {
-#pragma unroll
-        for (int j = i + 1; j < kA; ++j) {
-          if (j < n) {
-            const float rx = x[i][0] - x[j][0], ry = x[i][1] - x[j][1], rz = x[i][2] - x[j][2];
-            const float wx = p[i][0] * im[i] - p[j][0] * im[j];
-            const float wy = p[i][1] * im[i] - p[j][1] * im[j];
-            const float wz = p[i][2] * im[i] - p[j][2] * im[j];
-            const float a = wx * wx + wy * wy + wz * wz;
-            const float b = rx * wx + ry * wy + rz * wz;
-            const float c = rx * rx + ry * ry + rz * rz;
-            // approximate reciprocal square roots / reciprocal (a few ulp; the
-            // features are rounded to BF16 and the base is checked to 3e-5)
-            const float rsa = rsqrtf(a), rsc = rsqrtf(c);
-            const float sac = (a * rsa) * (c * rsc);
-            float g;
-            if (b >= 0.0f) {
-              g = sac + b;
-            } else {  // approaching pair: |r|^2|w|^2 - (r.w)^2 = |r x w|^2 avoids the cancellation
-              const float ux = ry * wz - rz * wy, uy = rz * wx - rx * wz, uz = rx * wy - ry * wx;
-              g = __fdividef(ux * ux + uy * uy + uz * uz, sac - b);
-            }
-            const float ig = __fdividef(1.0f, g);
-            const float I0 = ig * rsc, I1 = ig * rsa;
-            if (!(g > 0.0f) || !isfinite(I0) || !isfinite(I1)) bad = true;
-            const float fpair = kf * q[i] * q[j];
-            const float tx = fpair * (rx * I0 + wx * I1), ty = fpair * (ry * I0 + wy * I1),
-                        tz = fpair * (rz * I0 + wz * I1);
-            dp[i][0] += tx;
-            dp[i][1] += ty;
-            dp[i][2] += tz;
-            dp[j][0] -= tx;
-            dp[j][1] -= ty;
-            dp[j][2] -= tz;
-          }
-        }
-      }
-      // Base = (p + dp) rescaled to KE = E_0 (src/driver.cpp:38-42 on the ballistic state).
-      double ke = 0.0;
-#pragma unroll
-      for (int i = 0; i < kA; ++i) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          dp[i][c] += p[i][c];
-          ke += 0.5 * static_cast<double>(dp[i][c]) * dp[i][c] * im[i];
-        }
-      }
-      e0 = A.e0[s];
-      const float scl = static_cast<float>(sqrt(e0 / ke));
-      double p2 = 0.0, r2 = 0.0, q2 = 0.0;
-#pragma unroll
-      for (int i = 0; i < kA; ++i) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          dp[i][c] *= scl;
-          p2 += static_cast<double>(dp[i][c]) * dp[i][c];
-          const double d = static_cast<double>(dp[i][c]) - p[i][c];
-          q2 += d * d;
-          if (i < n) {
-            const double dx = x[i][c] - com[c];
-            r2 += dx * dx;
-          }
-        }
-      }
-      P = static_cast<float>(sqrt(p2 / n));
-      Q = static_cast<float>(sqrt(q2 / n));  // RMS per-atom size of the analytic step p -> p_base
-      L = static_cast<float>(sqrt(r2 / n));
-      if (bad || !(ke > 0.0) || !isfinite(scl) || !(P > 0.0f) || !isfinite(P) || !(Q > 0.0f) || !isfinite(Q) ||
-          !(L > 0.0f)) {
-        ok = false;
-        scale_out = __int_as_float(0x7fc00000);  // NaN: the gate sends the sim to plain integration
-      } else {
-        scale_out = Q;
-      }
-    }
-    if (tid < rows) A.p_scale[s] = scale_out;
-    if (ok) {
-#pragma unroll
-      for (int i = 0; i < kA; ++i) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) pb[3 * i + c] = dp[i][c];
-      }
-      // Features: per atom (x - x_com)/L, p/P, (p_base - p)/P, q/3,
-      // ln(m/amu)/3.5, 1; then the remaining PE fraction at the stop and n/10;
-      // zeros to the padded width.
-      const float iL = 1.0f / L, iP = 1.0f / P;
-#pragma unroll
-      for (int i = 0; i < kA; ++i) {
-        const bool on = i < n;
-        __nv_bfloat162* f2 = reinterpret_cast<__nv_bfloat162*>(f + kPerAtom * i);
-        const float v0 = on ? (x[i][0] - com[0]) * iL : 0.0f, v1 = on ? (x[i][1] - com[1]) * iL : 0.0f;
-        const float v2 = on ? (x[i][2] - com[2]) * iL : 0.0f, v3 = on ? p[i][0] * iP : 0.0f;
-        const float v4 = on ? p[i][1] * iP : 0.0f, v5 = on ? p[i][2] * iP : 0.0f;
-        const float v6 = on ? (dp[i][0] - p[i][0]) * iP : 0.0f, v7 = on ? (dp[i][1] - p[i][1]) * iP : 0.0f;
-        const float v8 = on ? (dp[i][2] - p[i][2]) * iP : 0.0f, v9 = on ? q[i] * (1.0f / 3.0f) : 0.0f;
-        const float v10 = on ? logf(static_cast<float>(ms[i] / kMassUnit)) * kLogMassScale : 0.0f;
-        const float v11 = on ? 1.0f : 0.0f;
-        f2[0] = __floats2bfloat162_rn(v0, v1);
-        f2[1] = __floats2bfloat162_rn(v2, v3);
-        f2[2] = __floats2bfloat162_rn(v4, v5);
-        f2[3] = __floats2bfloat162_rn(v6, v7);
-        f2[4] = __floats2bfloat162_rn(v8, v9);
-        f2[5] = __floats2bfloat162_rn(v10, v11);
-      }
-      __nv_bfloat162* g2 = reinterpret_cast<__nv_bfloat162*>(f + kPerAtom * kA);
-      g2[0] = __floats2bfloat162_rn(static_cast<float>(A.pe_final[s] / e0) * 20.0f, static_cast<float>(n) * 0.1f);
-#pragma unroll
-      for (int c = 1; c < (kFeat - kPerAtom * kA) / 2; ++c) g2[c] = __floats2bfloat162_rn(0.0f, 0.0f);
-
-      if (A.target) {
-        // Targets (p_true - p_base)/Q; weights w_scale / (3n) scaled by
-        // kRelRef / sqrt(rms^2 + kRelEps^2), rms = the RMS target of the sim, so
-        // the loss weighs each sim's relative rather than absolute residual.
-        const float iQ = 1.0f / Q;
-        const float* pt = A.p_true + s * 3 * kA;
-        float* t = A.target + s * kOut;
-        float* w = A.weight + s * kOut;
-        float ss = 0.0f;
-#pragma unroll
-        for (int i = 0; i < kA; ++i) {
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            const float v = i < n ? (pt[3 * i + c] - dp[i][c]) * iQ : 0.0f;
-            t[3 * i + c] = v;
-            ss += v * v;
-          }
-        }
-        const float rms2 = ss / static_cast<float>(3 * n);
-        const float wv = A.w_scale / static_cast<float>(3 * n) * kRelRef * rsqrtf(rms2 + kRelEps * kRelEps);
-#pragma unroll
-        for (int i = 0; i < kA; ++i) {
-#pragma unroll
-          for (int c = 0; c < 3; ++c) w[3 * i + c] = i < n ? wv : 0.0f;
-        }
-        for (int c = 3 * kA; c < kOut; ++c) t[c] = w[c] = 0.0f;
-      }
-    } else {
-      for (int c = 0; c < 3 * kA; ++c) pb[c] = 0.0f;
-      uint4* fz = reinterpret_cast<uint4*>(f);
-#pragma unroll
-      for (int c = 0; c < kFeat * 2 / 16; ++c) fz[c] = make_uint4(0u, 0u, 0u, 0u);
-      if (A.target && s < A.S_pad) {
-        float4* t = reinterpret_cast<float4*>(A.target + s * kOut);
-        float4* w = reinterpret_cast<float4*>(A.weight + s * kOut);
-#pragma unroll
-        for (int c = 0; c < kOut / 4; ++c) {
-          t[c] = make_float4(0.f, 0.f, 0.f, 0.f);
-          w[c] = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-      }
-    }
+    feat_one(A, t0 + tid, tid < rows, spb + tid * 3 * kA, sf + tid * kFRow);
     __syncthreads();
     // coalesced stores of the tile: feature rows (all 128, padded rows zero) and base momenta
     {
@@ -463,14 +467,15 @@ int launch_features(uint64_t S, const ce_mixed_batch* in, double k, const ce_clo
   A.weight = weight;
   int dev = 0;
   cudaGetDevice(&dev);
-  if (cudaFuncSetAttribute(closure_features_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           static_cast<int>(kFeatSmem)) != cudaSuccess)
-    return CE_ERR_CUDA;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const uint64_t tiles = A.S_pad / kFT;
   const uint64_t cap = static_cast<uint64_t>(sms) * 4;
-  closure_features_kernel<<<static_cast<unsigned>(tiles < cap ? tiles : cap), kFT, kFeatSmem, s>>>(A);
+  const unsigned grid = static_cast<unsigned>(tiles < cap ? tiles : cap);
+  if (cudaFuncSetAttribute(closure_features_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(kFeatSmem)) != cudaSuccess)
+    return CE_ERR_CUDA;
+  closure_features_kernel<<<grid, kFT, kFeatSmem, s>>>(A);
   return cudaGetLastError() == cudaSuccess ? CE_OK : CE_ERR_CUDA;
 }
 

@@ -179,6 +179,22 @@ def test_serve_reject_all_equals_plain_and_accept_all(ce, engine, cl):
     ok[5] = False
     np.testing.assert_allclose(_np(out2["ker"])[ok], _np(plain["ker"])[ok], rtol=1e-5)
     assert _np(out2["steps"])[ok].mean() < 0.75 * _np(plain["steps"])[ok].mean()
+    # the serving pipeline equals the step-by-step public calls bit for bit
+    loose = cl.run_loose(engine, b, _cfg(ce))
+    d = cl.features(b, loose)
+    o_net = cl.net_forward(net, d["feats"])
+    mom = torch.zeros((b.S, 10, 3), device="cuda")
+    fbf = torch.zeros(b.S, dtype=torch.uint8, device="cuda")
+    cnt = torch.zeros(2, dtype=torch.int64, device="cuda")
+    o = ce.CeOutputs(mom.data_ptr())
+    lib = ce.load_library()
+    gate = ce.CeClosureGate(inf, inf, inf)
+    assert lib.ce_closure_apply(b.S, C.byref(b.c()), C.byref(cl.closure_state(loose)),
+                                C.c_void_p(loose["steps"].data_ptr()), C.c_void_p(d["p_base"].data_ptr()),
+                                C.c_void_p(d["p_scale"].data_ptr()), C.c_void_p(o_net.data_ptr()), C.byref(gate),
+                                C.byref(o), C.c_void_p(fbf.data_ptr()), C.c_void_p(cnt.data_ptr()), None) == 0
+    torch.cuda.synchronize()
+    assert torch.equal(mom[torch.from_numpy(ok).cuda()], out2["momenta"][torch.from_numpy(ok).cuda()])
 
 
 def test_trained_network_beats_analytic_and_redistribution(ce, engine, cl):
