@@ -945,8 +945,10 @@ def main():
     cfg = ce.RunConfig(rtol=rtol, atol=atol, pe_stop_fraction=pes, precision_mode=args.mode)
 
     sp = importlib.import_module("coulomb_explosion_b200.sampling")
+    rp = importlib.import_module("coulomb_explosion_b200.replicas")
     # Seeded Philox geometries; rank r integrates sims [r*S, (r+1)*S) of one population.
-    pos_host, _, flags = sp.sample_ball_host(mol, S, seed=SEED, first_sim=rank * S)
+    first, _ = rp.shard(rank, world, S)
+    pos_host, _, flags = sp.sample_ball_host(mol, S, seed=SEED, first_sim=first)
     assert not flags.any()
     eng = ce.Engine(dev.index)
     eng.set_molecule(mol.masses_me, mol.charge_array)
@@ -989,12 +991,8 @@ def main():
     if world > 1:
         torch.distributed.barrier()
     per = [a.elapsed_time(b) for a, b in ev]  # ms per launch (flush excluded)
-    total_ms = float(sum(per))
-    if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * S * args.steps / (total_ms / 1e3)
+    total_ms = rp.max_over_ranks(float(sum(per)), dev)
+    value = rp.aggregate_rate(world, S, args.steps, total_ms)
 
     # ---- results of the last step: accuracy and FLOP accounting ----
     mom = mom_d.cpu().numpy()
@@ -1022,12 +1020,8 @@ def main():
     for _ in range(e2e_steps):
         rc = eng.lib.ce_run(eng.h, S, ctypes.c_void_p(pin_pos.data_ptr()), ctypes.byref(cc), ctypes.byref(hout))
         assert rc == 0, eng.lib.ce_last_error(eng.h)
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * S * e2e_steps / e2e_s
+    e2e_s = rp.max_over_ranks(time.perf_counter() - t0, dev)
+    e2e_value = rp.aggregate_rate(world, S, e2e_steps, e2e_s * 1e3)
     h2d = S * n * 3 * 4
     d2h = S * (n * 3 * 4 + 8 + 4 + 1)
 
