@@ -1,8 +1,10 @@
-// probe.cu -- FP32 FMA throughput probe (include/ce_probe.h).
+// probe.cu -- FP32 FMA throughput probe and the bounded-wait check
+// (include/ce_probe.h).
 #include <cuda_runtime.h>
 
 #include "ce_gpu.h"
 #include "ce_probe.h"
+#include "umma.cuh"
 
 namespace {
 
@@ -23,7 +25,35 @@ __global__ void __launch_bounds__(256) ffma_probe(float* out, float b, float c) 
   if (s == 1234.5f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;  // keeps the chains live
 }
 
+// An mbarrier that nothing arrives on, waited for with the same bounded poll
+// the tensor-core kernels use: the wait must give up, record its code and let
+// the kernel finish.
+__global__ void bounded_wait_probe(int* err, uint32_t spins) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) ce::umma::mbar_init(&bar, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) ce::umma::mbar_wait(&bar, 0u, err, 7, spins);
+}
+
 }  // namespace
+
+extern "C" int ce_probe_bounded_wait(int device, unsigned spins, int* code_out) {
+  if (!code_out || spins == 0 || spins > (1u << 20)) return CE_ERR_INVALID;
+  *code_out = 0;
+  if (cudaSetDevice(device) != cudaSuccess) return CE_ERR_NO_DEVICE;
+  int* d = nullptr;
+  if (cudaMalloc(&d, sizeof(int)) != cudaSuccess) return CE_ERR_CUDA;
+  int rc = CE_OK;
+  if (cudaMemset(d, 0, sizeof(int)) != cudaSuccess) rc = CE_ERR_CUDA;
+  if (rc == CE_OK) {
+    bounded_wait_probe<<<1, 32>>>(d, spins);
+    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess ||
+        cudaMemcpy(code_out, d, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+      rc = CE_ERR_CUDA;
+  }
+  cudaFree(d);
+  return rc;
+}
 
 extern "C" int ce_probe_fp32_peak(int device, double* tflops_out) {
   if (!tflops_out) return CE_ERR_INVALID;

@@ -28,7 +28,7 @@
 namespace ce {
 namespace umma {
 
-constexpr uint32_t kWaitSpins = 1u << 22;
+constexpr uint32_t kWaitSpins = 1u << 18;  // ~4 us per poll on B200: about one second
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -54,10 +54,12 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
-// Wait for the phase with parity `parity` of `bar` to complete; bounded.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code) {
+// Wait for the phase with parity `parity` of `bar` to complete; bounded by
+// `spins` polls, after which `code` is recorded in *err and false returned.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code,
+                                          uint32_t spins = kWaitSpins) {
   const uint32_t a = smem_addr(bar);
-  for (uint32_t i = 0; i < kWaitSpins; ++i) {
+  for (uint32_t i = 0; i < spins; ++i) {
     uint32_t done = 0;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"

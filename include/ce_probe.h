@@ -18,6 +18,13 @@ extern "C" {
  * negative CE_ERR_* code. */
 int ce_probe_fp32_peak(int device, double* tflops_out);
 
+/* Failure-detection check of the bounded waits the tensor-core kernels use
+ * (no counterpart in the reference): one kernel waits on an mbarrier that
+ * nothing arrives on, with at most `spins` polls (1 .. 2^20); the wait must give
+ * up and record its error code (7) in *code_out while the context stays usable.
+ * Returns 0 or a negative CE_ERR_* code. */
+int ce_probe_bounded_wait(int device, unsigned spins, int* code_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -149,3 +149,26 @@ def test_forward_limits(ce):
         assert lib.ce_mlp_check(h, None) == 0
     finally:
         lib.ce_mlp_destroy(h)
+
+
+def test_bounded_wait_gives_up_and_context_survives(ce, engine, wl):
+    """Failure detection of the tensor-core kernels: a wait on an mbarrier that
+    nothing arrives on gives up after its poll budget, records its code, and the
+    context keeps working (a plain integration runs afterwards)."""
+    import time
+
+    lib = ce.load_library()
+    code = C.c_int(-1)
+    timings = {}
+    for spins in (1000, 20000):
+        t0 = time.perf_counter()
+        assert lib.ce_probe_bounded_wait(0, spins, C.byref(code)) == 0
+        timings[spins] = time.perf_counter() - t0
+        assert code.value == 7
+    print(f"bounded wait: 1000 polls {timings[1000] * 1e3:.2f} ms, 20000 polls {timings[20000] * 1e3:.2f} ms")
+    assert lib.ce_probe_bounded_wait(0, 0, C.byref(code)) == ce.CE_ERR_INVALID
+    mol = wl.CH4
+    engine.set_molecule(mol.masses_me, mol.charge_array)
+    pos = wl.sample_molecule(mol, 64, seed=4).astype(np.float32)
+    r = engine.run(pos, ce.RunConfig(rtol=1e-6, atol=1e-7, pe_stop_fraction=1e-7))
+    assert np.all(r.status == 0)
