@@ -464,6 +464,10 @@ def run_closure(args):
     # ---- serving: held-out sims, closure vs plain
     sb = cl.sample_mixed_device(S, seed=seed, first_sim=S_train)
     eng.reserve_mixed(S)
+    # launch shape and schedule picked by the autotuner; plain RK45 and the
+    # closure's two integration passes all run with them
+    _, sched = eng.autotune_mixed(min(S, 1_000_000), sb.c(), cfg)
+    eng.reserve_mixed(S)
     clo = cl.Closure(eng, net, S)
 
     def outs():
@@ -495,7 +499,7 @@ def run_closure(args):
         return sum(a.elapsed_time(b) for a, b in ev) / args.steps
 
     with ClockSampler(0) as clk:
-        ms_plain = timed(lambda: eng.run_mixed_device(S, batch_c, cfg, c_op, ce.CE_SCHEDULE_ONE_LAUNCH, stream.cuda_stream))
+        ms_plain = timed(lambda: eng.run_mixed_device(S, batch_c, cfg, c_op, sched, stream.cuda_stream))
         ms_clo = timed(lambda: clo.serve(sb, cfg, gate, c_oc, loose_pe_stop=args.loose_pe_stop,
                                          stream=stream.cuda_stream, cbatch=batch_c))
     acc, fbk = clo.counts()
@@ -511,10 +515,9 @@ def run_closure(args):
     lo_st = torch.empty(S, dtype=torch.uint8, device=dev)
     c_lo = ce.CeOutputs(lo_m.data_ptr(), None, lo_s.data_ptr(), lo_st.data_ptr(), None, None, lo_d[1].data_ptr(),
                         None, lo_x.data_ptr(), lo_d[2].data_ptr())
-    ms_loose = timed(lambda: eng.run_mixed_device(S, batch_c, lcfg, c_lo, ce.CE_SCHEDULE_ONE_LAUNCH,
-                                                  stream.cuda_stream))
+    ms_loose = timed(lambda: eng.run_mixed_device(S, batch_c, lcfg, c_lo, sched, stream.cuda_stream))
     fb_batch = ce.CeMixedBatch(fbf.data_ptr(), sb.mass.data_ptr(), sb.charge.data_ptr(), sb.pos.data_ptr())
-    ms_fb = timed(lambda: eng.run_mixed_device(S, fb_batch, cfg, c_lo, ce.CE_SCHEDULE_ONE_LAUNCH, stream.cuda_stream))
+    ms_fb = timed(lambda: eng.run_mixed_device(S, fb_batch, cfg, c_lo, sched, stream.cuda_stream))
     del lo_m, lo_x, lo_d, lo_s, lo_st
 
     # network forward alone (tensor-core roofline of the learned part)
@@ -574,6 +577,7 @@ def run_closure(args):
                                "U{H,C,N,O,S}, q ~ U{+1,+2,+3}, radius 2.0 N^(1/3), min pair 0.5, Philox on device)",
                    "rtol": rtol, "atol": atol, "pe_stop": pes, "loose_pe_stop": args.loose_pe_stop,
                    "network": f"{ce.CLOSURE_FEATURES} -> {net.depth} x {net.hidden} SiLU -> 32, bf16 weights/activations, f32 accumulate",
+                   "schedule": "per-size launches" if sched == ce.CE_SCHEDULE_PER_SIZE else "one persistent launch",
                    "l2": "flushed between timed steps (256 MiB write, outside the events)"},
         "plain": {"value": S / (ms_plain / 1e3), "unit": UNIT, "ms_per_step": ms_plain,
                   "mean_steps": float(op["steps"].double().mean())},
@@ -691,6 +695,8 @@ def run_stream(args):
         d["host"] = {k: torch.empty(d[k].shape, dtype=d[k].dtype, pin_memory=True)
                      for k in ("momenta", "ker", "steps", "status")}
         slots.append(d)
+    _, sched = eng.autotune_mixed(C_, slots[0]["cb"], cfg)
+    eng.reserve_mixed(C_)
     clo = cl.Closure(eng, net, C_)
     compute = torch.cuda.Stream(device=dev)
     side = torch.cuda.Stream(device=dev)
@@ -706,13 +712,13 @@ def run_stream(args):
             if mode == "closure":
                 clo.serve(d["batch"], cfg, gate, d["out"], loose_pe_stop=args.loose_pe_stop, stream=cs, cbatch=d["cb"])
             else:
-                eng.run_mixed_device(C_, d["cb"], cfg, d["out"], ce.CE_SCHEDULE_ONE_LAUNCH, cs)
+                eng.run_mixed_device(C_, d["cb"], cfg, d["out"], sched, cs)
             torch.cuda.synchronize()
             eng.graph_begin(cs)
             if mode == "closure":
                 clo.serve(d["batch"], cfg, gate, d["out"], loose_pe_stop=args.loose_pe_stop, stream=cs, cbatch=d["cb"])
             else:
-                eng.run_mixed_device(C_, d["cb"], cfg, d["out"], ce.CE_SCHEDULE_ONE_LAUNCH, cs)
+                eng.run_mixed_device(C_, d["cb"], cfg, d["out"], sched, cs)
             graphs.append(eng.graph_end(cs))
         return graphs
 
