@@ -167,6 +167,57 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(const GemmArgs g) {
       umma::tmem_ld16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0), r);
       umma::tmem_wait_ld();
       if (row >= g.M) continue;
+      const int nb = n0 + c0;
+      if (nb + 16 <= g.N && g.epi != kEpiAtomicF32T && g.epi != kEpiFwdLinearF32) {
+        // full 16-column chunk: vector stores (16 B of BF16 / float4 atomics)
+        if (g.epi == kEpiAtomicF32) {
+          float4* c = reinterpret_cast<float4*>(g.C + static_cast<size_t>(row) * g.ldc + nb);
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            atomicAdd(c + q, make_float4(__uint_as_float(r[4 * q]), __uint_as_float(r[4 * q + 1]),
+                                         __uint_as_float(r[4 * q + 2]), __uint_as_float(r[4 * q + 3])));
+          continue;
+        }
+        uint32_t y[8], z[8];
+        if (g.epi == kEpiBwdAct) {
+          const uint4* zi = reinterpret_cast<const uint4*>(g.Zin + static_cast<size_t>(row) * g.ldz + nb);
+          const uint4 z0 = zi[0], z1 = zi[1];
+          const uint32_t zw[8] = {z0.x, z0.y, z0.z, z0.w, z1.x, z1.y, z1.z, z1.w};
+#pragma unroll
+          for (int q = 0; q < 8; ++q) z[q] = zw[q];
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          bf16 o0, o1;
+          const float a0 = __uint_as_float(r[2 * q]), a1 = __uint_as_float(r[2 * q + 1]);
+          if (g.epi == kEpiFwdAct) {
+            const bf16 z0 = __float2bfloat16(a0 + g.bias[nb + 2 * q]);
+            const bf16 z1 = __float2bfloat16(a1 + g.bias[nb + 2 * q + 1]);
+            z[q] = static_cast<uint32_t>(__bfloat16_as_ushort(z0)) | (static_cast<uint32_t>(__bfloat16_as_ushort(z1)) << 16);
+            o0 = silu_bf16(z0);
+            o1 = silu_bf16(z1);
+          } else if (g.epi == kEpiBwdAct) {
+            const float za = __bfloat162float(__ushort_as_bfloat16(static_cast<unsigned short>(z[q] & 0xffffu)));
+            const float zb = __bfloat162float(__ushort_as_bfloat16(static_cast<unsigned short>(z[q] >> 16)));
+            const float sa = sigmoidf_(za), sb = sigmoidf_(zb);
+            o0 = __float2bfloat16(a0 * (sa * (1.0f + za * (1.0f - sa))));
+            o1 = __float2bfloat16(a1 * (sb * (1.0f + zb * (1.0f - sb))));
+          } else {
+            o0 = __float2bfloat16(a0);
+            o1 = __float2bfloat16(a1);
+          }
+          y[q] = static_cast<uint32_t>(__bfloat16_as_ushort(o0)) | (static_cast<uint32_t>(__bfloat16_as_ushort(o1)) << 16);
+        }
+        uint4* yo = reinterpret_cast<uint4*>(g.Y + static_cast<size_t>(row) * g.ldy + nb);
+        yo[0] = make_uint4(y[0], y[1], y[2], y[3]);
+        yo[1] = make_uint4(y[4], y[5], y[6], y[7]);
+        if (g.epi == kEpiFwdAct) {
+          uint4* zo = reinterpret_cast<uint4*>(g.Zout + static_cast<size_t>(row) * g.ldz + nb);
+          zo[0] = make_uint4(z[0], z[1], z[2], z[3]);
+          zo[1] = make_uint4(z[4], z[5], z[6], z[7]);
+        }
+        continue;
+      }
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
         const int n = n0 + c0 + j;
@@ -221,13 +272,17 @@ __global__ void mse_grad_kernel(const float* out, const float* t, const float* w
   if ((threadIdx.x & 31) == 0) atomicAdd(loss, acc);
 }
 
-// db[n] = sum_rows dZ[row][n].
+// db[n] += sum_rows dZ[row][n]; blockIdx.y takes a slice of kColRows rows, so
+// the rows are summed in parallel (one atomic per column and slice).
+constexpr int kColRows = 256;
 __global__ void colsum_kernel(const bf16* dz, int rows, int cols, int ld, float* db) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= cols) return;
+  const int r0 = blockIdx.y * kColRows, r1 = min(rows, r0 + kColRows);
   float s = 0.0f;
-  for (int r = 0; r < rows; ++r) s += __bfloat162float(dz[static_cast<size_t>(r) * ld + n]);
-  db[n] += s;
+#pragma unroll 8
+  for (int r = r0; r < r1; ++r) s += __bfloat162float(dz[static_cast<size_t>(r) * ld + n]);
+  atomicAdd(db + n, s);
 }
 
 // Adam (Kingma & Ba 2015) on FP32 master weights; refreshes the BF16 copy.
@@ -660,7 +715,8 @@ int backward(ce_mlp* net, const bf16* x, const float* target, const float* w, ui
     }
     int rc = launch_gemm<true, true>(net, g, s, splits);
     if (rc != CE_OK) return rc;
-    colsum_kernel<<<(fo + 127) / 128, 128, 0, s>>>(dcur, static_cast<int>(B), fo, dcur_ld, net->g + net->b_off[l]);
+    colsum_kernel<<<dim3((fo + 127) / 128, static_cast<unsigned>((B + kColRows - 1) / kColRows)), 128, 0, s>>>(
+        dcur, static_cast<int>(B), fo, dcur_ld, net->g + net->b_off[l]);
     if (l == 0) break;
     // d(pre-activation of layer l-1) = (dcur W_l) * silu'(Z_{l-1})
     bf16* dnext = (dcur == net->dA) ? net->dB : net->dA;
