@@ -6,7 +6,7 @@ The reference's only closure is the uniform velocity rescale at the stop
 (src/driver.cpp:38-42). Here every sim is integrated to a loose stop
 (PE <= 5% PE_0), the closed-form straight-line pair impulse to t -> infinity
 plus that rescale gives a base, and a BF16 MLP (128 -> 4 x 256 SiLU -> 32)
-predicts the remaining correction in units of the base's RMS atom momentum.
+predicts the remaining correction in units of the analytic step's size.
 Training targets are the engine's own fully converged momenta on the same
 inputs. Device memory is held in torch tensors; every computation on the
 closure path runs in libce_gpu.so.
@@ -282,7 +282,8 @@ def rel_err(p, p_ref):
 
 
 def predict(batch: DeviceBatch, base: dict, out) -> object:
-    """Corrected momenta p_base + P * out (before the gate's projection)."""
+    """Corrected momenta p_base + Q * out (before the gate's projection); Q is
+    p_scale, the size of the analytic step."""
     S = batch.S
     return base["p_base"] + base["p_scale"][:, None, None] * out[:S, :3 * MAX_ATOMS].view(S, MAX_ATOMS, 3) * (
         (_torch().arange(MAX_ATOMS, device=batch.n.device)[None, :] < batch.n[:, None].long())[..., None])
@@ -322,7 +323,7 @@ class TrainReport:
 
 
 def train(net: Network, ts: TrainingSet, epochs: int = 20, minibatch: int = 8192, lr: float = 1e-3,
-          lr_final: float = 1e-5, seed: int = 7, train_rows=None, log_every: int = 0) -> TrainReport:
+          lr_final: float = 1e-5, seed: int = 7, train_rows=None) -> TrainReport:
     """Adam with cosine decay over `epochs` passes of a seeded shuffle of the
     training rows; one ce_mlp_train_step per minibatch (no host sync inside)."""
     import time
