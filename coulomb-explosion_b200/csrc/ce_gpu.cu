@@ -26,9 +26,10 @@ ce_tuning effective_tuning(const ce_engine* e, int n) {
   const ce_tuned_entry& a = e->tuned_fixed[n];
   if (t.block_threads == 0) t.block_threads = a.valid && a.t.block_threads ? a.t.block_threads : 128;
   if (t.blocks_per_sm == 0 && a.valid) t.blocks_per_sm = a.t.blocks_per_sm;
-  if (t.refill_threshold == 0) t.refill_threshold = a.valid && a.t.refill_threshold ? a.t.refill_threshold : 1;
+  if (t.refill_threshold == 0 && a.valid) t.refill_threshold = a.t.refill_threshold;
   if (t.lanes_per_sim == 0) t.lanes_per_sim = a.valid && a.t.lanes_per_sim ? a.t.lanes_per_sim : (n >= 2 ? n : 1);
   if (n < 2) t.lanes_per_sim = 1;
+  if (t.refill_threshold == 0) t.refill_threshold = ce::default_refill(n, t.lanes_per_sim);
   return t;
 }
 

@@ -116,12 +116,14 @@ __global__ void bucket_scatter_kernel(const uint8_t* __restrict__ n_per, uint64_
   }
 }
 
+// Launch shape of the mixed path; refill_threshold stays 0 ("per size") unless
+// set by the caller or the autotuner.
 ce_tuning mixed_tuning(const ce_engine* e) {
   ce_tuning t = e->tuning;
   const ce_tuned_entry& a = e->tuned_mixed;
   if (t.block_threads == 0) t.block_threads = a.valid && a.t.block_threads ? a.t.block_threads : 128;
   if (t.blocks_per_sm == 0 && a.valid) t.blocks_per_sm = a.t.blocks_per_sm;
-  if (t.refill_threshold == 0) t.refill_threshold = a.valid && a.t.refill_threshold ? a.t.refill_threshold : 1;
+  if (t.refill_threshold == 0 && a.valid) t.refill_threshold = a.t.refill_threshold;
   return t;
 }
 
@@ -195,7 +197,7 @@ int run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double 
   const ce_tuning t = mixed_tuning(e);
 
   ce::RunParams P{};
-  ce::fill_run_params(P, cfg, out, t.refill_threshold);
+  ce::fill_run_params(P, cfg, out, t.refill_threshold > 0 ? t.refill_threshold : 1);
   P.skip_empty = skip_empty ? 1 : 0;
   P.pos = in->pos;
   P.cursor = nullptr;
@@ -239,7 +241,9 @@ int run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double 
       }
       const uint64_t sims_per_block = static_cast<uint64_t>(block / 32) * (32 / n);
       const uint64_t grid = std::min<uint64_t>(static_cast<uint64_t>(e->sms) * per_sm, (S + sims_per_block - 1) / sims_per_block);
-      fn<<<static_cast<unsigned>(std::max<uint64_t>(grid, 1)), block, smem, s>>>(P, X, B);
+      ce::RunParams Pn = P;
+      if (t.refill_threshold == 0) Pn.refill_threshold = ce::default_refill(n, n);
+      fn<<<static_cast<unsigned>(std::max<uint64_t>(grid, 1)), block, smem, s>>>(Pn, X, B);
       ++launches;
     }
   }
