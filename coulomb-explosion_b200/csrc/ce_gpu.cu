@@ -168,12 +168,11 @@ int ce_run_device(ce_engine* e, uint64_t S, const float* pos, const ce_run_confi
                                     : ce::select_fixed_kernel(e->n, cfg->precision_mode);
   if (!fn) return ce::fail(e, CE_ERR_INVALID, "ce_run: no kernel for this atom count");
   const int block = t.block_threads;
-  const size_t smem = atom ? ce::atom_smem_bytes(block) : 0;
   const uint64_t sims_per_block =
       atom ? static_cast<uint64_t>(block / 32) * static_cast<uint64_t>(32 / e->n) : static_cast<uint64_t>(block);
   int per_sm = t.blocks_per_sm;
   if (per_sm == 0) {
-    st = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem);
+    st = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, 0);
     if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     if (per_sm < 1) per_sm = 1;
   }
@@ -189,7 +188,7 @@ int ce_run_device(ce_engine* e, uint64_t S, const float* pos, const ce_run_confi
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   st = cudaMemsetAsync(e->d_cursor, 0, sizeof(unsigned long long), s);
   if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMemsetAsync(cursor)");
-  fn<<<static_cast<unsigned>(grid), block, smem, s>>>(P, e->mol);
+  fn<<<static_cast<unsigned>(grid), block, 0, s>>>(P, e->mol);
   st = cudaGetLastError();
   if (st != cudaSuccess) return ce::cuda_fail(e, st, "rk45 kernel launch");
   e->last_launches = 1;

@@ -132,9 +132,4 @@ inline int default_refill(int n, int lanes_per_sim) {
   return g / 3 > 1 ? g / 3 : 1;
 }
 
-// Dynamic shared memory of a lane-per-atom block.
-inline size_t atom_smem_bytes(int block) {
-  return static_cast<size_t>(block / 32) * kAtomBufSlots * sizeof(float4);
-}
-
 }  // namespace ce

@@ -216,26 +216,25 @@ int run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double 
   int launches = 3;
 
   const int block = t.block_threads;
-  const size_t smem = ce::atom_smem_bytes(block);
   if (schedule == CE_SCHEDULE_ONE_LAUNCH) {
     const ce::MixedKernelFn fn = ce::select_mixed_kernel(0, cfg->precision_mode);
     int per_sm = t.blocks_per_sm;
     if (per_sm == 0) {
-      st = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem);
+      st = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, 0);
       if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
       if (per_sm < 1) per_sm = 1;
     }
     // Enough groups for the smallest molecules, never more than one wave.
     const uint64_t sims_per_block = static_cast<uint64_t>(block / 32) * (32 / 2);
     const uint64_t grid = std::min<uint64_t>(static_cast<uint64_t>(e->sms) * per_sm, (S + sims_per_block - 1) / sims_per_block);
-    fn<<<static_cast<unsigned>(std::max<uint64_t>(grid, 1)), block, smem, s>>>(P, X, B);
+    fn<<<static_cast<unsigned>(std::max<uint64_t>(grid, 1)), block, 0, s>>>(P, X, B);
     ++launches;
   } else {
     for (int n = CE_MAX_ATOMS; n >= 2; --n) {
       const ce::MixedKernelFn fn = ce::select_mixed_kernel(n, cfg->precision_mode);
       int per_sm = t.blocks_per_sm;
       if (per_sm == 0) {
-        st = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem);
+        st = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, 0);
         if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
         if (per_sm < 1) per_sm = 1;
       }
@@ -243,7 +242,7 @@ int run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double 
       const uint64_t grid = std::min<uint64_t>(static_cast<uint64_t>(e->sms) * per_sm, (S + sims_per_block - 1) / sims_per_block);
       ce::RunParams Pn = P;
       if (t.refill_threshold == 0) Pn.refill_threshold = ce::default_refill(n, n);
-      fn<<<static_cast<unsigned>(std::max<uint64_t>(grid, 1)), block, smem, s>>>(Pn, X, B);
+      fn<<<static_cast<unsigned>(std::max<uint64_t>(grid, 1)), block, 0, s>>>(Pn, X, B);
       ++launches;
     }
   }

@@ -7,11 +7,9 @@
 // x, v and six stage accelerations (~3x fewer registers than a whole sim per
 // thread), so occupancy is high and N = 10 needs no spills.
 //
-// Per force evaluation a lane publishes (x, y, z) to its slot of a per-warp
-// shared-memory buffer (three rotating buffers, one __syncwarp per evaluation)
-// and reads its partners with 16-byte loads; the partner set is fixed per lane,
-// so there is no self pair, and the lane's pair constants k q_i q_j sit in
-// registers. Each pair term is evaluated by one lane of the pair and handed to
+// Per force evaluation a lane reads its partners' positions from their lanes
+// with register shuffles; the partner set is fixed per lane, so there is no
+// self pair, and the lane's pair constants k q_i q_j sit in registers. Each pair term is evaluated by one lane of the pair and handed to
 // the other with shuffles (Newton's third law, see lane_force). Sums over a simulation (error norm, potential, kinetic energy,
 // Hairer norms) are gathered with N shuffles in a fixed order, so every lane of
 // a group holds the bit-identical value and takes the same accept/reject and
@@ -19,7 +17,7 @@
 //
 // Control flow is warp-uniform: every lane executes every attempt (lanes whose
 // simulation is finished, or that carry no atom, compute on stale data and
-// commit nothing), which keeps the shared-memory exchange fully synchronised.
+// commit nothing), which keeps the full-warp shuffles of the exchange valid.
 // The stage loop is unrolled: a lane carries three components, so the six
 // force loops stay small and every coefficient is a compile-time operand.
 //
@@ -40,7 +38,6 @@
 namespace ce {
 
 constexpr int kMixedStride = CE_MAX_ATOMS;  // atoms per sim row in the mixed layout
-constexpr int kAtomBufSlots = 96;           // float4 per warp: three 32-slot buffers
 
 template <int N>
 struct AtomShape {
@@ -117,11 +114,12 @@ struct AtomLane {
   unsigned long long sim;
 };
 
-// One force evaluation for every lane of the warp: publish xs, read partners,
-// accumulate a_i and (optionally) this lane's share of the potential. `which`
-// (0..2) selects one of three 32-slot buffers; consecutive calls always use
-// different buffers, so a lane never overwrites a slot that a slower lane is
-// still reading from the previous evaluation.
+// One force evaluation for every lane of the warp: read the partners'
+// positions from their lanes with register shuffles, accumulate a_i and
+// (optionally) this lane's share of the potential. Every lane of the warp takes
+// part (the shuffles are full-warp), so no shared memory or __syncwarp is
+// involved; a shuffle costs one shared-memory-pipe wavefront, against four
+// (plus bank conflicts where a group wraps) for a 16-byte shared-memory read.
 //
 // Newton's third law across lanes: partner d of lane i is atom i+1+d (mod N).
 // Lane i evaluates the pair terms f_d = k q_i q_j r / |r|^3 (r = x_i - x_j) for
@@ -131,14 +129,11 @@ struct AtomLane {
 // two lanes symmetrically; both evaluate it, each taking half of its potential.
 // Every pair's potential is counted once: the group sum of pe_part is PE.
 template <int N, typename Acc>
-__device__ __forceinline__ void lane_force(float4* __restrict__ buf, int which, int slot, const int (&nbr)[N - 1],
-                                           const int (&recv)[N - 1], const float (&pcv)[N - 1], const V3& xs,
-                                           const AtomConsts& ac, bool want_pe, V3& a, Acc& pe_part) {
+__device__ __forceinline__ void lane_force(const int (&nbr)[N - 1], const int (&recv)[N - 1],
+                                           const float (&pcv)[N - 1], const V3& xs, const AtomConsts& ac,
+                                           bool want_pe, V3& a, Acc& pe_part) {
   constexpr int H = (N - 1) / 2;
   constexpr bool kOpp = (N % 2) == 0;
-  float4* b = buf + which * 32;
-  b[slot] = make_float4(xs.xy.x, xs.xy.y, xs.z, 0.0f);
-  __syncwarp();
   float2 axy = make_float2(0.0f, 0.0f);
   float az = 0.0f;
   float2 fxy[H > 0 ? H : 1];
@@ -146,9 +141,11 @@ __device__ __forceinline__ void lane_force(float4* __restrict__ buf, int which, 
   Acc pe = Acc(0);
 #pragma unroll
   for (int d = 0; d < H; ++d) {
-    const float4 o = b[nbr[d]];
-    const float2 rxy = __ffma2_rn(bcast(-1.0f), make_float2(o.x, o.y), xs.xy);
-    const float rz = xs.z - o.z;
+    const float ox = __shfl_sync(0xffffffffu, xs.xy.x, nbr[d]);
+    const float oy = __shfl_sync(0xffffffffu, xs.xy.y, nbr[d]);
+    const float oz = __shfl_sync(0xffffffffu, xs.z, nbr[d]);
+    const float2 rxy = __ffma2_rn(bcast(-1.0f), make_float2(ox, oy), xs.xy);
+    const float rz = xs.z - oz;
     const float d2 = fmaf(rxy.x, rxy.x, fmaf(rxy.y, rxy.y, rz * rz));
     const float rinv = rsqrtf(d2);
     const float u = pcv[d] * rinv;  // k q_i q_j / r
@@ -161,9 +158,11 @@ __device__ __forceinline__ void lane_force(float4* __restrict__ buf, int which, 
   }
   if (kOpp) {
     constexpr int d = N / 2 - 1;
-    const float4 o = b[nbr[d]];
-    const float2 rxy = __ffma2_rn(bcast(-1.0f), make_float2(o.x, o.y), xs.xy);
-    const float rz = xs.z - o.z;
+    const float ox = __shfl_sync(0xffffffffu, xs.xy.x, nbr[d]);
+    const float oy = __shfl_sync(0xffffffffu, xs.xy.y, nbr[d]);
+    const float oz = __shfl_sync(0xffffffffu, xs.z, nbr[d]);
+    const float2 rxy = __ffma2_rn(bcast(-1.0f), make_float2(ox, oy), xs.xy);
+    const float rz = xs.z - oz;
     const float d2 = fmaf(rxy.x, rxy.x, fmaf(rxy.y, rxy.y, rz * rz));
     const float rinv = rsqrtf(d2);
     const float u = pcv[d] * rinv;
@@ -228,7 +227,7 @@ __device__ __forceinline__ void atom_finalize(const AtomLane<N, MODE>& s, int st
 template <int N, int MODE, bool MIXED>
 __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M, const MixedIn& X,
                                           unsigned long long* cursor, unsigned long long count,
-                                          const uint32_t* perm, float4* buf) {
+                                          const uint32_t* perm) {
   using L = AtomLane<N, MODE>;
   using Acc = typename L::Acc;
   constexpr int G = AtomShape<N>::G;
@@ -327,7 +326,7 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
       }
       V3 a0;
       Acc peh;
-      lane_force<N, Acc>(buf, 2, lane, nbr, recv, pcv, s.x, ac, true, a0, peh);  // stages use buffers 1, 0, 1, ...
+      lane_force<N, Acc>(nbr, recv, pcv, s.x, ac, true, a0, peh);
       const Acc pe0 = gsum<N>(peh, base);
       // Hairer norms from rest (sv = atol, probe accelerations = k1).
       float d0p = 0.0f, d1p = 0.0f;
@@ -400,7 +399,7 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
       } else {
         xs = v3_add(s.x, inc);
       }
-      lane_force<N, Acc>(buf, si & 1, lane, nbr, recv, pcv, xs, ac, si == 6, a, pe_half);
+      lane_force<N, Acc>(nbr, recv, pcv, xs, ac, si == 6, a, pe_half);
       if (si <= 5) s.k[si] = a;
     }
     // Stage 7 done: xs = x_new, a = k7. Velocity update and error estimate.
@@ -471,13 +470,11 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
 }
 
 // Persistent lane-per-atom kernel for one fixed molecule. Block = 32 * W
-// threads; each warp owns kAtomBufSlots float4 of dynamic shared memory.
+// threads; no shared memory.
 template <int N, int MODE>
 __global__ void __launch_bounds__(256) rk45_atom_kernel(const RunParams P, const FixedMol M) {
-  extern __shared__ float4 smem_pos[];
-  float4* buf = smem_pos + (threadIdx.x >> 5) * kAtomBufSlots;
   const MixedIn none{};
-  atom_loop<N, MODE, false>(P, M, none, P.cursor, P.S, nullptr, buf);
+  atom_loop<N, MODE, false>(P, M, none, P.cursor, P.S, nullptr);
 }
 
 // One size bucket of the one-launch mixed kernel, kept out of line so each
@@ -485,9 +482,9 @@ __global__ void __launch_bounds__(256) rk45_atom_kernel(const RunParams P, const
 // loops together needed ~230 registers; apart, the largest needs 128).
 template <int N, int MODE>
 __device__ __noinline__ void mixed_bucket(const RunParams P, const MixedIn X, unsigned long long* cur,
-                                          unsigned long long cnt, const uint32_t* perm, float4* buf) {
+                                          unsigned long long cnt, const uint32_t* perm) {
   const FixedMol none{};
-  atom_loop<N, MODE, true>(P, none, X, cur, cnt, perm, buf);
+  atom_loop<N, MODE, true>(P, none, X, cur, cnt, perm);
 }
 
 // Mixed molecules in one persistent launch: every warp walks the size buckets
@@ -496,8 +493,6 @@ __device__ __noinline__ void mixed_bucket(const RunParams P, const MixedIn X, un
 // cache), serving each bucket from its own queue until it is empty.
 template <int MODE>
 __global__ void __launch_bounds__(256) rk45_mixed_kernel(const RunParams P, const MixedIn X, const Buckets B) {
-  extern __shared__ float4 smem_pos[];
-  float4* buf = smem_pos + (threadIdx.x >> 5) * kAtomBufSlots;
 #pragma unroll 1
   for (int n = CE_MAX_ATOMS; n >= 2; --n) {
     const unsigned long long cnt = B.cnt[n];
@@ -505,15 +500,15 @@ __global__ void __launch_bounds__(256) rk45_mixed_kernel(const RunParams P, cons
     const uint32_t* perm = B.perm + B.off[n];
     unsigned long long* cur = B.cursor + n;
     switch (n) {
-      case 10: mixed_bucket<10, MODE>(P, X, cur, cnt, perm, buf); break;
-      case 9: mixed_bucket<9, MODE>(P, X, cur, cnt, perm, buf); break;
-      case 8: mixed_bucket<8, MODE>(P, X, cur, cnt, perm, buf); break;
-      case 7: mixed_bucket<7, MODE>(P, X, cur, cnt, perm, buf); break;
-      case 6: mixed_bucket<6, MODE>(P, X, cur, cnt, perm, buf); break;
-      case 5: mixed_bucket<5, MODE>(P, X, cur, cnt, perm, buf); break;
-      case 4: mixed_bucket<4, MODE>(P, X, cur, cnt, perm, buf); break;
-      case 3: mixed_bucket<3, MODE>(P, X, cur, cnt, perm, buf); break;
-      default: mixed_bucket<2, MODE>(P, X, cur, cnt, perm, buf); break;
+      case 10: mixed_bucket<10, MODE>(P, X, cur, cnt, perm); break;
+      case 9: mixed_bucket<9, MODE>(P, X, cur, cnt, perm); break;
+      case 8: mixed_bucket<8, MODE>(P, X, cur, cnt, perm); break;
+      case 7: mixed_bucket<7, MODE>(P, X, cur, cnt, perm); break;
+      case 6: mixed_bucket<6, MODE>(P, X, cur, cnt, perm); break;
+      case 5: mixed_bucket<5, MODE>(P, X, cur, cnt, perm); break;
+      case 4: mixed_bucket<4, MODE>(P, X, cur, cnt, perm); break;
+      case 3: mixed_bucket<3, MODE>(P, X, cur, cnt, perm); break;
+      default: mixed_bucket<2, MODE>(P, X, cur, cnt, perm); break;
     }
   }
 }
@@ -521,10 +516,8 @@ __global__ void __launch_bounds__(256) rk45_mixed_kernel(const RunParams P, cons
 // One size bucket of a mixed batch (the per-size launch schedule).
 template <int N, int MODE>
 __global__ void __launch_bounds__(256) rk45_bucket_kernel(const RunParams P, const MixedIn X, const Buckets B) {
-  extern __shared__ float4 smem_pos[];
-  float4* buf = smem_pos + (threadIdx.x >> 5) * kAtomBufSlots;
   const FixedMol none{};
-  atom_loop<N, MODE, true>(P, none, X, B.cursor + N, B.cnt[N], B.perm + B.off[N], buf);
+  atom_loop<N, MODE, true>(P, none, X, B.cursor + N, B.cnt[N], B.perm + B.off[N]);
 }
 
 using AtomKernelFn = void (*)(RunParams, FixedMol);
