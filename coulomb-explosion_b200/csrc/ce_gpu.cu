@@ -167,7 +167,7 @@ int ce_run_device(ce_engine* e, uint64_t S, const float* pos, const ce_run_confi
   const ce::FixedKernelFn fn = atom ? ce::select_atom_kernel(e->n, cfg->precision_mode)
                                     : ce::select_fixed_kernel(e->n, cfg->precision_mode);
   if (!fn) return ce::fail(e, CE_ERR_INVALID, "ce_run: no kernel for this atom count");
-  const int block = t.block_threads;
+  const int block = atom ? std::min(t.block_threads, ce::kAtomMaxBlock) : t.block_threads;
   const uint64_t sims_per_block =
       atom ? static_cast<uint64_t>(block / 32) * static_cast<uint64_t>(32 / e->n) : static_cast<uint64_t>(block);
   int per_sm = t.blocks_per_sm;

@@ -215,7 +215,7 @@ int run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double 
   bucket_scatter_kernel<<<sort_grid, sort_block, 0, s>>>(in->n_atoms, S, T.off, T.fill, T.perm, P);
   int launches = 3;
 
-  const int block = t.block_threads;
+  const int block = std::min(t.block_threads, ce::kAtomMaxBlock);
   if (schedule == CE_SCHEDULE_ONE_LAUNCH) {
     const ce::MixedKernelFn fn = ce::select_mixed_kernel(0, cfg->precision_mode);
     int per_sm = t.blocks_per_sm;
@@ -464,13 +464,14 @@ int ce_autotune_fixed(ce_engine* e, uint64_t S, const float* pos_dev, const ce_r
   e->tuned_fixed[e->n].valid = false;
   std::vector<int> layouts = {1};
   if (e->n >= 2) layouts.push_back(e->n);
-  const int blocks[] = {64, 128, 256};
+  const int blocks_sim[] = {64, 128, 256};
+  const int blocks_atom[] = {64, 96, ce::kAtomMaxBlock};
   const int refills[] = {1, 2, 4};
   double best = -1.0;
   ce_tuning best_t{};
   int count = 0;
   for (int L : layouts)
-    for (int B : blocks)
+    for (int B : (L == 1 ? blocks_sim : blocks_atom))
       for (int R : refills) {
         ce_tuning t{B, 0, R, L};
         e->tuning = t;
@@ -504,7 +505,7 @@ int ce_autotune_mixed(ce_engine* e, uint64_t S, const ce_mixed_batch* dev_in, do
   if (rc != CE_OK) return rc;
   const ce_tuning saved = e->tuning;
   e->tuned_mixed.valid = false;
-  const int blocks[] = {64, 128, 256};
+  const int blocks[] = {64, 96, ce::kAtomMaxBlock};
   const int refills[] = {1, 2, 4};
   const int schedules[] = {CE_SCHEDULE_ONE_LAUNCH, CE_SCHEDULE_PER_SIZE};
   double best = -1.0;

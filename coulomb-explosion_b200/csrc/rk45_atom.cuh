@@ -38,6 +38,11 @@
 namespace ce {
 
 constexpr int kMixedStride = CE_MAX_ATOMS;  // atoms per sim row in the mixed layout
+// Largest block of the lane-per-atom kernels. Declaring it as the launch bound
+// lets the register allocator size for 128-thread blocks (N = 5: 92 registers,
+// 5 blocks per SM) instead of for 256-thread ones (80 registers with spills, so
+// that 3 such blocks fit), which ran CH4 ~3 % slower.
+constexpr int kAtomMaxBlock = 128;
 
 template <int N>
 struct AtomShape {
@@ -191,12 +196,16 @@ __device__ __forceinline__ void atom_finalize(const AtomLane<N, MODE>& s, int st
                                               const AtomConsts& ac, int ai, int base, const RunParams& P) {
   const double vx = s.v.xy.x, vy = s.v.xy.y, vz = s.v.z;
   const double ke = gsum<N>(0.5 * ac.mass * (vx * vx + vy * vy + vz * vz), base);
-  const int fin = gsum<N>((isfinite(vx) && isfinite(vy) && isfinite(vz)) ? 0 : 1, base);
-  if (status == CE_SIM_OK && fin != 0) status = CE_SIM_NONFINITE;
+  // Non-finite velocity anywhere in the group: one vote, masked to the group's lanes.
+  const unsigned bad = __ballot_sync(0xffffffffu, !(isfinite(vx) && isfinite(vy) && isfinite(vz)));
+  const unsigned gmask = ((1u << N) - 1u) << base;
+  if (status == CE_SIM_OK && (bad & gmask) != 0u) status = CE_SIM_NONFINITE;
   const double sc = (P.redistribute && ke > 0.0) ? sqrt(static_cast<double>(s.e0) / ke) : 1.0;
   const double mm = ac.mass * sc;
   const double px = mm * vx, py = mm * vy, pz = mm * vz;
-  const double ker = gsum<N>((px * px + py * py + pz * pz) / (2.0 * ac.mass), base);
+  // KER = sum |p_i|^2 / (2 m_i) with p_i = s m_i v_i, i.e. s^2 KE (the FP64
+  // group sum above), so no per-atom division or second group sum is needed.
+  const double ker = (sc * sc) * ke;
   if (status < 0) return;
   float* dst = P.momenta + s.sim * (3ull * STRIDE) + 3 * ai;
   dst[0] = static_cast<float>(px);
@@ -328,33 +337,37 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
       Acc peh;
       lane_force<N, Acc>(nbr, recv, pcv, s.x, ac, true, a0, peh);
       const Acc pe0 = gsum<N>(peh, base);
-      // Hairer norms from rest (sv = atol, probe accelerations = k1).
+      // Hairer norms from rest (sv = atol, probe accelerations = k1). The
+      // initial step is a heuristic (any h within the controller's reach gives
+      // the same converged answer), so its quotients use the fast forms.
+      const float inv_atol = __frcp_rn(P.atol);
       float d0p = 0.0f, d1p = 0.0f;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         const float sx = P.atol + P.rtol * fabsf(s.x.get(c));
-        const float r0 = s.x.get(c) / sx;
-        const float r1 = a0.get(c) / P.atol;
+        const float r0 = __fdividef(s.x.get(c), sx);
+        const float r1 = a0.get(c) * inv_atol;
         d0p += r0 * r0;
         d1p += r1 * r1;
       }
-      const float d0sq = gsum<N>(d0p, base), d1sq = gsum<N>(d1p, base);
-      const float denom = static_cast<float>(6 * N);
-      const float d0 = sqrtf(d0sq / denom), d1 = sqrtf(d1sq / denom);
-      const float h0 = (static_cast<double>(d0) < 1e-5 || static_cast<double>(d1) < 1e-5) ? 1e-6f : 0.01f * d0 / d1;
+      constexpr float inv_denom = 1.0f / static_cast<float>(6 * N);
+      const float d0 = sqrtf(gsum<N>(d0p, base) * inv_denom), d1 = sqrtf(gsum<N>(d1p, base) * inv_denom);
+      const float h0 = (static_cast<double>(d0) < 1e-5 || static_cast<double>(d1) < 1e-5)
+                           ? 1e-6f
+                           : __fdividef(0.01f * d0, d1);
       float d2p = 0.0f;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         const float sx = P.atol + P.rtol * fabsf(s.x.get(c));
-        const float r = (a0.get(c) * h0) / sx;
+        const float r = __fdividef(a0.get(c) * h0, sx);
         d2p += r * r;
       }
-      const float d2 = sqrtf(gsum<N>(d2p, base) / denom) / h0;
+      const float d2 = __fdividef(sqrtf(gsum<N>(d2p, base) * inv_denom), h0);
       if (fresh) {
         s.k[0] = a0;
         const float h1 = (static_cast<double>(d1) <= 1e-15 && static_cast<double>(d2) <= 1e-15)
                              ? fmaxf(1e-6f, h0 * 1e-3f)
-                             : powf(0.01f / fmaxf(d1, d2), 0.2f);
+                             : __powf(__fdividef(0.01f, fmaxf(d1, d2)), 0.2f);
         float hm = 100.0f * h0;
         if (h1 < hm) hm = h1;
         if (P.max_dt < hm) hm = P.max_dt;
@@ -383,15 +396,21 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
 
     // ---- one DP5(4) attempt, all lanes ----
     const float hh = (P.max_dt < s.h) ? P.max_dt : s.h;
+    const float hh2 = hh * hh;
+    const V3 hv = v3_mul(hh, s.v);
     V3 xs, a;
     V3 cxn = v3_zero();
     Acc pe_half = Acc(0);
 #pragma unroll
     for (int si = 1; si <= 6; ++si) {
-      V3 sum = v3_zero();
+      // x_s = x + c_s h v + h^2 sum_l abar_sl k_l (stage 2 has no k term).
+      V3 inc = v3_mul(c_c[si + 1], hv);
+      if (si > 1) {
+        V3 sum = v3_mul(c_abar[si + 1][1], s.k[0]);
 #pragma unroll
-      for (int l = 0; l + 1 < si; ++l) sum = v3_fma(c_abar[si + 1][l + 1], s.k[l], sum);
-      const V3 inc = v3_mul(hh, v3_fma(hh, sum, v3_mul(c_c[si + 1], s.v)));
+        for (int l = 1; l + 1 < si; ++l) sum = v3_fma(c_abar[si + 1][l + 1], s.k[l], sum);
+        inc = v3_fma(hh2, sum, inc);
+      }
       if (L::kKahan && si == 6) {
         const V3 y = v3_sub(inc, s.cx);
         xs = v3_add(s.x, y);
@@ -419,7 +438,7 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
     } else {
       vn = v3_add(s.v, incv);
     }
-    const V3 ex = v3_mul(hh * hh, se);
+    const V3 ex = v3_mul(hh2, se);
     const V3 ev = v3_mul(hh, v3_fma(c_e[7], a, sev));
     float errp = 0.0f;
 #pragma unroll
@@ -435,8 +454,10 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
     const Acc pe_new = gsum<N>(pe_half, base);
     int fin_st = -1;
     if (active) {
-      const float en = sqrtf(err_sq * (1.0f / static_cast<float>(6 * N)));
-      if (en <= 1.0f) {
+      // RMS norm squared: en <= 1 exactly when en^2 <= 1, and the controller's
+      // en^-1/5 is (en^2)^-1/10, so no square root is taken.
+      const float en2 = err_sq * (1.0f / static_cast<float>(6 * N));
+      if (en2 <= 1.0f) {
         s.x = xs;
         s.v = vn;
         s.k[0] = a;
@@ -444,7 +465,7 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
           s.cx = cxn;
           s.cv = cvn;
         }
-        float factor = (en == 0.0f) ? kMaxFactor : fminf(kMaxFactor, kSafety * __powf(en, kExponent));
+        float factor = (en2 == 0.0f) ? kMaxFactor : fminf(kMaxFactor, kSafety * __powf(en2, 0.5f * kExponent));
         if (s.rej_once) factor = fminf(factor, 1.0f);
         const float hn = hh * factor;
         s.h = (P.max_dt < hn) ? P.max_dt : hn;
@@ -455,7 +476,7 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
         if (!(pe_new > s.pe_stop)) fin_st = CE_SIM_OK;
         else if (s.steps >= P.max_steps) fin_st = CE_SIM_MAX_STEPS;
       } else {
-        const float factor = fmaxf(kMinFactor, kSafety * __powf(en, kExponent));
+        const float factor = fmaxf(kMinFactor, kSafety * __powf(en2, 0.5f * kExponent));
         s.h = hh * factor;
         s.rej_once = true;
         s.rejects += 1u;
@@ -472,7 +493,7 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
 // Persistent lane-per-atom kernel for one fixed molecule. Block = 32 * W
 // threads; no shared memory.
 template <int N, int MODE>
-__global__ void __launch_bounds__(256) rk45_atom_kernel(const RunParams P, const FixedMol M) {
+__global__ void __launch_bounds__(kAtomMaxBlock) rk45_atom_kernel(const RunParams P, const FixedMol M) {
   const MixedIn none{};
   atom_loop<N, MODE, false>(P, M, none, P.cursor, P.S, nullptr);
 }
@@ -490,9 +511,11 @@ __device__ __noinline__ void mixed_bucket(const RunParams P, const MixedIn X, un
 // Mixed molecules in one persistent launch: every warp walks the size buckets
 // from 10 atoms down to 2 (the longest simulations first, and all warps on the
 // same N at nearly the same time, so one N's code is hot in the instruction
-// cache), serving each bucket from its own queue until it is empty.
+// cache), serving each bucket from its own queue until it is empty. Four
+// blocks per SM are asked for: left free, the nine out-of-line bucket loops
+// take 166 registers and only three blocks fit.
 template <int MODE>
-__global__ void __launch_bounds__(256) rk45_mixed_kernel(const RunParams P, const MixedIn X, const Buckets B) {
+__global__ void __launch_bounds__(kAtomMaxBlock, 4) rk45_mixed_kernel(const RunParams P, const MixedIn X, const Buckets B) {
 #pragma unroll 1
   for (int n = CE_MAX_ATOMS; n >= 2; --n) {
     const unsigned long long cnt = B.cnt[n];
@@ -515,7 +538,7 @@ __global__ void __launch_bounds__(256) rk45_mixed_kernel(const RunParams P, cons
 
 // One size bucket of a mixed batch (the per-size launch schedule).
 template <int N, int MODE>
-__global__ void __launch_bounds__(256) rk45_bucket_kernel(const RunParams P, const MixedIn X, const Buckets B) {
+__global__ void __launch_bounds__(kAtomMaxBlock) rk45_bucket_kernel(const RunParams P, const MixedIn X, const Buckets B) {
   const FixedMol none{};
   atom_loop<N, MODE, true>(P, none, X, B.cursor + N, B.cnt[N], B.perm + B.off[N]);
 }
