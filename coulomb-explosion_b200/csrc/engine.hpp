@@ -123,13 +123,14 @@ int run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double 
                      const ce_outputs* out, int schedule, void* stream, bool skip_empty);
 
 // Default refill granularity: with G = 32 / n sims per warp in the lane-per-atom
-// layout, a warp refills once a third of its groups are idle (measured best for
-// CH4, G = 6: 1.81e8 vs 1.72e8 explosions/s at threshold 1; N = 10, G = 3:
-// threshold 1). Thread-per-sim refills at once.
+// layout, a warp refills once floor((G - 1) / 3) of its groups are idle, at
+// least one (measured: CH4, G = 6: 1 beats 2 and 3 by 0.5 % and 1.5 %; stiff
+// H2O, G = 10: 3 beats 2 and 4 by 0.3 % and 3.7 %; N = 10, G = 3: 1).
+// Thread-per-sim refills at once.
 inline int default_refill(int n, int lanes_per_sim) {
   if (lanes_per_sim < 2 || n < 2) return 1;
   const int g = 32 / n;
-  return g / 3 > 1 ? g / 3 : 1;
+  return (g - 1) / 3 > 1 ? (g - 1) / 3 : 1;
 }
 
 }  // namespace ce
