@@ -30,8 +30,11 @@ struct ce_engine {
   int tuned_schedule = CE_SCHEDULE_ONE_LAUNCH;  // schedule ce_run_mixed uses (autotuner's pick)
   unsigned long long* d_cursor = nullptr;  // fixed path work-queue head (engine scratch)
   cudaStream_t stream = nullptr;           // stream of the host-buffer paths
-  // ce_run pipelining: copy-in / copy-out streams and per-slot events
-  cudaStream_t s_in = nullptr, s_out = nullptr;
+  // ce_run pipelining: copy-in / copy-out streams, a second compute stream (the
+  // chunks of the two device slots integrate on `stream` and `s_comp2`, so one
+  // chunk's blocks start while the other's last simulations finish) and per-slot
+  // events
+  cudaStream_t s_in = nullptr, s_out = nullptr, s_comp2 = nullptr;
   cudaEvent_t ev_loaded[2] = {nullptr, nullptr}, ev_computed[2] = {nullptr, nullptr},
               ev_copied[2] = {nullptr, nullptr};
   void* d_arena = nullptr;                 // device buffers of the host-buffer paths
