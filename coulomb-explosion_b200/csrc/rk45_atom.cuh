@@ -104,6 +104,20 @@ __device__ __forceinline__ V3 v3_sub(const V3& a, const V3& b) {
   return {__ffma2_rn(bcast(-1.0f), b.xy, a.xy), a.z - b.z};
 }
 
+// Approximate reciprocal and square root (PTX rcp.approx / sqrt.approx, flush
+// to zero): for the error-norm scales and the initial-step heuristic, where a
+// relative error of a few 1e-7 changes no decision the integrator relies on.
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float r;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 template <int N, int MODE>
 struct AtomLane {
   static constexpr bool kKahan = (MODE & CE_PREC_KAHAN) != 0;
@@ -200,7 +214,11 @@ __device__ __forceinline__ void atom_finalize(const AtomLane<N, MODE>& s, int st
   const unsigned bad = __ballot_sync(0xffffffffu, !(isfinite(vx) && isfinite(vy) && isfinite(vz)));
   const unsigned gmask = ((1u << N) - 1u) << base;
   if (status == CE_SIM_OK && (bad & gmask) != 0u) status = CE_SIM_NONFINITE;
-  const double sc = (P.redistribute && ke > 0.0) ? sqrt(static_cast<double>(s.e0) / ke) : 1.0;
+  // s = sqrt(E0 / KE), formed as E0 rsqrt(E0 KE) (one reciprocal square root
+  // instead of a division and a square root) when E0 > 0.
+  const double e0d = static_cast<double>(s.e0);
+  const double sc =
+      (P.redistribute && ke > 0.0) ? (e0d > 0.0 ? e0d * rsqrt(e0d * ke) : sqrt(e0d / ke)) : 1.0;
   const double mm = ac.mass * sc;
   const double px = mm * vx, py = mm * vy, pz = mm * vz;
   // KER = sum |p_i|^2 / (2 m_i) with p_i = s m_i v_i, i.e. s^2 KE (the FP64
@@ -351,7 +369,8 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
         d1p += r1 * r1;
       }
       constexpr float inv_denom = 1.0f / static_cast<float>(6 * N);
-      const float d0 = sqrtf(gsum<N>(d0p, base) * inv_denom), d1 = sqrtf(gsum<N>(d1p, base) * inv_denom);
+      const float d0 = sqrt_approx(gsum<N>(d0p, base) * inv_denom);
+      const float d1 = sqrt_approx(gsum<N>(d1p, base) * inv_denom);
       const float h0 = (static_cast<double>(d0) < 1e-5 || static_cast<double>(d1) < 1e-5)
                            ? 1e-6f
                            : __fdividef(0.01f * d0, d1);
@@ -362,7 +381,7 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
         const float r = __fdividef(a0.get(c) * h0, sx);
         d2p += r * r;
       }
-      const float d2 = __fdividef(sqrtf(gsum<N>(d2p, base) * inv_denom), h0);
+      const float d2 = __fdividef(sqrt_approx(gsum<N>(d2p, base) * inv_denom), h0);
       if (fresh) {
         s.k[0] = a0;
         const float h1 = (static_cast<double>(d1) <= 1e-15 && static_cast<double>(d2) <= 1e-15)
@@ -440,16 +459,21 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
     }
     const V3 ex = v3_mul(hh2, se);
     const V3 ev = v3_mul(hh, v3_fma(c_e[7], a, sev));
-    float errp = 0.0f;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const float scx = fmaf(P.rtol, fmaxf(fabsf(s.x.get(c)), fabsf(xs.get(c))), P.atol);
-      const float scv = fmaf(P.rtol, fmaxf(fabsf(s.v.get(c)), fabsf(vn.get(c))), P.atol);
-      const float rx = __fdividef(ex.get(c), scx);
-      const float rv = __fdividef(ev.get(c), scv);
-      errp = fmaf(rx, rx, errp);
-      errp = fmaf(rv, rv, errp);
-    }
+    // Scaled errors e / (atol + rtol max(|y0|, |y1|)); x and y packed.
+    const float2 scx = __ffma2_rn(bcast(P.rtol),
+                                  make_float2(fmaxf(fabsf(s.x.xy.x), fabsf(xs.xy.x)),
+                                              fmaxf(fabsf(s.x.xy.y), fabsf(xs.xy.y))),
+                                  bcast(P.atol));
+    const float2 scv = __ffma2_rn(bcast(P.rtol),
+                                  make_float2(fmaxf(fabsf(s.v.xy.x), fabsf(vn.xy.x)),
+                                              fmaxf(fabsf(s.v.xy.y), fabsf(vn.xy.y))),
+                                  bcast(P.atol));
+    const float2 rx = __fmul2_rn(ex.xy, make_float2(rcp_approx(scx.x), rcp_approx(scx.y)));
+    const float2 rv = __fmul2_rn(ev.xy, make_float2(rcp_approx(scv.x), rcp_approx(scv.y)));
+    const float2 e2 = __ffma2_rn(rv, rv, __fmul2_rn(rx, rx));
+    const float rxz = ex.z * rcp_approx(fmaf(P.rtol, fmaxf(fabsf(s.x.z), fabsf(xs.z)), P.atol));
+    const float rvz = ev.z * rcp_approx(fmaf(P.rtol, fmaxf(fabsf(s.v.z), fabsf(vn.z)), P.atol));
+    const float errp = fmaf(rvz, rvz, fmaf(rxz, rxz, e2.x + e2.y));
     const float err_sq = gsum<N>(errp, base);
     const Acc pe_new = gsum<N>(pe_half, base);
     int fin_st = -1;
