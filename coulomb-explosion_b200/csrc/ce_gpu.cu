@@ -19,7 +19,7 @@ namespace {
 
 // Launch shape for one run: explicit tuning fields win, then the autotuned
 // entry for this atom count, then the defaults (128 threads, occupancy-limited
-// grid, refill as soon as one lane or group is idle, one lane per atom for
+// grid, the per-size refill granularity of default_refill, one lane per atom for
 // N >= 2 -- measured faster on B200 than one thread per sim for CH4 and N = 10).
 ce_tuning effective_tuning(const ce_engine* e, int n) {
   ce_tuning t = e->tuning;

@@ -125,15 +125,5 @@ inline MixedKernelFn select_mixed_kernel(int n, int mode) {
 int run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coulomb_k, const ce_run_config* cfg,
                      const ce_outputs* out, int schedule, void* stream, bool skip_empty);
 
-// Default refill granularity: with G = 32 / n sims per warp in the lane-per-atom
-// layout, a warp refills once floor((G - 1) / 3) of its groups are idle, at
-// least one (measured: CH4, G = 6: 1 beats 2 and 3 by 0.5 % and 1.5 %; stiff
-// H2O, G = 10: 3 beats 2 and 4 by 0.3 % and 3.7 %; N = 10, G = 3: 1).
-// Thread-per-sim refills at once.
-inline int default_refill(int n, int lanes_per_sim) {
-  if (lanes_per_sim < 2 || n < 2) return 1;
-  const int g = 32 / n;
-  return (g - 1) / 3 > 1 ? (g - 1) / 3 : 1;
-}
 
 }  // namespace ce

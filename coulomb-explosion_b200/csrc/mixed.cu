@@ -197,7 +197,7 @@ int run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double 
   const ce_tuning t = mixed_tuning(e);
 
   ce::RunParams P{};
-  ce::fill_run_params(P, cfg, out, t.refill_threshold > 0 ? t.refill_threshold : 1);
+  ce::fill_run_params(P, cfg, out, t.refill_threshold);  // 0: each size's default
   P.skip_empty = skip_empty ? 1 : 0;
   P.pos = in->pos;
   P.cursor = nullptr;
@@ -466,7 +466,7 @@ int ce_autotune_fixed(ce_engine* e, uint64_t S, const float* pos_dev, const ce_r
   if (e->n >= 2) layouts.push_back(e->n);
   const int blocks_sim[] = {64, 128, 256};
   const int blocks_atom[] = {64, 96, ce::kAtomMaxBlock};
-  const int refills[] = {1, 2, 4};
+  const int refills[] = {0, 1, 2, 4};  // 0: the per-size default
   double best = -1.0;
   ce_tuning best_t{};
   int count = 0;
@@ -506,7 +506,7 @@ int ce_autotune_mixed(ce_engine* e, uint64_t S, const ce_mixed_batch* dev_in, do
   const ce_tuning saved = e->tuning;
   e->tuned_mixed.valid = false;
   const int blocks[] = {64, 96, ce::kAtomMaxBlock};
-  const int refills[] = {1, 2, 4};
+  const int refills[] = {0, 1, 2, 4};  // 0: each size's default
   const int schedules[] = {CE_SCHEDULE_ONE_LAUNCH, CE_SCHEDULE_PER_SIZE};
   double best = -1.0;
   ce_tuning best_t{};

@@ -44,6 +44,16 @@ constexpr int kMixedStride = CE_MAX_ATOMS;  // atoms per sim row in the mixed la
 // that 3 such blocks fit), which ran CH4 ~3 % slower.
 constexpr int kAtomMaxBlock = 128;
 
+// Default refill granularity: with G = 32 / n sims per warp in the lane-per-atom
+// layout, a warp refills once floor((G - 1) / 3) of its groups are idle, at
+// least one (measured: CH4, G = 6: 1 beats 2 and 3 by 0.5 % and 1.5 %; stiff
+// H2O, G = 10: 3 beats 2 and 4 by 0.3 % and 3.7 %; N = 10, G = 3: 1).
+// Thread-per-sim refills at once. A refill threshold of 0 in RunParams or
+// ce_tuning means this per-size default.
+__host__ __device__ constexpr int default_refill(int n, int lanes_per_sim) {
+  return (lanes_per_sim < 2 || n < 2) ? 1 : ((32 / n - 1) / 3 > 1 ? (32 / n - 1) / 3 : 1);
+}
+
 template <int N>
 struct AtomShape {
   static constexpr int G = 32 / N;     // simulations per warp
@@ -546,16 +556,18 @@ __global__ void __launch_bounds__(kAtomMaxBlock, 4) rk45_mixed_kernel(const RunP
     if (cnt == 0ull) continue;
     const uint32_t* perm = B.perm + B.off[n];
     unsigned long long* cur = B.cursor + n;
+    RunParams Pn = P;
+    if (Pn.refill_threshold == 0) Pn.refill_threshold = default_refill(n, n);
     switch (n) {
-      case 10: mixed_bucket<10, MODE>(P, X, cur, cnt, perm); break;
-      case 9: mixed_bucket<9, MODE>(P, X, cur, cnt, perm); break;
-      case 8: mixed_bucket<8, MODE>(P, X, cur, cnt, perm); break;
-      case 7: mixed_bucket<7, MODE>(P, X, cur, cnt, perm); break;
-      case 6: mixed_bucket<6, MODE>(P, X, cur, cnt, perm); break;
-      case 5: mixed_bucket<5, MODE>(P, X, cur, cnt, perm); break;
-      case 4: mixed_bucket<4, MODE>(P, X, cur, cnt, perm); break;
-      case 3: mixed_bucket<3, MODE>(P, X, cur, cnt, perm); break;
-      default: mixed_bucket<2, MODE>(P, X, cur, cnt, perm); break;
+      case 10: mixed_bucket<10, MODE>(Pn, X, cur, cnt, perm); break;
+      case 9: mixed_bucket<9, MODE>(Pn, X, cur, cnt, perm); break;
+      case 8: mixed_bucket<8, MODE>(Pn, X, cur, cnt, perm); break;
+      case 7: mixed_bucket<7, MODE>(Pn, X, cur, cnt, perm); break;
+      case 6: mixed_bucket<6, MODE>(Pn, X, cur, cnt, perm); break;
+      case 5: mixed_bucket<5, MODE>(Pn, X, cur, cnt, perm); break;
+      case 4: mixed_bucket<4, MODE>(Pn, X, cur, cnt, perm); break;
+      case 3: mixed_bucket<3, MODE>(Pn, X, cur, cnt, perm); break;
+      default: mixed_bucket<2, MODE>(Pn, X, cur, cnt, perm); break;
     }
   }
 }

@@ -113,7 +113,8 @@ typedef struct ce_tuning {
                              * lane-per-atom and mixed-batch kernels run at most     *
                              * 128 and clamp a larger request to 128                 */
   int32_t blocks_per_sm;    /* persistent grid = SMs * this (0: occupancy limit)    */
-  int32_t refill_threshold; /* refill a warp once this many sims are idle (1..32)   */
+  int32_t refill_threshold; /* refill a warp once this many sims are idle (1..32;   *
+                             * 0: a default per molecule size)                       */
   int32_t lanes_per_sim;    /* 1 = one thread per sim; 2..10 = one lane per atom    */
 } ce_tuning;
 

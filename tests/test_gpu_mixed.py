@@ -154,7 +154,8 @@ def test_autotuner_picks_a_measured_candidate_and_keeps_results(ce, wl):
     engine.run_mixed_device(S, batch, cfg, o0, ce.CE_SCHEDULE_ONE_LAUNCH, stream.cuda_stream)
     stream.synchronize()
     report, best = engine.autotune_mixed(S, batch, cfg)
-    assert len(report) == 18 and all(r["sims_per_s"] > 0 for r in report)
+    # 2 schedules x 3 block sizes x 4 refill thresholds (0 = each size's default)
+    assert len(report) == 24 and all(r["sims_per_s"] > 0 for r in report)
     assert best in (ce.CE_SCHEDULE_ONE_LAUNCH, ce.CE_SCHEDULE_PER_SIZE)
     d1, o1 = _device_out(torch, ce, S)
     engine.run_mixed_device(S, batch, cfg, o1, best, stream.cuda_stream)
@@ -165,8 +166,10 @@ def test_autotuner_picks_a_measured_candidate_and_keeps_results(ce, wl):
     engine.set_molecule(mol.masses_me, mol.charge_array)
     x = torch.from_numpy(wl.sample_molecule(mol, S, seed=36).astype(np.float32)).cuda()
     rep = engine.autotune_fixed(S, x.data_ptr(), cfg)
-    assert len(rep) == 18 and {r["lanes_per_sim"] for r in rep} == {1, 5}
+    # 2 layouts x 3 block sizes x 4 refill thresholds
+    assert len(rep) == 24 and {r["lanes_per_sim"] for r in rep} == {1, 5}
     t = engine.get_tuning()
     best_f = max(rep, key=lambda r: r["sims_per_s"])
+    # get_tuning reports the resolved shape: refill 0 is CH4's default of 1 in both layouts
     assert (t["block_threads"], t["refill_threshold"], t["lanes_per_sim"]) == (
-        best_f["block_threads"], best_f["refill_threshold"], best_f["lanes_per_sim"])
+        best_f["block_threads"], best_f["refill_threshold"] or 1, best_f["lanes_per_sim"])
