@@ -152,6 +152,33 @@ def test_ragged_sizes_and_empty(engine, ce, wl):
         np.testing.assert_array_equal(part.steps, full.steps[:S])
 
 
+def test_chunked_host_path_matches_device_path(engine, ce, wl):
+    # ce_run cuts a batch above 2^17 sims into chunks that alternate between two
+    # device slots, each integrated on its own stream with its own work queue; an
+    # uneven batch of 5 chunks must give bit for bit what one ce_run_device
+    # launch gives, in every output.
+    torch = pytest.importorskip("torch")
+    mol = wl.CH4
+    engine.set_molecule(mol.masses_me, mol.charge_array)
+    S = 5 * 65536 + 777
+    pos = wl.sample_molecule(mol, S, seed=41).astype(np.float32)
+    cfg = cfg_for(ce, wl.TIGHT, 3)
+    host = engine.run(pos, cfg, diagnostics=True)
+    dev = torch.device("cuda", 0)
+    x = torch.from_numpy(pos).to(dev)
+    names = ("momenta", "ker", "steps", "status", "rejects", "t_final", "pe_final", "ke_before", "positions", "e0")
+    # raw byte buffers on the device, read back with each output's dtype and shape
+    d = {k: torch.zeros(getattr(host, k).nbytes, dtype=torch.uint8, device=dev) for k in names}
+    out = ce.CeOutputs(*(d[k].data_ptr() for k in names))
+    stream = torch.cuda.Stream(device=dev)
+    engine.run_device(S, x.data_ptr(), cfg, out, stream.cuda_stream)
+    stream.synchronize()
+    assert (host.status == 0).all()
+    for k in names:
+        h = getattr(host, k)
+        np.testing.assert_array_equal(h, d[k].cpu().numpy().view(h.dtype).reshape(h.shape), err_msg=k)
+
+
 @pytest.mark.parametrize("lanes", [1, 5])
 def test_results_independent_of_launch_shape(engine, ce, wl, lanes):
     # Each sim's arithmetic is private to its thread (or its lane group), so
