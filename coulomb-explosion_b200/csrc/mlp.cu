@@ -315,14 +315,17 @@ __global__ void f32_to_bf16_kernel(const float* a, bf16* b, int n) {
 //   warp 1  MMA issuer: one thread runs the (layer, tile) jobs in the order
 //           A0 B0 A1 B1 ..., each job's slices into its tile's accumulator
 //           (two 128 x 256 FP32 blocks, 512 TMEM columns);
-//   warps 2-9 / 10-17  epilogue of tile A / tile B: TMEM -> bias + SiLU ->
+//   warps 2-13 / 14-25  epilogue of tile A / tile B (12 warps a tile: each of
+//           the 4 TMEM lane quarters by 3 warps, one third of the columns each,
+//           so that enough warps hide the TMEM-load and SiLU latencies): TMEM -> bias + SiLU ->
 //           BF16 -> the tile's activation operand in shared memory (the input
 //           of the next layer), or FP32 outputs after the last layer; they also
 //           load the next input tile.
 // So tile A's epilogue of layer l overlaps tile B's MMAs of layer l and vice
 // versa; activations never leave shared memory. All waits are bounded.
 constexpr int kFwdMaxLayers = 8;
-constexpr int kFwdThreads = 576;               // 18 warps: producer, MMA issuer, 2 x 8 epilogue
+constexpr int kFwdGroups = 3;                  // epilogue column groups per tile
+constexpr int kFwdThreads = 32 * (2 + 2 * 4 * kFwdGroups);  // producer, MMA issuer, 2 x 12 epilogue
 constexpr int kFwdKmax = 256;                  // widest layer input held in shared memory
 constexpr int kFwdSboA = (kFwdKmax / 8) * 128; // 4096 B between row-adjacent core matrices
 constexpr int kFwdAct = kTM * kFwdKmax * 2;    // 64 KB activation operand per tile
@@ -423,7 +426,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) mlp_forward_fused_kernel(const
     }
     for (int t = 0; t < 2; ++t) {
       umma::mbar_init(&acc_full[t], 1);
-      umma::mbar_init(&act_ready[t], 2 * kTM);  // the tile's 8 epilogue warps
+      umma::mbar_init(&act_ready[t], kFwdGroups * kTM);  // the tile's epilogue threads
     }
     *abort_flag = 0;
   }
@@ -494,15 +497,15 @@ __global__ void __launch_bounds__(kFwdThreads, 1) mlp_forward_fused_kernel(const
       }
     }
   } else {
-    // ---- epilogue: warps 2-9 tile A, 10-17 tile B; each warp one lane quarter
-    // (warp % 4, the TMEM lanes it may read) and one half of the columns ----
-    const int ew = warp - 2, t = ew >> 3, half = (ew & 7) >> 2, quarter = warp & 3;
+    // ---- epilogue: 12 warps a tile; each warp one lane quarter (warp % 4, the
+    // TMEM lanes it may read) and one group of 16-column chunks ----
+    const int ew = warp - 2, t = ew / (4 * kFwdGroups), grp = (ew % (4 * kFwdGroups)) / 4, quarter = warp & 3;
     const int row = quarter * 32 + lane;
     const uint32_t tbase = tmem + (static_cast<uint32_t>(quarter * 32) << 16) + t * kTNmax;
     const int G = A.fan_in[0] / 8;
     auto load_x = [&](int pair) {
       const int m0 = (2 * pair + t) * kTM;
-      for (int i = half * kTM + row; i < kTM * G; i += 2 * kTM) {
+      for (int i = grp * kTM + row; i < kTM * G; i += kFwdGroups * kTM) {
         const int r = i / G, g = i - r * G;
         cp_async16(act[t] + (r >> 3) * kFwdSboA + g * kLBO + (r & 7) * 16,
                    A.x + static_cast<size_t>(m0 + r) * A.fan_in[0] + g * 8);
@@ -522,7 +525,8 @@ __global__ void __launch_bounds__(kFwdThreads, 1) mlp_forward_fused_kernel(const
       if (t >= tiles_of(pair)) break;
       const int m0 = (2 * pair + t) * kTM;
       for (int l = 0; l < A.layers && ok; ++l) {
-        const int N = A.fan_out[l], cols = N / 2, cbeg = half * cols;
+        const int N = A.fan_out[l], nch16 = N / 16;
+        const int cbeg = 16 * (grp * nch16 / kFwdGroups), cend = 16 * ((grp + 1) * nch16 / kFwdGroups);
         const float* bias = A.p + A.b_off[l];
         const bool last = l + 1 == A.layers;
         // this warp's first 16 biases, one per lane, fetched before the wait
@@ -530,11 +534,11 @@ __global__ void __launch_bounds__(kFwdThreads, 1) mlp_forward_fused_kernel(const
         if (!(ok = wait(&acc_full[t], ph_acc))) break;
         ph_acc ^= 1u;
         umma::tc_fence_after();
-        for (int c0 = cbeg; c0 < cbeg + cols; c0 += 16) {
+        for (int c0 = cbeg; c0 < cend; c0 += 16) {
           uint32_t r[16];
           umma::tmem_ld16(tbase + static_cast<uint32_t>(c0), r);
           const float bl = bnext;  // lane j holds bias[c0 + j]
-          if (c0 + 16 < cbeg + cols) bnext = lane < 16 ? __ldg(bias + c0 + 16 + lane) : 0.0f;
+          if (c0 + 16 < cend) bnext = lane < 16 ? __ldg(bias + c0 + 16 + lane) : 0.0f;
           umma::tmem_wait_ld();
           float b[16];
 #pragma unroll
