@@ -31,6 +31,7 @@
 #include <mutex>
 
 #include "ce_gpu.h"
+#include "rk45_atom.cuh"
 #include "rk45_sim.cuh"
 
 namespace {
@@ -69,7 +70,17 @@ int scratch_address(int dev, unsigned long long** addr, char* err, size_t err_le
   return CE_OK;
 }
 
+// The kernel ce_run_device launches by default: one lane per atom for n >= 2,
+// one thread per simulation for a single atom.
 ce::FixedKernelFn kernel_for(int n, int mode) {
+  if (n >= 2) {
+    switch (mode & 3) {
+      case 0: return ce::atom_kernel_m0(n);
+      case 1: return ce::atom_kernel_m1(n);
+      case 2: return ce::atom_kernel_m2(n);
+      default: return ce::atom_kernel_m3(n);
+    }
+  }
   switch (mode & 3) {
     case 0: return ce::fixed_kernel_m0(n);
     case 1: return ce::fixed_kernel_m1(n);
@@ -107,6 +118,7 @@ extern "C" int ce_run_device_noalloc(int n, const double* mass_me, const double*
     m.kq[i] = static_cast<float>(coulomb_k * charge[i]);
     for (int j = 0; j < n; ++j) m.pc[i * n + j] = static_cast<float>(coulomb_k * charge[i] * charge[j]);
   }
+  m.k = static_cast<float>(coulomb_k);
   if (S == 0) return CE_OK;
   if (!pos || !out || !out->momenta)
     return report(err, err_len, CE_ERR_INVALID, "ce_run_device_noalloc: pos and out->momenta are required");
@@ -125,7 +137,10 @@ extern "C" int ce_run_device_noalloc(int n, const double* mass_me, const double*
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     return report(err, err_len, CE_ERR_CUDA, "ce_run_device_noalloc: device query failed");
   if (per_sm < 1) per_sm = 1;
-  const uint64_t need = (S + block - 1) / block;
+  const int lanes = n >= 2 ? n : 1;
+  const uint64_t sims_per_block =
+      lanes >= 2 ? static_cast<uint64_t>(block / 32) * static_cast<uint64_t>(32 / n) : static_cast<uint64_t>(block);
+  const uint64_t need = (S + sims_per_block - 1) / sims_per_block;
   const uint64_t grid = need < static_cast<uint64_t>(sms) * per_sm ? need : static_cast<uint64_t>(sms) * per_sm;
 
   ce::RunParams P{};
@@ -149,7 +164,7 @@ extern "C" int ce_run_device_noalloc(int n, const double* mass_me, const double*
   P.pe_stop_d = cfg->pe_stop_fraction;
   P.max_steps = cfg->max_steps > 0xffffffffull ? 0xffffffffu : static_cast<uint32_t>(cfg->max_steps);
   P.redistribute = cfg->redistribute_energy ? 1 : 0;
-  P.refill_threshold = 1;
+  P.refill_threshold = ce::default_refill(n, lanes);
 
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   st = cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), s);  // the cursor must start at 0

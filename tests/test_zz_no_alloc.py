@@ -47,11 +47,10 @@ def test_noalloc_entry_point_matches_ce_run_device(ce, wl):
     cfg = ce.RunConfig(rtol=wl.TIGHT[0], atol=wl.TIGHT[1], pe_stop_fraction=wl.TIGHT[2],
                        precision_mode=ce.CE_PREC_KAHAN | ce.CE_PREC_FP64)
 
-    # Ordinary path: engine-owned scratch, pinned to the same one-thread-per-sim
-    # kernel the allocation-free entry point launches.
+    # Ordinary path: engine-owned scratch, default launch shape (one lane per
+    # atom, the kernel the allocation-free entry point launches too).
     eng = ce.Engine(0)
     eng.set_molecule(mol.masses_me, mol.charge_array)
-    eng.set_tuning(lanes_per_sim=1)
     ref = _device_buffers(torch, S, mol.n)
     stream = torch.cuda.current_stream().cuda_stream
     eng.run_device(S, pos.data_ptr(), cfg, _outputs(ce, ref), stream)
