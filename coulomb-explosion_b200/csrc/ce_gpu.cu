@@ -245,7 +245,30 @@ int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
   // (measured on CH4 1e6: 8 chunks 1.79e8/s end to end, 16 1.85e8, 32 1.75e8)
   constexpr uint64_t kMinChunk = 1ull << 16;
   const uint64_t nchunks = S < 2 * kMinChunk ? 1 : std::min<uint64_t>(16, S / kMinChunk);
-  const uint64_t C = (S + nchunks - 1) / nchunks;
+  // Chunk k spans [bnd[k], bnd[k + 1]). From 6 chunks on, the first and last two
+  // are tapered (weights 1/4, 1/2, 1, ..., 1, 1/2, 1/4), so the copy-in before
+  // the first kernel and the copy-out after the last are short. C is the largest.
+  uint64_t bnd[17];
+  {
+    const bool taper = nchunks >= 6;
+    auto w = [&](uint64_t k) -> uint64_t {  // in quarters
+      if (!taper) return 4;
+      if (k == 0 || k + 1 == nchunks) return 1;
+      if (k == 1 || k + 2 == nchunks) return 2;
+      return 4;
+    };
+    uint64_t wsum = 0;
+    for (uint64_t k = 0; k < nchunks; ++k) wsum += w(k);
+    uint64_t acc = 0;
+    for (uint64_t k = 0; k < nchunks; ++k) {
+      bnd[k] = S * acc / wsum;  // S <= 2^40 and acc <= 64: no overflow
+      acc += w(k);
+    }
+    bnd[nchunks] = S;
+  }
+  auto bound = [&](uint64_t k) -> uint64_t { return bnd[k]; };
+  uint64_t C = 0;
+  for (uint64_t k = 0; k < nchunks; ++k) C = std::max<uint64_t>(C, bound(k + 1) - bound(k));
   const size_t n3 = static_cast<size_t>(e->n) * 3;
   auto al = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
   const size_t b_pos = al(C * n3 * sizeof(float));
@@ -300,9 +323,9 @@ int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
 
   int launches = 0;
   for (uint64_t k = 0; k < nchunks; ++k) {
-    const uint64_t s0 = k * C;
-    if (s0 >= S) break;
-    const uint64_t Sk = std::min<uint64_t>(C, S - s0);
+    const uint64_t s0 = bound(k);
+    const uint64_t Sk = bound(k + 1) - s0;
+    if (Sk == 0) continue;
     const int sl = static_cast<int>(k % nslots);
     Slot& slot = slots[sl];
     // positions up once the slot's previous chunk has been integrated

@@ -136,9 +136,10 @@ int ce_get_tuning(const ce_engine* e, ce_tuning* t);
 /* Integrate S explosions of the fixed molecule from rest.
  * pos: [S][N][3] float initial positions (host for ce_run, device for
  * ce_run_device). ce_run copies in, runs and copies out synchronously, in up to
- * sixteen chunks whose copies overlap the integration of the neighbouring chunks
- * when the host buffers are pinned (neighbouring chunks integrate on two streams,
- * so one chunk's last simulations overlap the next chunk's first);
+ * sixteen chunks (smaller at both ends) whose copies overlap the integration of
+ * the neighbouring chunks when the host buffers are pinned (neighbouring chunks
+ * integrate on two streams, so one chunk's last simulations overlap the next
+ * chunk's first);
  * ce_run_device enqueues on `stream` (cudaStream_t, NULL = legacy default) and
  * returns without synchronizing. S == 0 is a no-op. */
 int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,

@@ -154,13 +154,13 @@ def test_ragged_sizes_and_empty(engine, ce, wl):
 
 def test_chunked_host_path_matches_device_path(engine, ce, wl):
     # ce_run cuts a batch above 2^17 sims into chunks that alternate between two
-    # device slots, each integrated on its own stream with its own work queue; an
-    # uneven batch of 5 chunks must give bit for bit what one ce_run_device
-    # launch gives, in every output.
+    # device slots, each integrated on its own stream with its own work queue (7
+    # chunks here, the two at each end tapered); the batch must give bit for bit
+    # what one ce_run_device launch gives, in every output.
     torch = pytest.importorskip("torch")
     mol = wl.CH4
     engine.set_molecule(mol.masses_me, mol.charge_array)
-    S = 5 * 65536 + 777
+    S = 7 * 65536 + 777
     pos = wl.sample_molecule(mol, S, seed=41).astype(np.float32)
     cfg = cfg_for(ce, wl.TIGHT, 3)
     host = engine.run(pos, cfg, diagnostics=True)
