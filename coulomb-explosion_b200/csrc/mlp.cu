@@ -360,7 +360,7 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                : "memory");
 }
 // 1-D bulk copy global -> this CTA's shared memory, completion reported as
-// transaction bytes on `bar` (no multicast).
+// transaction bytes on `bar`; the destination is this CTA alone.
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                    umma::smem_addr(dst)),
