@@ -150,6 +150,25 @@ int ce_get_tuning(const ce_engine* e, ce_tuning* t) {
 
 }  // extern "C"
 
+namespace ce {
+
+int ensure_pipeline(ce_engine* e) {
+  if (e->s_in) return CE_OK;
+  cudaError_t st;
+  if ((st = cudaStreamCreateWithFlags(&e->s_in, cudaStreamNonBlocking)) != cudaSuccess ||
+      (st = cudaStreamCreateWithFlags(&e->s_out, cudaStreamNonBlocking)) != cudaSuccess ||
+      (st = cudaStreamCreateWithFlags(&e->s_comp2, cudaStreamNonBlocking)) != cudaSuccess)
+    return cuda_fail(e, st, "cudaStreamCreate(pipeline streams)");
+  for (int i = 0; i < 2; ++i)
+    if ((st = cudaEventCreateWithFlags(&e->ev_loaded[i], cudaEventDisableTiming)) != cudaSuccess ||
+        (st = cudaEventCreateWithFlags(&e->ev_computed[i], cudaEventDisableTiming)) != cudaSuccess ||
+        (st = cudaEventCreateWithFlags(&e->ev_copied[i], cudaEventDisableTiming)) != cudaSuccess)
+      return cuda_fail(e, st, "cudaEventCreate");
+  return CE_OK;
+}
+
+}  // namespace ce
+
 namespace {
 
 // One fixed-molecule launch on `s`, its work queue at `cursor` (reset to 0 on
@@ -229,46 +248,14 @@ int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
   if (S > (1ull << 40)) return ce::fail(e, CE_ERR_INVALID, "ce_run: S too large");
   cudaError_t st = cudaSetDevice(e->device);
   if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaSetDevice");
-  if (!e->s_in) {
-    if ((st = cudaStreamCreateWithFlags(&e->s_in, cudaStreamNonBlocking)) != cudaSuccess ||
-        (st = cudaStreamCreateWithFlags(&e->s_out, cudaStreamNonBlocking)) != cudaSuccess ||
-        (st = cudaStreamCreateWithFlags(&e->s_comp2, cudaStreamNonBlocking)) != cudaSuccess)
-      return ce::cuda_fail(e, st, "cudaStreamCreate(pipeline streams)");
-    for (int i = 0; i < 2; ++i)
-      if ((st = cudaEventCreateWithFlags(&e->ev_loaded[i], cudaEventDisableTiming)) != cudaSuccess ||
-          (st = cudaEventCreateWithFlags(&e->ev_computed[i], cudaEventDisableTiming)) != cudaSuccess ||
-          (st = cudaEventCreateWithFlags(&e->ev_copied[i], cudaEventDisableTiming)) != cudaSuccess)
-        return ce::cuda_fail(e, st, "cudaEventCreate");
-  }
+  rc = ce::ensure_pipeline(e);
+  if (rc != CE_OK) return rc;
 
   // chunking: one chunk below 2^17 sims, else up to 16 chunks of at least 2^16
   // (measured on CH4 1e6: 8 chunks 1.79e8/s end to end, 16 1.85e8, 32 1.75e8)
-  constexpr uint64_t kMinChunk = 1ull << 16;
-  const uint64_t nchunks = S < 2 * kMinChunk ? 1 : std::min<uint64_t>(16, S / kMinChunk);
-  // Chunk k spans [bnd[k], bnd[k + 1]). From 6 chunks on, the first and last two
-  // are tapered (weights 1/4, 1/2, 1, ..., 1, 1/2, 1/4), so the copy-in before
-  // the first kernel and the copy-out after the last are short. C is the largest.
-  uint64_t bnd[17];
-  {
-    const bool taper = nchunks >= 6;
-    auto w = [&](uint64_t k) -> uint64_t {  // in quarters
-      if (!taper) return 4;
-      if (k == 0 || k + 1 == nchunks) return 1;
-      if (k == 1 || k + 2 == nchunks) return 2;
-      return 4;
-    };
-    uint64_t wsum = 0;
-    for (uint64_t k = 0; k < nchunks; ++k) wsum += w(k);
-    uint64_t acc = 0;
-    for (uint64_t k = 0; k < nchunks; ++k) {
-      bnd[k] = S * acc / wsum;  // S <= 2^40 and acc <= 64: no overflow
-      acc += w(k);
-    }
-    bnd[nchunks] = S;
-  }
+  uint64_t bnd[17], C = 0;
+  const uint64_t nchunks = ce::chunk_bounds(S, 1ull << 16, 16, bnd, &C);
   auto bound = [&](uint64_t k) -> uint64_t { return bnd[k]; };
-  uint64_t C = 0;
-  for (uint64_t k = 0; k < nchunks; ++k) C = std::max<uint64_t>(C, bound(k + 1) - bound(k));
   const size_t n3 = static_cast<size_t>(e->n) * 3;
   auto al = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
   const size_t b_pos = al(C * n3 * sizeof(float));

@@ -126,4 +126,39 @@ int run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double 
                      const ce_outputs* out, int schedule, void* stream, bool skip_empty);
 
 
+// Chunk bounds of the pipelined host-buffer paths: nchunks = 1 below
+// 2 * min_chunk sims, else min(max_chunks, S / min_chunk) (max_chunks <= 16); chunk
+// k spans [bnd[k], bnd[k + 1]). From 6 chunks on, the first and last two are
+// tapered (weights 1/4, 1/2, 1, ..., 1, 1/2, 1/4), which keeps the copy-in before
+// the first kernel and the copy-out after the last short. Returns nchunks; *cmax is
+// the largest chunk.
+inline uint64_t chunk_bounds(uint64_t S, uint64_t min_chunk, uint64_t max_chunks, uint64_t (&bnd)[17],
+                             uint64_t* cmax) {
+  const uint64_t nchunks = S < 2 * min_chunk ? 1 : (S / min_chunk < max_chunks ? S / min_chunk : max_chunks);
+  const bool taper = nchunks >= 6;
+  auto w = [&](uint64_t k) -> uint64_t {  // in quarters
+    if (!taper) return 4;
+    if (k == 0 || k + 1 == nchunks) return 1;
+    if (k == 1 || k + 2 == nchunks) return 2;
+    return 4;
+  };
+  uint64_t wsum = 0;
+  for (uint64_t k = 0; k < nchunks; ++k) wsum += w(k);
+  uint64_t acc = 0;
+  for (uint64_t k = 0; k < nchunks; ++k) {
+    bnd[k] = S * acc / wsum;  // S <= 2^40 and acc <= 64: no overflow
+    acc += w(k);
+  }
+  bnd[nchunks] = S;
+  uint64_t c = 0;
+  for (uint64_t k = 0; k < nchunks; ++k) c = bnd[k + 1] - bnd[k] > c ? bnd[k + 1] - bnd[k] : c;
+  *cmax = c;
+  return nchunks;
+}
+
+// Creates, once per engine, the copy-in / copy-out streams, the second compute
+// stream and the per-slot events of the pipelined host-buffer paths. Defined in
+// ce_gpu.cu.
+int ensure_pipeline(ce_engine* e);
+
 }  // namespace ce

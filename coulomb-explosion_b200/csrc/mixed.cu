@@ -256,6 +256,12 @@ int run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double 
 
 extern "C" {
 
+// Host-buffer path, pipelined like ce_run: the batch is cut into up to 8 chunks
+// that alternate between two device slots; chunk k's inputs go up on a copy-in
+// stream while chunk k-1 integrates on the engine stream and chunk k-2's results
+// come down on a copy-out stream (with pinned host buffers the copies overlap the
+// kernels). The chunks integrate one after another on the engine stream, since
+// they share the engine's bucket-sort scratch.
 int ce_run_mixed(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coulomb_k, const ce_run_config* cfg,
                  const ce_outputs* out) {
   if (!e) return CE_ERR_INVALID;
@@ -263,20 +269,30 @@ int ce_run_mixed(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coul
   if (rc != CE_OK || S == 0) return rc;
   cudaError_t st = cudaSetDevice(e->device);
   if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaSetDevice");
+  rc = ce::ensure_pipeline(e);
+  if (rc != CE_OK) return rc;
+  uint64_t bnd[17], C = 0;
+  const uint64_t nchunks = ce::chunk_bounds(S, 1ull << 17, 8, bnd, &C);
+  rc = ce_reserve_mixed(e, C);  // before any chunk is queued: a reallocation synchronises
+  if (rc != CE_OK) return rc;
+
   const size_t A = CE_MAX_ATOMS;
   auto al = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
-  const size_t sizes[] = {al(S),                              // n_atoms
-                          al(S * A * sizeof(double)),         // mass
-                          al(S * A * sizeof(double)),         // charge
-                          al(S * A * 3 * sizeof(float)),      // pos
-                          al(S * A * 3 * sizeof(float)),      // momenta
-                          al(S * sizeof(double)) * 5,         // ker, t_final, pe_final, ke_before, e0
-                          al(S * sizeof(uint32_t)) * 2,       // steps, rejects
-                          al(S),                              // status
-                          al(S * A * 3 * sizeof(float))};     // positions at termination
-  size_t total = 0;
-  for (size_t b : sizes) total += b;
+  const size_t sizes[] = {al(C),                              // n_atoms
+                          al(C * A * sizeof(double)),         // mass
+                          al(C * A * sizeof(double)),         // charge
+                          al(C * A * 3 * sizeof(float)),      // pos
+                          al(C * A * 3 * sizeof(float)),      // momenta
+                          al(C * sizeof(double)) * 5,         // ker, t_final, pe_final, ke_before, e0
+                          al(C * sizeof(uint32_t)) * 2,       // steps, rejects
+                          al(C),                              // status
+                          al(C * A * 3 * sizeof(float))};     // positions at termination
+  size_t slot_bytes = 0;
+  for (size_t b : sizes) slot_bytes += b;
+  const int nslots = nchunks > 1 ? 2 : 1;
+  const size_t total = slot_bytes * nslots;
   if (total > e->arena_bytes) {
+    cudaDeviceSynchronize();
     if (e->d_arena) cudaFree(e->d_arena);
     e->d_arena = nullptr;
     e->arena_bytes = 0;
@@ -284,64 +300,100 @@ int ce_run_mixed(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coul
     if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMalloc(arena)");
     e->arena_bytes = total;
   }
-  char* p = static_cast<char*>(e->d_arena);
-  ce_mixed_batch d_in;
-  d_in.n_atoms = reinterpret_cast<const uint8_t*>(p);
-  char* d_n = p;
-  p += sizes[0];
-  char* d_m = p;
-  d_in.mass_me = reinterpret_cast<const double*>(p);
-  p += sizes[1];
-  char* d_q = p;
-  d_in.charge = reinterpret_cast<const double*>(p);
-  p += sizes[2];
-  char* d_x = p;
-  d_in.pos = reinterpret_cast<const float*>(p);
-  p += sizes[3];
-  ce_outputs d{};
-  d.momenta = reinterpret_cast<float*>(p);
-  p += sizes[4];
-  const size_t bd = al(S * sizeof(double));
-  d.ker = out->ker ? reinterpret_cast<double*>(p) : nullptr;
-  d.t_final = out->t_final ? reinterpret_cast<double*>(p + bd) : nullptr;
-  d.pe_final = out->pe_final ? reinterpret_cast<double*>(p + 2 * bd) : nullptr;
-  d.ke_before = out->ke_before ? reinterpret_cast<double*>(p + 3 * bd) : nullptr;
-  d.e0 = out->e0 ? reinterpret_cast<double*>(p + 4 * bd) : nullptr;
-  p += sizes[5];
-  const size_t bu = al(S * sizeof(uint32_t));
-  d.steps = out->steps ? reinterpret_cast<uint32_t*>(p) : nullptr;
-  d.rejects = out->rejects ? reinterpret_cast<uint32_t*>(p + bu) : nullptr;
-  p += sizes[6];
-  d.status = out->status ? reinterpret_cast<uint8_t*>(p) : nullptr;
-  p += sizes[7];
-  d.positions = out->positions ? reinterpret_cast<float*>(p) : nullptr;
+  struct Slot {
+    char *n, *m, *q, *x;
+    ce_outputs d;
+  } slots[2];
+  const size_t bd = al(C * sizeof(double)), bu = al(C * sizeof(uint32_t));
+  for (int k = 0; k < nslots; ++k) {
+    char* p = static_cast<char*>(e->d_arena) + k * slot_bytes;
+    Slot& sl = slots[k];
+    sl.n = p;
+    p += sizes[0];
+    sl.m = p;
+    p += sizes[1];
+    sl.q = p;
+    p += sizes[2];
+    sl.x = p;
+    p += sizes[3];
+    sl.d = ce_outputs{};
+    sl.d.momenta = reinterpret_cast<float*>(p);
+    p += sizes[4];
+    sl.d.ker = out->ker ? reinterpret_cast<double*>(p) : nullptr;
+    sl.d.t_final = out->t_final ? reinterpret_cast<double*>(p + bd) : nullptr;
+    sl.d.pe_final = out->pe_final ? reinterpret_cast<double*>(p + 2 * bd) : nullptr;
+    sl.d.ke_before = out->ke_before ? reinterpret_cast<double*>(p + 3 * bd) : nullptr;
+    sl.d.e0 = out->e0 ? reinterpret_cast<double*>(p + 4 * bd) : nullptr;
+    p += sizes[5];
+    sl.d.steps = out->steps ? reinterpret_cast<uint32_t*>(p) : nullptr;
+    sl.d.rejects = out->rejects ? reinterpret_cast<uint32_t*>(p + bu) : nullptr;
+    p += sizes[6];
+    sl.d.status = out->status ? reinterpret_cast<uint8_t*>(p) : nullptr;
+    p += sizes[7];
+    sl.d.positions = out->positions ? reinterpret_cast<float*>(p) : nullptr;
+  }
 
   struct Copy {
     void* dst;
     const void* src;
     size_t bytes;
   };
-  const Copy h2d[] = {{d_n, in->n_atoms, S},
-                      {d_m, in->mass_me, S * A * sizeof(double)},
-                      {d_q, in->charge, S * A * sizeof(double)},
-                      {d_x, in->pos, S * A * 3 * sizeof(float)}};
-  for (const Copy& c : h2d) {
-    st = cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyHostToDevice, e->stream);
-    if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMemcpyAsync(H2D)");
+  int launches = 0;
+  for (uint64_t k = 0; k < nchunks; ++k) {
+    const uint64_t s0 = bnd[k], Sk = bnd[k + 1] - bnd[k];
+    if (Sk == 0) continue;
+    const int si = static_cast<int>(k % nslots);
+    Slot& sl = slots[si];
+    // inputs up once the slot's previous chunk has been integrated
+    if (k >= 2 && (st = cudaStreamWaitEvent(e->s_in, e->ev_computed[si], 0)) != cudaSuccess)
+      return ce::cuda_fail(e, st, "cudaStreamWaitEvent");
+    const Copy h2d[] = {{sl.n, in->n_atoms + s0, Sk},
+                        {sl.m, in->mass_me + s0 * A, Sk * A * sizeof(double)},
+                        {sl.q, in->charge + s0 * A, Sk * A * sizeof(double)},
+                        {sl.x, in->pos + s0 * A * 3, Sk * A * 3 * sizeof(float)}};
+    for (const Copy& c : h2d) {
+      st = cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyHostToDevice, e->s_in);
+      if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMemcpyAsync(H2D)");
+    }
+    cudaEventRecord(e->ev_loaded[si], e->s_in);
+    // integrate once the inputs are in and the slot's previous results are out
+    cudaStreamWaitEvent(e->stream, e->ev_loaded[si], 0);
+    if (k >= 2) cudaStreamWaitEvent(e->stream, e->ev_copied[si], 0);
+    // the kernels write atoms < n only: clear the rows, so the padding that comes
+    // back is zero and not an earlier chunk's
+    st = cudaMemsetAsync(sl.d.momenta, 0, Sk * A * 3 * sizeof(float), e->stream);
+    if (st == cudaSuccess && sl.d.positions)
+      st = cudaMemsetAsync(sl.d.positions, 0, Sk * A * 3 * sizeof(float), e->stream);
+    if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMemsetAsync(rows)");
+    const ce_mixed_batch d_in{reinterpret_cast<const uint8_t*>(sl.n), reinterpret_cast<const double*>(sl.m),
+                              reinterpret_cast<const double*>(sl.q), reinterpret_cast<const float*>(sl.x)};
+    rc = ce_run_mixed_device(e, Sk, &d_in, coulomb_k, cfg, &sl.d, e->tuned_schedule, e->stream);
+    if (rc != CE_OK) return rc;
+    launches += e->last_launches;
+    cudaEventRecord(e->ev_computed[si], e->stream);
+    // results down
+    cudaStreamWaitEvent(e->s_out, e->ev_computed[si], 0);
+    const Copy d2h[] = {
+        {out->momenta + s0 * A * 3, sl.d.momenta, Sk * A * 3 * sizeof(float)},
+        {out->ker ? out->ker + s0 : nullptr, sl.d.ker, Sk * sizeof(double)},
+        {out->t_final ? out->t_final + s0 : nullptr, sl.d.t_final, Sk * sizeof(double)},
+        {out->pe_final ? out->pe_final + s0 : nullptr, sl.d.pe_final, Sk * sizeof(double)},
+        {out->ke_before ? out->ke_before + s0 : nullptr, sl.d.ke_before, Sk * sizeof(double)},
+        {out->steps ? out->steps + s0 : nullptr, sl.d.steps, Sk * sizeof(uint32_t)},
+        {out->rejects ? out->rejects + s0 : nullptr, sl.d.rejects, Sk * sizeof(uint32_t)},
+        {out->status ? out->status + s0 : nullptr, sl.d.status, Sk},
+        {out->positions ? out->positions + s0 * A * 3 : nullptr, sl.d.positions, Sk * A * 3 * sizeof(float)},
+        {out->e0 ? out->e0 + s0 : nullptr, sl.d.e0, Sk * sizeof(double)}};
+    for (const Copy& c : d2h) {
+      if (!c.dst) continue;
+      st = cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, e->s_out);
+      if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMemcpyAsync(D2H)");
+    }
+    cudaEventRecord(e->ev_copied[si], e->s_out);
   }
-  rc = ce_run_mixed_device(e, S, &d_in, coulomb_k, cfg, &d, e->tuned_schedule, e->stream);
-  if (rc != CE_OK) return rc;
-  const Copy d2h[] = {{out->momenta, d.momenta, S * A * 3 * sizeof(float)}, {out->ker, d.ker, S * sizeof(double)},
-                      {out->t_final, d.t_final, S * sizeof(double)},     {out->pe_final, d.pe_final, S * sizeof(double)},
-                      {out->ke_before, d.ke_before, S * sizeof(double)}, {out->steps, d.steps, S * sizeof(uint32_t)},
-                      {out->rejects, d.rejects, S * sizeof(uint32_t)},   {out->status, d.status, S},
-                      {out->positions, d.positions, S * A * 3 * sizeof(float)}, {out->e0, d.e0, S * sizeof(double)}};
-  for (const Copy& c : d2h) {
-    if (!c.dst) continue;
-    st = cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, e->stream);
-    if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMemcpyAsync(D2H)");
-  }
-  st = cudaStreamSynchronize(e->stream);
+  e->last_launches = launches;
+  st = cudaStreamSynchronize(e->s_out);
+  if (st == cudaSuccess) st = cudaStreamSynchronize(e->stream);
   if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaStreamSynchronize");
   return CE_OK;
 }

@@ -188,7 +188,9 @@ int ce_reserve_mixed(ce_engine* e, uint64_t S);
 int ce_run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coulomb_k,
                         const ce_run_config* cfg, const ce_outputs* out, int schedule, void* stream);
 /* Host buffers, synchronous; one-launch schedule unless ce_autotune_mixed found
- * the per-size schedule faster. */
+ * the per-size schedule faster. Up to 8 chunks whose copies overlap the
+ * neighbouring chunks' integration when the host buffers are pinned. Whole rows
+ * come back: entries past n in out->momenta and out->positions are zero. */
 int ce_run_mixed(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coulomb_k,
                  const ce_run_config* cfg, const ce_outputs* out);
 

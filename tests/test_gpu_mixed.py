@@ -109,6 +109,27 @@ def _device_out(torch, ce, S):
     return d, o
 
 
+def test_chunked_host_mixed_path_matches_device_path(engine, ce, wl):
+    # ce_run_mixed cuts a batch of 2^18 sims or more into chunks over two device
+    # slots with the copies on side streams (3 chunks here); every chunk's result
+    # must equal one ce_run_mixed_device launch over the whole batch, bit for bit.
+    torch = pytest.importorskip("torch")
+    S = 3 * 131072 + 123
+    n_per, m, q, pos = wl.sample_mixed(S, seed=51)
+    cfg = tight(ce, wl)
+    host = engine.run_mixed(n_per, m, q, pos, cfg)
+    keep, batch = _device_batch(torch, ce, n_per, m, q, pos)
+    d, o = _device_out(torch, ce, S)
+    stream = torch.cuda.Stream()
+    engine.run_mixed_device(S, batch, cfg, o, ce.CE_SCHEDULE_ONE_LAUNCH, stream.cuda_stream)
+    stream.synchronize()
+    assert (host.status == 0).all()
+    np.testing.assert_array_equal(host.momenta, d["m"].cpu().numpy())
+    np.testing.assert_array_equal(host.ker, d["k"].cpu().numpy())
+    np.testing.assert_array_equal(host.steps, d["s"].cpu().numpy().astype(np.uint32))
+    np.testing.assert_array_equal(host.status, d["t"].cpu().numpy())
+
+
 def test_schedules_and_graph_replay_are_bit_identical(engine, ce, wl):
     torch = pytest.importorskip("torch")
     S = 5000
