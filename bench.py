@@ -516,8 +516,17 @@ def run_closure(args):
     c_lo = ce.CeOutputs(lo_m.data_ptr(), None, lo_s.data_ptr(), lo_st.data_ptr(), None, None, lo_d[1].data_ptr(),
                         None, lo_x.data_ptr(), lo_d[2].data_ptr())
     ms_loose = timed(lambda: eng.run_mixed_device(S, batch_c, lcfg, c_lo, sched, stream.cuda_stream))
-    fb_batch = ce.CeMixedBatch(fbf.data_ptr(), sb.mass.data_ptr(), sb.charge.data_ptr(), sb.pos.data_ptr())
-    ms_fb = timed(lambda: eng.run_mixed_device(S, fb_batch, cfg, c_lo, sched, stream.cuda_stream))
+    # the plain rerun of the sims the gate sent back, on those rows alone (the serve
+    # skips the accepted rows; it also sorts all S rows, which stays in "rest")
+    idx = torch.nonzero(fbf).squeeze(1)
+    n_fb = int(idx.numel())
+    ms_fb = 0.0
+    if n_fb:
+        fb = cl.DeviceBatch(fbf[idx].contiguous(), sb.mass[idx].contiguous(), sb.charge[idx].contiguous(),
+                            sb.pos[idx].contiguous())
+        fb_c = fb.c()
+        ms_fb = timed(lambda: eng.run_mixed_device(n_fb, fb_c, cfg, c_lo, sched, stream.cuda_stream))
+        del fb
     del lo_m, lo_x, lo_d, lo_s, lo_st
 
     # network forward alone (tensor-core roofline of the learned part)
