@@ -9,11 +9,12 @@
 //
 // Per force evaluation a lane reads its partners' positions from their lanes
 // with register shuffles; the partner set is fixed per lane, so there is no
-// self pair, and the lane's pair constants k q_i q_j sit in registers. Each pair term is evaluated by one lane of the pair and handed to
-// the other with shuffles (Newton's third law, see lane_force). Sums over a simulation (error norm, potential, kinetic energy,
-// Hairer norms) are gathered with N shuffles in a fixed order, so every lane of
-// a group holds the bit-identical value and takes the same accept/reject and
-// stop decisions.
+// self pair, and the lane's pair constants k q_i q_j sit in registers. Each pair
+// term is evaluated by one lane of the pair and handed to the other with
+// shuffles (Newton's third law, see lane_force). Sums over a simulation (error
+// norm, potential, kinetic energy, Hairer norms) are gathered with N shuffles in
+// a fixed order, so every lane of a group holds the bit-identical value and
+// takes the same accept/reject and stop decisions.
 //
 // Control flow is warp-uniform: every lane executes every attempt (lanes whose
 // simulation is finished, or that carry no atom, compute on stale data and
