@@ -893,7 +893,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--sims", type=int, default=S_DEFAULT)
-    ap.add_argument("--mode", type=int, default=3, help="CE_PREC_* bits")
+    ap.add_argument("--mode", type=int, default=0,
+                    help="CE_PREC_* bits: 0 plain FP32 (the f32 the workloads name, like the reference f32 engine); "
+                         "1 Kahan x/v, 2 FP64 t/E, 3 both (see --workload precision)")
     ap.add_argument("--lanes", type=int, default=0, help="lanes per sim: 0 auto, 1 thread-per-sim, N lane-per-atom")
     ap.add_argument("--block", type=int, default=0, help="threads per block (0: engine default)")
     ap.add_argument("--molecule", default="ch4", choices=["ch4", "c2h6", "h2o"],
