@@ -316,20 +316,19 @@ int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
     const int sl = static_cast<int>(k % nslots);
     Slot& slot = slots[sl];
     // positions up once the slot's previous chunk has been integrated
-    if (k >= 2 && (st = cudaStreamWaitEvent(e->s_in, e->ev_computed[sl], 0)) != cudaSuccess)
-      return ce::cuda_fail(e, st, "cudaStreamWaitEvent");
+    if (k >= 2 && (rc = ce::wait_on(e, e->s_in, e->ev_computed[sl])) != CE_OK) return rc;
     st = cudaMemcpyAsync(slot.pos, pos + s0 * n3, Sk * n3 * sizeof(float), cudaMemcpyHostToDevice, e->s_in);
     if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMemcpyAsync(pos H2D)");
-    cudaEventRecord(e->ev_loaded[sl], e->s_in);
+    if ((rc = ce::record(e, e->ev_loaded[sl], e->s_in)) != CE_OK) return rc;
     // integrate once the positions are in and the slot's previous results are out
-    cudaStreamWaitEvent(slot.s, e->ev_loaded[sl], 0);
-    if (k >= 2) cudaStreamWaitEvent(slot.s, e->ev_copied[sl], 0);
+    if ((rc = ce::wait_on(e, slot.s, e->ev_loaded[sl])) != CE_OK) return rc;
+    if (k >= 2 && (rc = ce::wait_on(e, slot.s, e->ev_copied[sl])) != CE_OK) return rc;
     rc = launch_fixed(e, Sk, slot.pos, cfg, &slot.d, slot.s, slot.cursor);
     if (rc != CE_OK) return rc;
     launches += e->last_launches;
-    cudaEventRecord(e->ev_computed[sl], slot.s);
+    if ((rc = ce::record(e, e->ev_computed[sl], slot.s)) != CE_OK) return rc;
     // results down
-    cudaStreamWaitEvent(e->s_out, e->ev_computed[sl], 0);
+    if ((rc = ce::wait_on(e, e->s_out, e->ev_computed[sl])) != CE_OK) return rc;
     struct Copy {
       void* dst;
       const void* src;
@@ -350,7 +349,7 @@ int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
       st = cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, e->s_out);
       if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMemcpyAsync(D2H)");
     }
-    cudaEventRecord(e->ev_copied[sl], e->s_out);
+    if ((rc = ce::record(e, e->ev_copied[sl], e->s_out)) != CE_OK) return rc;
   }
   e->last_launches = launches;
   st = cudaStreamSynchronize(e->s_out);

@@ -156,6 +156,17 @@ inline uint64_t chunk_bounds(uint64_t S, uint64_t min_chunk, uint64_t max_chunks
   return nchunks;
 }
 
+// Event record / stream wait of the pipelined host-buffer paths, checked: a
+// dependency that failed to register would let a copy race its kernel.
+inline int record(ce_engine* e, cudaEvent_t ev, cudaStream_t s) {
+  const cudaError_t st = cudaEventRecord(ev, s);
+  return st == cudaSuccess ? CE_OK : cuda_fail(e, st, "cudaEventRecord");
+}
+inline int wait_on(ce_engine* e, cudaStream_t s, cudaEvent_t ev) {
+  const cudaError_t st = cudaStreamWaitEvent(s, ev, 0);
+  return st == cudaSuccess ? CE_OK : cuda_fail(e, st, "cudaStreamWaitEvent");
+}
+
 // Creates, once per engine, the copy-in / copy-out streams, the second compute
 // stream and the per-slot events of the pipelined host-buffer paths. Defined in
 // ce_gpu.cu.

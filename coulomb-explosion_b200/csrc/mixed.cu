@@ -345,8 +345,7 @@ int ce_run_mixed(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coul
     const int si = static_cast<int>(k % nslots);
     Slot& sl = slots[si];
     // inputs up once the slot's previous chunk has been integrated
-    if (k >= 2 && (st = cudaStreamWaitEvent(e->s_in, e->ev_computed[si], 0)) != cudaSuccess)
-      return ce::cuda_fail(e, st, "cudaStreamWaitEvent");
+    if (k >= 2 && (rc = ce::wait_on(e, e->s_in, e->ev_computed[si])) != CE_OK) return rc;
     const Copy h2d[] = {{sl.n, in->n_atoms + s0, Sk},
                         {sl.m, in->mass_me + s0 * A, Sk * A * sizeof(double)},
                         {sl.q, in->charge + s0 * A, Sk * A * sizeof(double)},
@@ -355,10 +354,10 @@ int ce_run_mixed(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coul
       st = cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyHostToDevice, e->s_in);
       if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMemcpyAsync(H2D)");
     }
-    cudaEventRecord(e->ev_loaded[si], e->s_in);
+    if ((rc = ce::record(e, e->ev_loaded[si], e->s_in)) != CE_OK) return rc;
     // integrate once the inputs are in and the slot's previous results are out
-    cudaStreamWaitEvent(e->stream, e->ev_loaded[si], 0);
-    if (k >= 2) cudaStreamWaitEvent(e->stream, e->ev_copied[si], 0);
+    if ((rc = ce::wait_on(e, e->stream, e->ev_loaded[si])) != CE_OK) return rc;
+    if (k >= 2 && (rc = ce::wait_on(e, e->stream, e->ev_copied[si])) != CE_OK) return rc;
     // the kernels write atoms < n only: clear the rows, so the padding that comes
     // back is zero and not an earlier chunk's
     st = cudaMemsetAsync(sl.d.momenta, 0, Sk * A * 3 * sizeof(float), e->stream);
@@ -370,9 +369,9 @@ int ce_run_mixed(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coul
     rc = ce_run_mixed_device(e, Sk, &d_in, coulomb_k, cfg, &sl.d, e->tuned_schedule, e->stream);
     if (rc != CE_OK) return rc;
     launches += e->last_launches;
-    cudaEventRecord(e->ev_computed[si], e->stream);
+    if ((rc = ce::record(e, e->ev_computed[si], e->stream)) != CE_OK) return rc;
     // results down
-    cudaStreamWaitEvent(e->s_out, e->ev_computed[si], 0);
+    if ((rc = ce::wait_on(e, e->s_out, e->ev_computed[si])) != CE_OK) return rc;
     const Copy d2h[] = {
         {out->momenta + s0 * A * 3, sl.d.momenta, Sk * A * 3 * sizeof(float)},
         {out->ker ? out->ker + s0 : nullptr, sl.d.ker, Sk * sizeof(double)},
@@ -389,7 +388,7 @@ int ce_run_mixed(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coul
       st = cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, e->s_out);
       if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMemcpyAsync(D2H)");
     }
-    cudaEventRecord(e->ev_copied[si], e->s_out);
+    if ((rc = ce::record(e, e->ev_copied[si], e->s_out)) != CE_OK) return rc;
   }
   e->last_launches = launches;
   st = cudaStreamSynchronize(e->s_out);
