@@ -53,7 +53,8 @@ def flops_per_sim(steps: np.ndarray, n: int) -> np.ndarray:
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed region
+    (NVML, read only; nvidia-smi as the fallback)."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -66,16 +67,40 @@ class ClockSampler:
         self._t = None
 
     def _run(self):
+        # NVML read-only queries every 10 ms (a timed region can be ~0.1 s);
+        # nvidia-smi every 0.2 s where NVML is not available.
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            bits = [pynvml.nvmlClocksEventReasonHwSlowdown, pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                    pynvml.nvmlClocksEventReasonSwThermalSlowdown, pynvml.nvmlClocksEventReasonSwPowerCap]
+        except Exception:
+            h = None
         while not self._stop.is_set():
             try:
-                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                     timeout=5).stdout.strip()
-                if out:
-                    self.rows.append([c.strip() for c in out.split(",")])
+                if h is not None:
+                    sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                    mx = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+                    pw = pynvml.nvmlDeviceGetPowerUsage(h) / 1000.0
+                    rs = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.rows.append([str(self.index), str(sm), str(mx), f"{pw:.1f}", hex(rs)] +
+                                     ["Active" if rs & b else "Not Active" for b in bits])
+                else:
+                    out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5).stdout.strip()
+                    if out:
+                        self.rows.append([c.strip() for c in out.split(",")])
             except Exception:
                 pass
-            self._stop.wait(0.2)
+            self._stop.wait(0.01 if h is not None else 0.2)
+        if h is not None:
+            try:
+                pynvml.nvmlShutdown()
+            except Exception:
+                pass
 
     def __enter__(self):
         self._t = threading.Thread(target=self._run, daemon=True)
