@@ -179,6 +179,49 @@ def test_chunked_host_path_matches_device_path(engine, ce, wl):
         np.testing.assert_array_equal(h, d[k].cpu().numpy().view(h.dtype).reshape(h.shape), err_msg=k)
 
 
+def test_full_size_invariants(engine, ce, wl):
+    # The benchmark's full size (1e6 CH4 explosions, tight point, plain FP32),
+    # checked per sim through properties that hold at any size: every sim
+    # converges, KER equals E_0 after redistribution, the momenta sum to zero
+    # (the reference's check, demo/sanity_check.py:102-106: mean over sims of
+    # |sum p| / the typical per-atom |p| below 1e-4; here also every sim's
+    # |sum p| / sum |p|), and a second run reproduces every bit.
+    torch = pytest.importorskip("torch")
+    import importlib
+
+    sp = importlib.import_module("coulomb_explosion_b200.sampling")
+    mol = wl.CH4
+    S = 1_000_000
+    pos, _, flags = sp.sample_ball_host(mol, S, seed=20261203)
+    assert not flags.any()
+    engine.set_molecule(mol.masses_me, mol.charge_array)
+    cfg = cfg_for(ce, wl.TIGHT, 0)
+    x = torch.from_numpy(pos).cuda()
+    runs = []
+    for _ in range(2):
+        mom = torch.zeros((S, mol.n, 3), dtype=torch.float32, device="cuda")
+        ker = torch.zeros(S, dtype=torch.float64, device="cuda")
+        steps = torch.zeros(S, dtype=torch.int32, device="cuda")
+        status = torch.full((S,), 255, dtype=torch.uint8, device="cuda")
+        e0 = torch.zeros(S, dtype=torch.float64, device="cuda")
+        out = ce.CeOutputs(mom.data_ptr(), ker.data_ptr(), steps.data_ptr(), status.data_ptr(), None, None, None,
+                           None, None, e0.data_ptr())
+        stream = torch.cuda.Stream()
+        engine.run_device(S, x.data_ptr(), cfg, out, stream.cuda_stream)
+        stream.synchronize()
+        runs.append([t.cpu().numpy() for t in (mom, ker, steps, status, e0)])
+    mom, ker, steps, status, e0 = runs[0]
+    assert (status == ce.CE_SIM_OK).all()
+    assert np.abs(ker / e0 - 1.0).max() < 1e-9
+    p = mom.astype(np.float64)
+    tot = np.linalg.norm(p.sum(axis=1), axis=1)
+    assert (tot / np.linalg.norm(p, axis=2).mean()).mean() < 1e-4
+    assert (tot / np.linalg.norm(p, axis=2).sum(axis=1)).max() < 1e-4
+    assert 30 < steps.mean() < 60
+    for a, b in zip(runs[0], runs[1]):
+        np.testing.assert_array_equal(a, b)
+
+
 @pytest.mark.parametrize("lanes", [1, 5])
 def test_results_independent_of_launch_shape(engine, ce, wl, lanes):
     # Each sim's arithmetic is private to its thread (or its lane group), so
