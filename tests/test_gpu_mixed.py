@@ -130,6 +130,37 @@ def test_chunked_host_mixed_path_matches_device_path(engine, ce, wl):
     np.testing.assert_array_equal(host.status, d["t"].cpu().numpy())
 
 
+def test_full_size_mixed_invariants(engine, ce, wl):
+    # The benchmark's full mixed population (1e7 sims of 2..10 atoms from the
+    # device sampler, one persistent launch, plain FP32), checked per sim on the
+    # device: every sim converges, KER equals E_0 after redistribution, and the
+    # momenta sum to zero (|sum p| / sum |p| < 1e-4, demo/sanity_check.py:102-106).
+    torch = pytest.importorskip("torch")
+    import importlib
+
+    cl = importlib.import_module("coulomb_explosion_b200.closure")
+    S = 10_000_000
+    b = cl.sample_mixed_device(S, seed=20261203)
+    cfg = tight(ce, wl, mode=0)
+    mom = torch.zeros((S, 10, 3), dtype=torch.float32, device="cuda")
+    ker = torch.zeros(S, dtype=torch.float64, device="cuda")
+    steps = torch.zeros(S, dtype=torch.int32, device="cuda")
+    status = torch.full((S,), 255, dtype=torch.uint8, device="cuda")
+    e0 = torch.zeros(S, dtype=torch.float64, device="cuda")
+    out = ce.CeOutputs(mom.data_ptr(), ker.data_ptr(), steps.data_ptr(), status.data_ptr(), None, None, None, None,
+                       None, e0.data_ptr())
+    engine.reserve_mixed(S)
+    stream = torch.cuda.Stream()
+    engine.run_mixed_device(S, b.c(), cfg, out, ce.CE_SCHEDULE_ONE_LAUNCH, stream.cuda_stream)
+    stream.synchronize()
+    assert bool((status == ce.CE_SIM_OK).all())
+    assert float((ker / e0 - 1.0).abs().max()) < 1e-9
+    tot = mom.double().sum(dim=1).norm(dim=1)
+    size = mom.double().norm(dim=2).sum(dim=1)
+    assert float((tot / size).max()) < 1e-4
+    assert 30.0 < float(steps.double().mean()) < 70.0
+
+
 def test_schedules_and_graph_replay_are_bit_identical(engine, ce, wl):
     torch = pytest.importorskip("torch")
     S = 5000
