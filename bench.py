@@ -198,7 +198,7 @@ def run_reference_arm(args):
 
 
 def run_mixed(args):
-    """Config-2 workload: a mixed population of 2..10-atom molecules (species
+    """Mixed workload: a population of 2..10-atom molecules (species
     H/C/N/O/S, charges +1..+3, ball radius 2.0 N^(1/3), pairs >= 0.5), generated
     on the device, integrated by one persistent launch (captured in a CUDA graph)
     and, for comparison, by the per-size launch schedule."""
@@ -298,7 +298,7 @@ def run_mixed(args):
     err = np.array([ol.config_norm_error(mom_one[i:i + 1, :k], ref["momenta"][j:j + 1, :k])[0]
                     for j, (i, k) in enumerate(zip(sub, nn_s))])
     line = {
-        "metric": METRIC + " [config 2: mixed 2..10-atom population]", "value": value, "unit": UNIT, "n_gpus": 1,
+        "metric": METRIC + " [mixed 2..10-atom population, 1e7 sims, one persistent launch]", "value": value, "unit": UNIT, "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_one / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"mixed population, {S} sims per step, N ~ U{{2..10}}, species U{{H,C,N,O,S}}, "
@@ -324,7 +324,7 @@ def run_mixed(args):
 
 
 def run_precision(args):
-    """Config-3 study: CH4 and stiff H2O (O q=+3, 2 H q=+1, 2.0-bohr ball, pairs
+    """Precision study: CH4 and stiff H2O (O q=+3, 2 H q=+1, 2.0-bohr ball, pairs
     >= 0.3), 1e6 sims each, every precision mode at the production and tight
     points. Errors against the FP64 reference (oracle f64 at rtol 1e-12 /
     atol 1e-20 / pe_stop 1e-13) on a 1e4 subset: per-atom |dp_i| / |p_i| and the
@@ -392,13 +392,13 @@ def run_precision(args):
                     "status_ok_frac": float((sts.cpu().numpy() == 0).mean()),
                 })
     eng.close()
-    print(json.dumps({"metric": "precision study (config 3)", "sims_per_case": S, "fp64_subset": n_sub,
+    print(json.dumps({"metric": "precision study (CH4 and stiff H2O, every precision mode)", "sims_per_case": S, "fp64_subset": n_sub,
                       "fp64_reference": "oracle f64, rtol 1e-12, atol 1e-20, pe_stop 1e-13", "rows": rows}))
     return 0
 
 
 def run_closure(args):
-    """Config-4 study: the learned closure on the mixed 2..10-atom population.
+    """Closure study: the learned closure on the mixed 2..10-atom population.
 
     Training pairs: `--train-sims` sims (default 5e6) integrated to the loose
     stop (PE <= 5% PE_0, no rescale) and, for targets, to convergence by plain
@@ -603,7 +603,7 @@ def run_closure(args):
 
     steps_c = oc["steps"].double()
     line = {
-        "metric": METRIC + " [config 4: learned closure vs plain RK45, mixed 2..10-atom population]",
+        "metric": METRIC + " [learned closure vs plain RK45, mixed 2..10-atom population, 1e7 sims]",
         "value": S / (ms_clo / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_clo, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 integration, bf16/f32-accumulate network", "data": "synthetic",
@@ -648,7 +648,7 @@ def run_closure(args):
 
 
 def run_stream(args):
-    """Config-5 production generation: `--total` (default 1e8) explosions of the
+    """Streamed production generation: `--total` (default 1e8) explosions of the
     10-atom C2H6-like molecule (2 C q=+2, 8 H q=+1, radius 4.0, pairs >= 0.5) in
     1e6-sim chunks. Per chunk, on a compute stream: Philox geometries on the
     device, then the integration replayed from a CUDA graph captured once per
@@ -831,7 +831,7 @@ def run_stream(args):
         return {"median": float(np.median(e)), "p99": float(np.percentile(e, 99)), "max": float(e.max())}
 
     line = {
-        "metric": METRIC + " [config 5: 1e8 C2H6-like N=10 explosions streamed in 1e6 chunks, closure vs plain]",
+        "metric": METRIC + " [1e8 C2H6-like N=10 explosions streamed in 1e6 chunks, closure vs plain]",
         "value": res["closure"]["explosions_per_s"], "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": 1,
         "ms_per_step": res["closure"]["seconds"] * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 integration, bf16/f32-accumulate network", "data": "synthetic",

@@ -137,7 +137,8 @@ class DeviceBatch:
 
 
 def sample_mixed_device(S: int, seed: int, first_sim: int = 0, device: int = 0, **kw) -> DeviceBatch:
-    """Config-2 population (2..10 atoms) from the device Philox sampler."""
+    """The mixed population (2..10 atoms, species H/C/N/O/S, charges +1..+3) from
+    the device Philox sampler."""
     torch = _torch()
     lib = load_library()
     dev = torch.device("cuda", device)
