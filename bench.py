@@ -12,8 +12,8 @@ atol 1e-7, pe_stop 1e-7 -- the operating point at which every sim is within
   e2e     the same through the C ABI host-buffer call (ce_run): pinned host
           positions in, momenta / KER / steps / status out, every step
   roofline  FP32 CUDA-core bound of the integration kernel (the pair force is
-          not a dense contraction): algorithmic FLOPs per launch
-          over the event-timed launch, against a measured FP32 FMA peak
+          not a dense contraction): algorithmic FLOPs (flops_per_sim) per
+          launch over the event-timed launch, against a measured FP32 FMA peak
   cpu_baseline  the reference scalar engine (built from its own sources,
           oracle/_ref) on all host cores, bounded sample
 
@@ -47,7 +47,12 @@ TIGHT = (1e-6, 1e-7, 1e-7)
 
 def flops_per_sim(steps: np.ndarray, n: int) -> np.ndarray:
     """Algorithmic FP32 FLOPs per sim: steps * (137 P + 438 N) + C_init with
-    C_init = 2 (21 P + 3 N) + 11 P + 60 N (counting rules in DESIGN.md)."""
+    C_init = 2 (21 P + 3 N) + 11 P + 60 N, P = N (N - 1) / 2 pairs. Counting:
+    add, sub and mul 1, FMA 2, rsqrt, div and sqrt 1, abs and max 0; zero
+    Butcher coefficients skipped; each pair counted once. Per accepted step: 6
+    force evaluations of 21 P + 3 N (pair: 3 sub + 5 for r^2 + 3 for r^-3 + 1
+    scale + 3 force + 6 accumulate), the potential 11 P, stage combinations
+    52 * 6N, error norm 18 * 6N. C_init: k1, the initial-step probe and PE_0."""
     p = n * (n - 1) // 2
     return steps.astype(np.float64) * (137 * p + 438 * n) + (2 * (21 * p + 3 * n) + 11 * p + 60 * n)
 
