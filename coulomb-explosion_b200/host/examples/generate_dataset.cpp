@@ -188,7 +188,7 @@ int main(int argc, char** argv) {
         }
         check(cudaMemcpyAsync(s.d_pos, s.h_pos, cnt * n3 * sizeof(float), cudaMemcpyHostToDevice, compute), "H2D");
       }
-      ce_outputs out{s.d_mom, nullptr, s.d_steps, s.d_status, nullptr, nullptr, nullptr, nullptr};
+      ce_outputs out{s.d_mom, nullptr, s.d_steps, s.d_status, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
       if (ce_run_device(e, cnt, s.d_pos, &cfg, &out, compute) != CE_OK) throw std::runtime_error(ce_last_error(e));
       check(cudaEventRecord(integrated, compute), "event");
       check(cudaStreamWaitEvent(copy, integrated, 0), "wait");

@@ -79,7 +79,8 @@ BatchedRK45::Result BatchedRK45::run(const RunConfig& cfg) {
   std::vector<std::uint8_t> status(lanes_);
   Result r;
   r.ker.resize(lanes_);
-  ce_outputs out{mom.data(), r.ker.data(), steps.data(), status.data(), rejects.data(), nullptr, nullptr, nullptr};
+  ce_outputs out{mom.data(), r.ker.data(), steps.data(), status.data(), rejects.data(), nullptr, nullptr, nullptr,
+                 nullptr, nullptr};
   const int rc = ce_run(engine_->handle(), lanes_, pos_.data(), &c, &out);
   if (rc != CE_OK) engine_->throw_last(rc, "ce_run");
   r.momenta.assign(mom.begin(), mom.end());
@@ -119,7 +120,7 @@ std::vector<RunResult> run_to_convergence_batch(const Molecule& mol, std::vector
   std::vector<std::uint32_t> steps(S), rejects(S);
   std::vector<std::uint8_t> status(S);
   ce_outputs out{mom.data(), ker.data(), steps.data(), status.data(), rejects.data(), t_final.data(),
-                 pe_final.data(), ke_before.data()};
+                 pe_final.data(), ke_before.data(), nullptr, nullptr};
   const ce_run_config c = to_c(cfg, opts.rtol, opts.atol, precision_mode);
   const int rc = ce_run(eng.handle(), S, pos.data(), &c, &out);
   if (rc != CE_OK) eng.throw_last(rc, "ce_run");
