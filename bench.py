@@ -246,7 +246,7 @@ def run_mixed(args):
 
     eng = ce.Engine(0)
     t0 = time.perf_counter()
-    report, best = eng.autotune_mixed(min(S, 1_000_000), batch, cfg)
+    report, best = ([], 0) if args.no_autotune else eng.autotune_mixed(min(S, 1_000_000), batch, cfg)
     tune_s = time.perf_counter() - t0
     eng.reserve_mixed(S)
     stream = torch.cuda.Stream(device=dev)
@@ -314,8 +314,9 @@ def run_mixed(args):
                    "l2": "flushed between timed steps (256 MiB write, outside the events)"},
         "per_size_schedule": {"value": per_size, "unit": UNIT, "ms_per_step": ms_per / args.steps,
                               "speedup_one_launch": value / per_size, "identical_results": same},
-        "autotune": {"seconds": tune_s, "best_schedule": "one_launch" if best == 0 else "per_size",
-                     "best": max(report, key=lambda r: r["sims_per_s"]), "candidates": len(report)},
+        "autotune": ({"seconds": tune_s, "best_schedule": "one_launch" if best == 0 else "per_size",
+                      "best": max(report, key=lambda r: r["sims_per_s"]), "candidates": len(report)}
+                     if report else "off (engine defaults)"),
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak["tflops"], "unit": "TFLOP/s",
                      "frac": achieved / peak["tflops"], "peak_source": peak["source"]},
         "accuracy": {"vs": "fp64 oracle (rtol 1e-10, pe_stop 1e-11)", "subset": int(len(sub)),
@@ -931,6 +932,8 @@ def main():
     ap.add_argument("--molecule", default="ch4", choices=["ch4", "c2h6", "h2o"],
                     help="ch4 (the headline workload), c2h6 (10-atom C2H6-like), h2o (stiff H2O)")
     ap.add_argument("--cpu-budget", type=float, default=8.0)
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="mixed: skip the autotuner (engine defaults), e.g. to profile a known launch shape")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="fixed",
                     choices=["fixed", "mixed", "precision", "closure", "network", "stream"],
