@@ -1,0 +1,21 @@
+// Prints the chunk schedule of the pipelined host-buffer paths (ce::chunk_bounds)
+// for the sizes given on the command line: "S nchunks cmax b0 b1 ... bn" per line.
+// Host code only; compiled by tests/test_chunking.py.
+#include <cstdio>
+#include <cstdlib>
+
+#include "engine.hpp"
+
+int main(int argc, char** argv) {
+  for (int a = 3; a < argc; ++a) {
+    const uint64_t S = std::strtoull(argv[a], nullptr, 10);
+    uint64_t bnd[17], cmax = 0;
+    const uint64_t n = ce::chunk_bounds(S, std::strtoull(argv[1], nullptr, 10), std::strtoull(argv[2], nullptr, 10),
+                                        bnd, &cmax);
+    std::printf("%llu %llu %llu", static_cast<unsigned long long>(S), static_cast<unsigned long long>(n),
+                static_cast<unsigned long long>(cmax));
+    for (uint64_t k = 0; k <= n; ++k) std::printf(" %llu", static_cast<unsigned long long>(bnd[k]));
+    std::printf("\n");
+  }
+  return 0;
+}

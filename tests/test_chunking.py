@@ -1,0 +1,49 @@
+"""Chunk schedule of the pipelined host-buffer calls (ce_run: chunks of at least
+2^16 sims, at most 16; ce_run_mixed: 2^17, at most 8), checked on the CPU: the
+chunks cover [0, S) in order with none empty, below 2 minimum chunks there is one,
+from 6 chunks on the two at each end weigh 1/4 and 1/2 of a full one, and the
+reported largest chunk is the one the device slots are sized for."""
+from __future__ import annotations
+
+import shutil
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+
+CSRC = ROOT / "coulomb-explosion_b200" / "csrc"
+SIZES = [1, 1000, 131071, 131072, 131073, 196608, 5 * 65536 + 777, 7 * 65536 + 777, 1_000_000, 10_000_000,
+         123_456_789, 1 << 40]
+
+
+@pytest.fixture(scope="module")
+def schedule(tmp_path_factory):
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    exe = tmp_path_factory.mktemp("chunk") / "chunk_bounds"
+    subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++17", "-I", str(ROOT / "include"),
+                    "-I", str(CSRC), "-o", str(exe),
+                    str(ROOT / "tests" / "cpp" / "chunk_bounds_main.cu")], check=True, capture_output=True)
+
+    def run(min_chunk, max_chunks):
+        out = subprocess.run([str(exe), str(min_chunk), str(max_chunks), *map(str, SIZES)], check=True,
+                             capture_output=True, text=True).stdout
+        return [list(map(int, line.split())) for line in out.splitlines()]
+    return run
+
+
+@pytest.mark.parametrize("min_chunk,max_chunks", [(1 << 16, 16), (1 << 17, 8)])
+def test_chunks_cover_the_batch(schedule, min_chunk, max_chunks):
+    for row in schedule(min_chunk, max_chunks):
+        S, n, cmax, bnd = row[0], row[1], row[2], row[3:]
+        assert len(bnd) == n + 1 and bnd[0] == 0 and bnd[-1] == S
+        sizes = [bnd[k + 1] - bnd[k] for k in range(n)]
+        assert min(sizes) > 0 and max(sizes) == cmax
+        expect = 1 if S < 2 * min_chunk else min(max_chunks, S // min_chunk)
+        assert n == expect
+        if n >= 6:
+            full = sizes[2]
+            for k, quarters in ((0, 1), (1, 2), (n - 2, 2), (n - 1, 1)):
+                assert abs(sizes[k] - full * quarters / 4) <= 2
+        else:
+            assert max(sizes) - min(sizes) <= 1
