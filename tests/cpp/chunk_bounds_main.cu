@@ -1,5 +1,7 @@
 // Prints the chunk schedule of the pipelined host-buffer paths (ce::chunk_bounds)
-// for the sizes given on the command line: "S nchunks cmax b0 b1 ... bn" per line.
+// for the sizes given on the command line: "S nchunks cmax b0 b1 ... bn" per line;
+// with the single argument "refill", the default refill granularity
+// (ce::default_refill) for n = 1..10 atoms: "n lane-per-atom thread-per-sim".
 // Host code only; compiled by tests/test_chunking.py.
 #include <cstdio>
 #include <cstdlib>
@@ -7,6 +9,10 @@
 #include "engine.hpp"
 
 int main(int argc, char** argv) {
+  if (argc == 2 && argv[1][0] == 'r') {
+    for (int n = 1; n <= 10; ++n) std::printf("%d %d %d\n", n, ce::default_refill(n, n), ce::default_refill(n, 1));
+    return 0;
+  }
   for (int a = 3; a < argc; ++a) {
     const uint64_t S = std::strtoull(argv[a], nullptr, 10);
     uint64_t bnd[17], cmax = 0;

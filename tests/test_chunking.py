@@ -2,7 +2,8 @@
 2^16 sims, at most 16; ce_run_mixed: 2^17, at most 8), checked on the CPU: the
 chunks cover [0, S) in order with none empty, below 2 minimum chunks there is one,
 from 6 chunks on the two at each end weigh 1/4 and 1/2 of a full one, and the
-reported largest chunk is the one the device slots are sized for."""
+reported largest chunk is the one the device slots are sized for. Also the
+default refill granularity of the lane-per-atom kernels per molecule size."""
 from __future__ import annotations
 
 import shutil
@@ -25,9 +26,9 @@ def schedule(tmp_path_factory):
                     "-I", str(CSRC), "-o", str(exe),
                     str(ROOT / "tests" / "cpp" / "chunk_bounds_main.cu")], check=True, capture_output=True)
 
-    def run(min_chunk, max_chunks):
-        out = subprocess.run([str(exe), str(min_chunk), str(max_chunks), *map(str, SIZES)], check=True,
-                             capture_output=True, text=True).stdout
+    def run(min_chunk, max_chunks=None):
+        args = [str(min_chunk)] if max_chunks is None else [str(min_chunk), str(max_chunks), *map(str, SIZES)]
+        out = subprocess.run([str(exe), *args], check=True, capture_output=True, text=True).stdout
         return [list(map(int, line.split())) for line in out.splitlines()]
     return run
 
@@ -47,3 +48,12 @@ def test_chunks_cover_the_batch(schedule, min_chunk, max_chunks):
                 assert abs(sizes[k] - full * quarters / 4) <= 2
         else:
             assert max(sizes) - min(sizes) <= 1
+
+
+def test_default_refill(schedule):
+    # floor((G - 1) / 3) idle groups of G = 32 / n sims per warp, at least one;
+    # one thread per sim refills at once
+    rows = schedule("refill")
+    assert [r[0] for r in rows] == list(range(1, 11))
+    assert {r[0]: r[1] for r in rows} == {1: 1, 2: 5, 3: 3, 4: 2, 5: 1, 6: 1, 7: 1, 8: 1, 9: 1, 10: 1}
+    assert all(r[2] == 1 for r in rows)
