@@ -16,7 +16,7 @@ units.hpp:11-14), integer charges, Coulomb constant 1 (atomic units).
 Every atom is placed independently and uniformly in the ball; a geometry with
 any pair closer than the minimum is redrawn whole. (The reference's
 UniformSphereSampler instead redraws atom by atom, src/sampler.cpp:28-57; the
-host C++ mirror of that sampler lives in host/src/sampler.cpp.)
+host C++ mirror of that sampler lives in host/src/host.cpp.)
 """
 from __future__ import annotations
 

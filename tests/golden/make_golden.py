@@ -18,13 +18,21 @@ where the reference checkout and the reference engine built from it exist).
   h2o_ref.npz           96 stiff H2O geometries, reference f32/f64 outputs.
   sampler_ref.npz       reference UniformSphereSampler draws (mt19937_64) for
                         the host C++ sampler mirror.
+  scipy_ref.npz         the reference's scipy oracle (simulate_explosion) on 48
+                        sims each of CH4, stiff H2O, the C2H6-like 10-atom
+                        molecule and the mixed 2..10-atom population (Philox
+                        geometries of the benchmark workloads), to pin the
+                        restated scipy oracle (oracle/scipy_oracle.py).
 
-Usage: python tests/golden/make_golden.py   (needs oracle/_ref, `make -C oracle`)
+Usage: python tests/golden/make_golden.py --reference <reference checkout> [--only scipy]
+(or COULOMB_REFERENCE_DIR=<checkout>); needs oracle/_ref (`make -C oracle REF=<checkout>`).
 """
 from __future__ import annotations
 
+import argparse
 import importlib.util
 import json
+import os
 import sys
 from pathlib import Path
 
@@ -32,12 +40,13 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
-REF = Path("/root/reference")
+REF: Path  # the reference checkout, from --reference or COULOMB_REFERENCE_DIR
 sys.path.insert(0, str(ROOT / "tests"))
 import oracle_lib as ol  # noqa: E402
 from pkg_loader import load_submodule  # noqa: E402
 
 wl = load_submodule("workloads")
+sp = load_submodule("sampling")
 
 
 def load_reference_oracle():
@@ -96,9 +105,52 @@ def ref_outputs(pos, mass, q, points):
     return out
 
 
+def make_scipy_ref(co):
+    """48 sims per workload through the reference's simulate_explosion."""
+    out = {}
+    count = 48
+
+    def run(pos, m, q, n_per=None):
+        p = np.zeros(pos.shape)
+        for s in range(pos.shape[0]):
+            n = pos.shape[1] if n_per is None else int(n_per[s])
+            ms = m[s] if m.ndim == 2 else m
+            qs = q[s] if q.ndim == 2 else q
+            _, vf = co.simulate_explosion(pos[s, :n], np.zeros((n, 3)), ms[:n], qs[:n])
+            p[s, :n] = ms[:n, None] * vf
+        return p
+
+    for tag, mol in (("ch4", wl.CH4), ("h2o", wl.H2O_STIFF), ("c2h6", wl.C2H6_LIKE)):
+        pos32, _, flags = sp.sample_ball_host(mol, count, seed=20261203)
+        assert not flags.any()
+        pos = pos32.astype(np.float64)
+        out[f"{tag}_pos"], out[f"{tag}_masses"], out[f"{tag}_charges"] = pos, mol.masses_me, mol.charge_array
+        out[f"{tag}_p"] = run(pos, mol.masses_me, mol.charge_array)
+    n_per, m, q, pos32, _, flags = sp.sample_mixed_host(count, 20261203)
+    assert not flags.any()
+    pos = pos32.astype(np.float64)
+    out.update(mixed_n=n_per, mixed_masses=m, mixed_charges=q, mixed_pos=pos)
+    out["mixed_p"] = run(pos, m, q, n_per)
+    np.savez_compressed(HERE / "scipy_ref.npz", **out)
+
+
 def main():
+    global REF
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=os.environ.get("COULOMB_REFERENCE_DIR"),
+                    help="the reference checkout (or COULOMB_REFERENCE_DIR)")
+    ap.add_argument("--only", choices=["scipy"], default=None, help="regenerate one fixture only")
+    args = ap.parse_args()
+    if not args.reference:
+        ap.error("give the reference checkout with --reference or COULOMB_REFERENCE_DIR")
+    REF = Path(args.reference)
     co = load_reference_oracle()
+    if args.only == "scipy":
+        make_scipy_ref(co)
+        print("scipy_ref.npz written to", HERE)
+        return
     make_reference_cases(co)
+    make_scipy_ref(co)
     points = {"prod": wl.PRODUCTION, "tight": wl.TIGHT}
 
     # CH4, 256 sims.

@@ -2,6 +2,9 @@
 
   oracle/libce_oracle.so   the C restatement of the reference scalar engine
   oracle/_ref/libref_*.so  the reference scalar engine built from its own sources
+  oracle/_ref/libref_batched_<isa>.so  the reference SIMD batched engine
+                           (BatchedRK45<T>) built from its unmodified headers
+                           against the project's Highway-API shim
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this.
 """
@@ -16,6 +19,7 @@ ROOT = Path(__file__).resolve().parents[1]
 ORACLE_SO = ROOT / "oracle" / "libce_oracle.so"
 REF_F32_SO = ROOT / "oracle" / "_ref" / "libref_f32.so"
 REF_F64_SO = ROOT / "oracle" / "_ref" / "libref_f64.so"
+REF_BATCHED_SO = {isa: ROOT / "oracle" / "_ref" / f"libref_batched_{isa}.so" for isa in ("avx512", "avx2")}
 
 KAHAN = 1
 FP64 = 2
@@ -103,6 +107,75 @@ def ref(bits: int) -> C.CDLL:
         lib.ref_real_bytes.restype = C.c_int
         _refs[bits] = lib
     return _refs[bits]
+
+
+def host_isa() -> str | None:
+    """The widest vector ISA of this host the batched engine is built for, as the
+    reference's -march=native static dispatch would pick it: "avx512"
+    (x86-64-v4: AVX-512 F/BW/CD/DQ/VL), "avx2" (x86-64-v3: AVX2 + FMA) or None."""
+    try:
+        flags = set()
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("flags"):
+                flags = set(line.split(":", 1)[1].split())
+                break
+    except OSError:
+        return None
+    if {"avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"} <= flags:
+        return "avx512"
+    if {"avx2", "fma", "bmi2"} <= flags:
+        return "avx2"
+    return None
+
+
+def batched_available(isa: str | None = None) -> bool:
+    isa = isa or host_isa()
+    return isa is not None and REF_BATCHED_SO[isa].exists()
+
+
+_batched: dict = {}
+
+
+def ref_batched(isa: str | None = None) -> C.CDLL:
+    """The reference's BatchedRK45<T> library for `isa` (default: this host's)."""
+    isa = isa or host_isa()
+    if isa is None:
+        raise RuntimeError("no AVX2/AVX-512 support on this host for the batched engine")
+    if isa not in _batched:
+        path = REF_BATCHED_SO[isa]
+        if not path.exists():
+            raise RuntimeError(f"reference batched engine not built: {path}")
+        lib = C.CDLL(str(path))
+        vp = C.c_void_p
+        lib.refb_lanes.argtypes = [C.c_int]
+        lib.refb_lanes.restype = C.c_int
+        lib.refb_run.argtypes = [C.c_int, C.c_int, vp, vp, C.c_double, C.c_uint64, vp, C.c_double, C.c_double,
+                                 C.c_double, C.c_double, C.c_uint64, C.c_int, vp, vp, vp, vp, C.c_int]
+        lib.refb_run.restype = C.c_uint64
+        _batched[isa] = lib
+    return _batched[isa]
+
+
+def batched_run(pos, mass, charge, *, bits=32, k=1.0, rtol=1e-8, atol=1e-16, pe_stop=1e-9, max_dt=1e12,
+                max_steps=1_000_000, redistribute=True, threads=1, isa=None, outputs=True):
+    """The reference's SIMD lockstep engine BatchedRK45<float> (bits 32) or
+    <double> (bits 64) over pos [S, N, 3], K sims per batch as
+    examples/generate_dataset.cpp:184-227 drives it. Returns a dict with
+    momenta [S, N, 3] (float64, post-redistribution), steps, converged, status and
+    batch_steps (lockstep iterations summed over batches)."""
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    mass = np.ascontiguousarray(mass, dtype=np.float64)
+    charge = np.ascontiguousarray(charge, dtype=np.float64)
+    S, n, _ = pos.shape
+    lib = ref_batched(isa)
+    out = dict(momenta=np.zeros((S, n, 3)), steps=np.zeros(S, np.uint32), converged=np.zeros(S, np.uint8),
+               status=np.zeros(S, np.uint8)) if outputs else {}
+    bs = lib.refb_run(int(bits), n, _p(mass), _p(charge), k, S, _p(pos), rtol, atol, pe_stop, max_dt,
+                      int(max_steps), 1 if redistribute else 0, _p(out.get("momenta")), _p(out.get("steps")),
+                      _p(out.get("converged")), _p(out.get("status")), int(threads))
+    out["batch_steps"] = int(bs)
+    out["lanes"] = int(lib.refb_lanes(int(bits)))
+    return out
 
 
 def cfg(rtol=1e-8, atol=1e-16, pe_stop=1e-9, max_dt=1e12, max_steps=1_000_000, redistribute=True, mode=0,
