@@ -134,6 +134,8 @@ _SIGNATURES = {
     ),
     "ce_last_launch_count": ([C.c_void_p], C.c_int),
     "ce_probe_fp32_peak": ([C.c_int, C.POINTER(C.c_double)], C.c_int),
+    "ce_probe_fp32_peak_ex": ([C.c_int, C.c_int, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double)],
+                              C.c_int),
     "ce_probe_bounded_wait": ([C.c_int, C.c_uint, C.POINTER(C.c_int)], C.c_int),
     "ce_reserve_mixed": ([C.c_void_p, C.c_uint64], C.c_int),
     "ce_run_mixed_device": (

@@ -14,9 +14,17 @@
 extern "C" {
 #endif
 
-/* FP32 FMA throughput of `device` in TFLOP/s (an FMA counts 2). Returns 0 or a
- * negative CE_ERR_* code. */
+/* FP32 FMA throughput of `device` in TFLOP/s (an FMA counts 2), from a short
+ * (~0.2 ms) scalar-FFMA kernel. Returns 0 or a negative CE_ERR_* code. */
 int ce_probe_fp32_peak(int device, double* tflops_out);
+
+/* The same throughput from a kernel sized to last at least `min_ms` (0 .. 1000)
+ * milliseconds per launch, so the SM clock settles under load: scalar FFMA
+ * (packed 0) or packed FFMA2 (packed 1, two FP32 FMAs per instruction with
+ * per-element IEEE rounding, the form the explosion kernel's x/y components
+ * use). Best of 5 timed launches after sizing. *ms_out (may be NULL) receives
+ * the best launch's duration. Returns 0 or a negative CE_ERR_* code. */
+int ce_probe_fp32_peak_ex(int device, int packed, double min_ms, double* tflops_out, double* ms_out);
 
 /* Failure-detection check of the bounded waits the tensor-core kernels use
  * (no counterpart in the reference): one kernel waits on an mbarrier that

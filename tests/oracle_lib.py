@@ -267,3 +267,130 @@ def config_norm_error(p, p_ref):
     p = np.asarray(p, dtype=np.float64).reshape(len(p), -1)
     q = np.asarray(p_ref, dtype=np.float64).reshape(len(p_ref), -1)
     return np.linalg.norm(p - q, axis=1) / np.linalg.norm(q, axis=1)
+
+
+# ---------------------------------------------------------------------------
+# Timed CPU baseline: one pinned process per core (test / bench infrastructure)
+# ---------------------------------------------------------------------------
+
+def usable_cores() -> list[int]:
+    """The logical CPUs this process may run on, in order."""
+    import os
+
+    return sorted(os.sched_getaffinity(0))
+
+
+def _core_worker(core, pos, mass, charge, params, cmd_q, res_q):
+    """Pinned to `core`; runs its slice once per "run" command."""
+    import os
+    import time
+
+    try:
+        os.sched_setaffinity(0, {core})
+        engine = params.pop("engine")
+        if engine == "batched":
+            ref_batched(params.get("isa"))
+        else:
+            ref(params["bits"])
+        res_q.put(("ready", core, 0.0, 0))
+        while True:
+            cmd = cmd_q.get()
+            if cmd is None:
+                break
+            t0 = time.perf_counter()
+            if engine == "batched":
+                r = batched_run(pos, mass, charge, threads=1, **params)
+                work = r["batch_steps"]
+            else:
+                p = {k: v for k, v in params.items() if k != "isa"}
+                r = ref_run_batch(pos, mass, charge, threads=1, **p)
+                work = int(r["steps"].sum())
+            res_q.put(("done", core, time.perf_counter() - t0, work))
+    except Exception as e:  # report instead of dying silently
+        res_q.put(("error", core, repr(e), 0))
+
+
+class CorePool:
+    """One `spawn` process per core, each pinned to its core (sched_setaffinity,
+    the `taskset` of the reference's single-core measurements) and owning a
+    disjoint contiguous slice of the sims. step() runs every slice once and
+    returns the wall time of the whole step (coordinator clock: command out to
+    last result in). engine "batched": the reference's BatchedRK45<T> driven
+    like examples/generate_dataset.cpp:184-227; "scalar": the reference's
+    run_to_convergence per sim. Geometries are generated before the pool starts
+    and never timed (bench/bench_batched_integrator.cpp:140-174)."""
+
+    def __init__(self, pos, mass, charge, cores, *, engine="batched", bits=32, rtol=1e-8, atol=1e-16,
+                 pe_stop=1e-9, isa=None, timeout=600.0):
+        import multiprocessing as mp
+
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        self.S = pos.shape[0]
+        self.cores = list(cores)
+        self.timeout = timeout
+        ctx = mp.get_context("spawn")
+        self.res_q = ctx.Queue()
+        self.cmd_qs = []
+        self.procs = []
+        # slices in whole K = 16 lane batches, so the lockstep batches are the
+        # ones a single process would run
+        bounds = (np.linspace(0, self.S // 16, len(self.cores) + 1).astype(int) * 16)
+        bounds[-1] = self.S
+        params = dict(engine=engine, bits=bits, rtol=rtol, atol=atol, pe_stop=pe_stop, isa=isa)
+        for c, a, b in zip(self.cores, bounds[:-1], bounds[1:]):
+            q = ctx.Queue()
+            p = ctx.Process(target=_core_worker, args=(c, pos[a:b], mass, charge, dict(params), q, self.res_q),
+                            daemon=True)
+            p.start()
+            self.cmd_qs.append(q)
+            self.procs.append(p)
+        self._collect("ready")
+
+    def _collect(self, kind):
+        out = []
+        for _ in self.procs:
+            msg = self.res_q.get(timeout=self.timeout)
+            if msg[0] == "error":
+                self.close()
+                raise RuntimeError(f"CPU baseline worker on core {msg[1]} failed: {msg[2]}")
+            assert msg[0] == kind, msg
+            out.append(msg)
+        return out
+
+    def step(self) -> tuple[float, float, int]:
+        """(wall seconds of one pass over all S sims, slowest worker's own
+        seconds, work units: lockstep iterations or scalar steps)."""
+        import time
+
+        t0 = time.perf_counter()
+        for q in self.cmd_qs:
+            q.put("run")
+        res = self._collect("done")
+        wall = time.perf_counter() - t0
+        return wall, max(r[2] for r in res), sum(r[3] for r in res)
+
+    def close(self):
+        for q in self.cmd_qs:
+            try:
+                q.put(None)
+            except Exception:
+                pass
+        for p in self.procs:
+            p.join(timeout=10)
+            if p.is_alive():
+                p.kill()
+        self.procs = []
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def single_core_rate(pos, mass, charge, *, core=None, reps=7, **kw):
+    """Explosions/s of one pinned core: median of `reps` passes over pos."""
+    core = usable_cores()[-1] if core is None else core
+    with CorePool(pos, mass, charge, [core], **kw) as pool:
+        secs = [pool.step()[0] for _ in range(reps)]
+    return len(pos) / float(np.median(secs)), secs
