@@ -1,10 +1,11 @@
-"""Build recipe for libce_gpu.so (sm_100a) and the C++ host mirror.
+"""Build recipe for libce_gpu.so (sm_100a) and the C++ drop-in (coulomb::gpu).
 
 Compiles every CUDA translation unit with
 ``nvcc -gencode arch=compute_100a,code=sm_100a -lineinfo -O3`` in parallel
 into ``_build/`` and links the shared library in-tree (next to this file), so
-it travels with the repository snapshot. Incremental: a unit is rebuilt only
-when a source or header is newer than its object.
+it travels with the repository snapshot. Incremental by default (a unit is
+rebuilt only when a source or header is newer than its object); `force=True`,
+which __graft_entry__.build() passes, recompiles everything.
 """
 from __future__ import annotations
 
@@ -53,13 +54,13 @@ def _stale(obj: Path, src: Path) -> bool:
     return any(p.stat().st_mtime > t for p in [src, *_headers(), Path(__file__)])
 
 
-def build_cuda(verbose: bool = False, ptxas_info: bool = False) -> Path:
+def build_cuda(verbose: bool = False, ptxas_info: bool = False, force: bool = False) -> Path:
     nvcc = _nvcc()
     BUILD.mkdir(exist_ok=True)
     jobs = []
     for obj, src, extra in UNITS:
         o, s = BUILD / obj, CSRC / src
-        if _stale(o, s) or ptxas_info:
+        if force or _stale(o, s) or ptxas_info:
             cmd = [nvcc, *NVFLAGS, *extra, "-c", str(s), "-o", str(o)]
             if ptxas_info:
                 cmd += ["-Xptxas", "-v"]
@@ -82,7 +83,7 @@ def build_cuda(verbose: bool = False, ptxas_info: bool = False) -> Path:
         raise RuntimeError(f"nvcc failed:\n{msg}")
     objs = [str(BUILD / o) for o, _, _ in UNITS]
     newest = max(Path(o).stat().st_mtime for o in objs)
-    if not LIB.exists() or LIB.stat().st_mtime < newest:
+    if force or not LIB.exists() or LIB.stat().st_mtime < newest:
         cmd = [nvcc, *ARCH, "-shared", "-o", str(LIB), *objs, "-lcudart"]
         p = subprocess.run(cmd, capture_output=True, text=True)
         if p.returncode != 0:
@@ -109,32 +110,71 @@ def _run(cmd: list[str]) -> None:
         raise RuntimeError(f"build step failed: {' '.join(cmd)}\n{p.stderr}")
 
 
-def build_host() -> None:
-    """libce_host.so (the coulomb:: host API over the C ABI), the dataset
-    generator example and the C++ test driver, linked against libce_gpu.so."""
+def reference_dir(explicit: str | os.PathLike | None = None) -> Path | None:
+    """The reference checkout (its include/coulomb/ and src/) the host library is
+    built beside: `explicit`, else $COULOMB_REFERENCE_DIR; None if neither names
+    a checkout."""
+    cand = explicit or os.environ.get("COULOMB_REFERENCE_DIR")
+    if cand and (Path(cand) / "include" / "coulomb" / "driver.hpp").exists():
+        return Path(cand)
+    return None
+
+
+ENGINE_LIB = BIN / "libcoulomb_engine.so"
+
+
+def build_host(reference: str | os.PathLike | None = None, force: bool = False) -> bool:
+    """The C++ drop-in, built beside the reference's coulomb::engine:
+
+    * bin/libcoulomb_engine.so -- the reference's own engine library
+      (src/system.cpp, integrators.cpp, driver.cpp, sampler.cpp, compiled where
+      they lie with its Release flags, src/CMakeLists.txt:3-17), the host
+      project the drop-in plugs into;
+    * libce_host.so -- coulomb::gpu (BatchedRK45, run_to_convergence_batch,
+      PhiloxBallSampler, DatasetWriter) compiled against the reference's
+      include/coulomb headers and libce_gpu.so;
+    * bin/ce_generate_dataset and bin/ce_test_host, linked against both.
+
+    Needs a reference checkout (`reference_dir`); returns False and builds
+    nothing without one."""
+    ref = reference_dir(reference)
+    if ref is None:
+        print("build_host: no reference checkout (COULOMB_REFERENCE_DIR); C++ drop-in not built", file=sys.stderr)
+        return False
     cxx = _cxx()
-    inc = ["-I", str(HOST / "include"), "-I", str(INCLUDE)]
+    ref_inc = ref / "include"
+    inc = ["-I", str(HOST / "include"), "-I", str(ref_inc), "-I", str(INCLUDE)]
     flags = ["-std=c++20", "-O2", "-ffp-contract=off", "-Wall", "-Wextra"]
+    BIN.mkdir(exist_ok=True)
+    eng_srcs = [ref / "src" / f for f in ("system.cpp", "integrators.cpp", "driver.cpp", "sampler.cpp")]
+    ref_hdrs = list((ref_inc / "coulomb").glob("*.hpp"))
+    newest_eng = max(p.stat().st_mtime for p in [*eng_srcs, *ref_hdrs])
+    if force or not ENGINE_LIB.exists() or ENGINE_LIB.stat().st_mtime < newest_eng:
+        _run([cxx, "-std=c++20", "-O3", "-DNDEBUG", "-fPIC", "-shared", "-I", str(ref_inc), *map(str, eng_srcs),
+              "-o", str(ENGINE_LIB)])
     srcs = sorted((HOST / "src").glob("*.cpp"))
-    hdrs = list((HOST / "include").rglob("*.hpp")) + list(INCLUDE.glob("*.h"))
+    hdrs = list((HOST / "include").rglob("*.hpp")) + list(INCLUDE.glob("*.h")) + ref_hdrs
     newest_in = max(p.stat().st_mtime for p in [*srcs, *hdrs, LIB])
-    if not HOST_LIB.exists() or HOST_LIB.stat().st_mtime < newest_in:
+    if force or not HOST_LIB.exists() or HOST_LIB.stat().st_mtime < newest_in:
         _run([cxx, *flags, "-fPIC", "-shared", *inc, *map(str, srcs), "-L", str(PKG), "-lce_gpu",
               "-Wl,-rpath,$ORIGIN", "-o", str(HOST_LIB)])
-    BIN.mkdir(exist_ok=True)
     progs = {"ce_generate_dataset": HOST / "examples" / "generate_dataset.cpp",
              "ce_test_host": ROOT / "tests" / "cpp" / "test_host.cpp"}
     for name, src in progs.items():
         out = BIN / name
-        if out.exists() and out.stat().st_mtime >= max(src.stat().st_mtime, HOST_LIB.stat().st_mtime):
+        if not force and out.exists() and out.stat().st_mtime >= max(
+                src.stat().st_mtime, HOST_LIB.stat().st_mtime, ENGINE_LIB.stat().st_mtime):
             continue
         _run([cxx, *flags, *inc, "-I", "/usr/local/cuda/include", str(src), "-L", str(PKG), "-lce_host", "-lce_gpu",
-              "-L", str(CUDA_LIB), "-lcudart", "-Wl,-rpath,$ORIGIN/..", "-Wl,-rpath," + str(CUDA_LIB), "-o", str(out)])
+              "-L", str(BIN), "-lcoulomb_engine", "-L", str(CUDA_LIB), "-lcudart", "-Wl,-rpath,$ORIGIN",
+              "-Wl,-rpath,$ORIGIN/..", "-Wl,-rpath," + str(CUDA_LIB), "-o", str(out)])
+    return True
 
 
-def build_all(verbose: bool = False) -> None:
-    build_cuda(verbose=verbose)
-    build_host()
+def build_all(verbose: bool = False, reference: str | os.PathLike | None = None, force: bool = False) -> None:
+    """Everything; `force` recompiles every unit whatever the timestamps say."""
+    build_cuda(verbose=verbose, force=force)
+    build_host(reference, force=force)
 
 
 if __name__ == "__main__":

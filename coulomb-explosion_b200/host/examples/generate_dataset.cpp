@@ -1,10 +1,11 @@
 // generate_dataset.cpp -- Coulomb-explosion dataset generator on the B200 engine.
 //
-// Drop-in for the reference's examples/generate_dataset.cpp: same flags and
+// Drop-in for the reference's examples/generate_dataset.cpp, built beside the
+// reference's coulomb::engine (its Molecule and UniformSphereSampler): same flags and
 // defaults (--out --sims --seed --radius --min-separation --rtol --atol
 // --pe-stop --progress-every; CH4 singly ionised, 1e7 sims, seed 49188291,
 // r 4.0, min_sep 0.25, rtol 1e-4, atol 1e-7, pe_stop 1e-5), same record format
-// and sidecar (coulomb/dataset.hpp), readable by the reference's to_parquet.py,
+// and sidecar (coulomb/gpu/dataset.hpp), readable by the reference's to_parquet.py,
 // verify_subset.py and sanity_check.py. Added flags:
 //   --sampler uniform-sphere|philox   the reference's sequential mt19937_64
 //        sampler on the host (bit-identical geometries to the reference run with
@@ -27,14 +28,25 @@
 
 #include "ce_gpu.h"
 #include "ce_sampler.h"
-#include "coulomb/dataset.hpp"
+#include "coulomb/gpu/dataset.hpp"
 #include "coulomb/molecule.hpp"
 #include "coulomb/sampler.hpp"
+#include "coulomb/system.hpp"
 
 using namespace coulomb;
+using gpu::DatasetWriter;
 using Clock = std::chrono::steady_clock;
 
 namespace {
+
+// Methane, singly ionised on every atom: C then 4 H (the reference generator's
+// molecule, examples/generate_dataset.cpp:56-66).
+Molecule make_methane() {
+  Molecule m;
+  m.atoms.push_back(atom_from_amu("C", static_cast<Real>(12.011), Real{1}));
+  for (int i = 0; i < 4; ++i) m.atoms.push_back(atom_from_amu("H", static_cast<Real>(1.008), Real{1}));
+  return m;
+}
 
 struct Args {
   std::size_t sims = 10'000'000;
@@ -118,8 +130,8 @@ int main(int argc, char** argv) {
     if (ce_create(&e, args.device) != CE_OK) throw std::runtime_error("no usable B200");
     std::vector<double> m(n), q(n);
     for (std::size_t i = 0; i < n; ++i) {
-      m[i] = mol.atoms[i].mass;
-      q[i] = mol.atoms[i].charge;
+      m[i] = static_cast<double>(mol.atoms[i].mass);
+      q[i] = static_cast<double>(mol.atoms[i].charge);
     }
     if (ce_set_molecule(e, static_cast<int>(n), m.data(), q.data(), 1.0) != CE_OK)
       throw std::runtime_error(ce_last_error(e));
@@ -149,7 +161,8 @@ int main(int argc, char** argv) {
     cudaEvent_t integrated;
     check(cudaEventCreateWithFlags(&integrated, cudaEventDisableTiming), "event");
 
-    UniformSphereSampler host_sampler({args.radius, args.min_separation, 10000}, args.seed);
+    UniformSphereSampler host_sampler({static_cast<Real>(args.radius), static_cast<Real>(args.min_separation), 10000},
+                                      args.seed);
     const ce_ball_sampler dev_sampler{args.seed, args.radius, args.min_separation, 0};
     DatasetWriter writer(args.out, mol);
     std::size_t n_failed = 0, done = 0, steps_sum = 0;

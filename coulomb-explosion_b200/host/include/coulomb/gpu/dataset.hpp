@@ -1,4 +1,4 @@
-// dataset.hpp -- the reference's dataset output format.
+// dataset.hpp -- the reference's dataset output format (coulomb::gpu::DatasetWriter).
 //
 // Fixed-width little-endian records, written field by field with no padding
 // (examples/generate_dataset.cpp:10-19, 198-217), readable unchanged by the
@@ -22,7 +22,7 @@
 
 #include "coulomb/molecule.hpp"
 
-namespace coulomb {
+namespace coulomb::gpu {
 
 inline constexpr std::size_t record_bytes(std::size_t n_atoms) { return n_atoms * 3 * 4 * 2 + 4 + 1; }
 
@@ -47,4 +47,4 @@ class DatasetWriter {
   std::size_t written_ = 0;
 };
 
-}  // namespace coulomb
+}  // namespace coulomb::gpu

@@ -1,5 +1,6 @@
 // gpu.cpp -- coulomb::gpu::Engine, BatchedRK45 and run_to_convergence_batch:
-// the host C++ API over the C ABI of libce_gpu.so.
+// the reference's batched and scalar drivers over the C ABI of libce_gpu.so,
+// taking and returning the reference's own coulomb:: types.
 #include <algorithm>
 #include <cmath>
 #include <stdexcept>
@@ -27,22 +28,22 @@ void Engine::throw_last(int rc, const char* what) const {
 void Engine::set_molecule(const Molecule& mol, Real coulomb_k) {
   std::vector<double> m(mol.size()), q(mol.size());
   for (std::size_t i = 0; i < mol.size(); ++i) {
-    m[i] = mol.atoms[i].mass;
-    q[i] = mol.atoms[i].charge;
+    m[i] = static_cast<double>(mol.atoms[i].mass);
+    q[i] = static_cast<double>(mol.atoms[i].charge);
   }
-  const int rc = ce_set_molecule(e_, static_cast<int>(mol.size()), m.data(), q.data(), coulomb_k);
+  const int rc = ce_set_molecule(e_, static_cast<int>(mol.size()), m.data(), q.data(), static_cast<double>(coulomb_k));
   if (rc != CE_OK) throw_last(rc, "ce_set_molecule");
 }
 
 namespace {
 
-ce_run_config to_c(const RunConfig& cfg, Real rtol, Real atol, int mode) {
+ce_run_config to_c(const RunConfig& cfg, double rtol, double atol, int mode) {
   ce_run_config c;
   ce_default_config(&c);
   c.rtol = rtol;
   c.atol = atol;
-  c.pe_stop_fraction = cfg.pe_stop_fraction;
-  c.max_dt = cfg.max_dt;
+  c.pe_stop_fraction = static_cast<double>(cfg.pe_stop_fraction);
+  c.max_dt = static_cast<double>(cfg.max_dt);
   c.max_steps = cfg.max_steps;
   c.redistribute_energy = cfg.redistribute_energy ? 1 : 0;
   c.precision_mode = mode;
@@ -98,7 +99,7 @@ BatchedRK45::Result BatchedRK45::run(const RunConfig& cfg) {
 
 std::vector<RunResult> run_to_convergence_batch(const Molecule& mol, std::vector<State>& states, const RunConfig& cfg,
                                                 const IntegratorOptions& opts, Real coulomb_k, int device,
-                                                int precision_mode) {
+                                                int precision_mode, BatchStatus* extra) {
   const std::size_t S = states.size(), n = mol.size();
   std::vector<RunResult> res(S);
   if (S == 0) return res;
@@ -116,31 +117,38 @@ std::vector<RunResult> run_to_convergence_batch(const Molecule& mol, std::vector
       pos[(s * n + i) * 3 + 2] = static_cast<float>(states[s].positions[i].z);
     }
   }
-  std::vector<double> ker(S), t_final(S), pe_final(S), ke_before(S);
+  std::vector<double> ker(S), t_final(S), pe_final(S), ke_before(S), e0(S);
   std::vector<std::uint32_t> steps(S), rejects(S);
   std::vector<std::uint8_t> status(S);
   ce_outputs out{mom.data(), ker.data(), steps.data(), status.data(), rejects.data(), t_final.data(),
-                 pe_final.data(), ke_before.data(), nullptr, nullptr};
-  const ce_run_config c = to_c(cfg, opts.rtol, opts.atol, precision_mode);
+                 pe_final.data(), ke_before.data(), nullptr, e0.data()};
+  const ce_run_config c = to_c(cfg, static_cast<double>(opts.rtol), static_cast<double>(opts.atol), precision_mode);
   const int rc = ce_run(eng.handle(), S, pos.data(), &c, &out);
   if (rc != CE_OK) eng.throw_last(rc, "ce_run");
+  if (extra) {
+    extra->status.resize(S);
+    extra->rejects = rejects;
+  }
   for (std::size_t s = 0; s < S; ++s) {
+    // energy_initial is E0 = PE0 of the geometry the device integrated (narrowed
+    // to float like BatchedRK45<float>::set_lane_geometry), the energy the
+    // redistribution restores.
     RunResult& r = res[s];
     r.steps = steps[s];
-    r.t_final = t_final[s];
-    r.energy_initial = potential_energy(mol, states[s].positions, coulomb_k);
-    r.pe_final = pe_final[s];
-    r.ke_before_redist = ke_before[s];
-    r.ke_after_redist = ker[s];
-    r.redistribution_scale =
-        (cfg.redistribute_energy && ke_before[s] > 0) ? std::sqrt(r.energy_initial / ke_before[s]) : 1.0;
-    r.status = static_cast<SimStatus>(status[s]);
+    r.t_final = static_cast<Real>(t_final[s]);
+    r.energy_initial = static_cast<Real>(e0[s]);
+    r.pe_final = static_cast<Real>(pe_final[s]);
+    r.ke_before_redist = static_cast<Real>(ke_before[s]);
+    r.ke_after_redist = static_cast<Real>(ker[s]);
+    r.redistribution_scale = static_cast<Real>(
+        (cfg.redistribute_energy && ke_before[s] > 0) ? std::sqrt(e0[s] / ke_before[s]) : 1.0);
     r.converged = status[s] == CE_SIM_OK;
-    r.rejects = rejects[s];
+    if (extra) extra->status[s] = static_cast<SimStatus>(status[s]);
     for (std::size_t i = 0; i < n; ++i) {
-      const double m = mol.atoms[i].mass;
-      states[s].velocities[i] = Vec3{mom[(s * n + i) * 3] / m, mom[(s * n + i) * 3 + 1] / m,
-                                     mom[(s * n + i) * 3 + 2] / m};
+      const double m = static_cast<double>(mol.atoms[i].mass);
+      states[s].velocities[i] = Vec3{static_cast<Real>(mom[(s * n + i) * 3] / m),
+                                     static_cast<Real>(mom[(s * n + i) * 3 + 1] / m),
+                                     static_cast<Real>(mom[(s * n + i) * 3 + 2] / m)};
     }
   }
   return res;

@@ -1,5 +1,7 @@
-// host.cpp -- molecule helpers, the two samplers and the dataset writer of the
-// host API (coulomb-explosion_b200/host/include/coulomb/*.hpp).
+// host.cpp -- the counter-based sampler and the dataset writer of the GPU host
+// library (coulomb::gpu, include/coulomb/gpu/{philox_sampler,dataset}.hpp).
+// Molecules, states and the reference's UniformSphereSampler come from the
+// reference's coulomb::engine.
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -7,75 +9,11 @@
 #include <stdexcept>
 
 #include "ce_sampler.h"
-#include "coulomb/dataset.hpp"
-#include "coulomb/molecule.hpp"
-#include "coulomb/sampler.hpp"
+#include "coulomb/gpu/dataset.hpp"
+#include "coulomb/gpu/philox_sampler.hpp"
+#include "coulomb/units.hpp"
 
-namespace coulomb {
-
-Real potential_energy(const Molecule& mol, const std::vector<Vec3>& pos, Real coulomb_k) {
-  Real u = 0;
-  for (std::size_t i = 0; i < mol.size(); ++i)
-    for (std::size_t j = i + 1; j < mol.size(); ++j)
-      u += coulomb_k * mol.atoms[i].charge * mol.atoms[j].charge / norm(pos[i] - pos[j]);
-  return u;
-}
-
-Real kinetic_energy(const Molecule& mol, const std::vector<Vec3>& vel) {
-  Real t = 0;
-  for (std::size_t i = 0; i < mol.size(); ++i) t += 0.5 * mol.atoms[i].mass * dot(vel[i], vel[i]);
-  return t;
-}
-
-Molecule make_methane() {
-  Molecule m;
-  m.atoms = {atom_from_amu("C", 12.011, 1.0), atom_from_amu("H", 1.008, 1.0), atom_from_amu("H", 1.008, 1.0),
-             atom_from_amu("H", 1.008, 1.0), atom_from_amu("H", 1.008, 1.0)};
-  return m;
-}
-
-// ---- UniformSphereSampler (the reference's distribution and RNG stream) ----
-
-UniformSphereSampler::UniformSphereSampler(Options options, std::uint64_t seed) : opts_(options), rng_(seed) {
-  if (!(opts_.radius > 0)) throw std::invalid_argument("UniformSphereSampler: radius must be positive");
-  if (opts_.min_separation < 0)
-    throw std::invalid_argument("UniformSphereSampler: min_separation must be non-negative");
-}
-
-Vec3 UniformSphereSampler::point_in_ball() {
-  std::uniform_real_distribution<Real> u(-opts_.radius, opts_.radius);
-  const Real r2 = opts_.radius * opts_.radius;
-  for (;;) {
-    const Real x = u(rng_);
-    const Real y = u(rng_);
-    const Real z = u(rng_);
-    const Vec3 p{x, y, z};
-    if (dot(p, p) <= r2) return p;
-  }
-}
-
-void UniformSphereSampler::sample(const Molecule& molecule, State& state) {
-  const std::size_t n = molecule.size();
-  state.positions.resize(n);
-  state.velocities.assign(n, Vec3{});
-  const Real min2 = opts_.min_separation * opts_.min_separation;
-  for (std::size_t i = 0; i < n; ++i) {
-    for (std::size_t tries = 0;;) {
-      const Vec3 c = point_in_ball();
-      bool clear = true;
-      for (std::size_t j = 0; j < i && clear; ++j) {
-        const Vec3 d = c - state.positions[j];
-        clear = dot(d, d) >= min2;
-      }
-      if (clear) {
-        state.positions[i] = c;
-        break;
-      }
-      if (++tries >= opts_.max_attempts_per_atom)
-        throw std::runtime_error("UniformSphereSampler: cannot place an atom at the requested separation");
-    }
-  }
-}
+namespace coulomb::gpu {
 
 // ---- PhiloxBallSampler (counter-based; same draws as the device sampler) ----
 
@@ -98,7 +36,9 @@ void PhiloxBallSampler::sample(const Molecule& molecule, State& state) {
   ++next_;
   state.positions.resize(n);
   state.velocities.assign(n, Vec3{});
-  for (int i = 0; i < n; ++i) state.positions[i] = Vec3{pos64[i * 3], pos64[i * 3 + 1], pos64[i * 3 + 2]};
+  for (int i = 0; i < n; ++i)
+    state.positions[i] = Vec3{static_cast<Real>(pos64[i * 3]), static_cast<Real>(pos64[i * 3 + 1]),
+                              static_cast<Real>(pos64[i * 3 + 2])};
 }
 
 // ---- DatasetWriter ----
@@ -154,4 +94,4 @@ void DatasetWriter::write_metadata(const std::map<std::string, double>& numbers,
        "\"converged: uint8\"]\n}\n";
 }
 
-}  // namespace coulomb
+}  // namespace coulomb::gpu
