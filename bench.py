@@ -1022,6 +1022,7 @@ def main():
                          "1 Kahan x/v, 2 FP64 t/E, 3 both (see --workload precision)")
     ap.add_argument("--lanes", type=int, default=0, help="lanes per sim: 0 auto, 1 thread-per-sim, N lane-per-atom")
     ap.add_argument("--block", type=int, default=0, help="threads per block (0: engine default)")
+    ap.add_argument("--refill", type=int, default=0, help="refill threshold in idle sims per warp (0: engine default)")
     ap.add_argument("--molecule", default="ch4", choices=["ch4", "c2h6", "h2o"],
                     help="ch4 (the headline workload), c2h6 (10-atom C2H6-like), h2o (stiff H2O)")
     ap.add_argument("--cpu-budget", type=float, default=8.0)
@@ -1095,8 +1096,8 @@ def main():
     assert not flags.any()
     eng = ce.Engine(dev.index)
     eng.set_molecule(mol.masses_me, mol.charge_array)
-    if args.lanes or args.block:
-        eng.set_tuning(block_threads=args.block, lanes_per_sim=args.lanes)
+    if args.lanes or args.block or args.refill:
+        eng.set_tuning(block_threads=args.block, lanes_per_sim=args.lanes, refill_threshold=args.refill)
 
     stream = torch.cuda.Stream(device=dev)
     pos_d = torch.from_numpy(pos_host).to(dev)

@@ -182,12 +182,19 @@ int launch_fixed(ce_engine* e, uint64_t S, const float* pos, const ce_run_config
   const ce::FixedKernelFn fn = atom ? ce::select_atom_kernel(e->n, cfg->precision_mode)
                                     : ce::select_fixed_kernel(e->n, cfg->precision_mode);
   if (!fn) return ce::fail(e, CE_ERR_INVALID, "ce_run: no kernel for this atom count");
-  const int block = atom ? std::min(t.block_threads, ce::kAtomMaxBlock) : t.block_threads;
+  const int block = std::min(t.block_threads, atom ? ce::kAtomMaxBlock : ce::kThreadMaxBlock);
   const uint64_t sims_per_block =
       atom ? static_cast<uint64_t>(block / 32) * static_cast<uint64_t>(32 / e->n) : static_cast<uint64_t>(block);
+  // The thread-per-sim kernel keeps its stage accelerations in dynamic shared memory.
+  const size_t smem = atom ? 0 : ce::thread_smem_bytes(e->n, block);
+  if (smem > 0) {
+    st = cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              static_cast<int>(smem));
+    if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaFuncSetAttribute(max dynamic shared memory)");
+  }
   int per_sm = t.blocks_per_sm;
   if (per_sm == 0) {
-    st = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, 0);
+    st = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem);
     if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     if (per_sm < 1) per_sm = 1;
   }
@@ -202,7 +209,7 @@ int launch_fixed(ce_engine* e, uint64_t S, const float* pos, const ce_run_config
 
   st = cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), s);
   if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMemsetAsync(cursor)");
-  fn<<<static_cast<unsigned>(grid), block, 0, s>>>(P, e->mol);
+  fn<<<static_cast<unsigned>(grid), block, smem, s>>>(P, e->mol);
   st = cudaGetLastError();
   if (st != cudaSuccess) return ce::cuda_fail(e, st, "rk45 kernel launch");
   e->last_launches = 1;

@@ -20,6 +20,9 @@
 // only a stand-in, not a device address. The first call on each device, with
 // that device current, looks the address up once with cudaGetSymbolAddress and
 // caches it; that first call should therefore come before any stream capture.
+// The cached address is valid for the life of the device's primary context: a
+// cudaDeviceReset between calls is not supported (the module reloads and the
+// array can move).
 // Every call shares the one cursor and leaves its last value behind, so each
 // call clears it (cudaMemsetAsync on the caller's stream) before the launch;
 // calls whose launches overlap on the GPU (different streams, no ordering)
@@ -132,8 +135,11 @@ extern "C" int ce_run_device_noalloc(int n, const double* mass_me, const double*
 
   const ce::FixedKernelFn fn = kernel_for(n, cfg->precision_mode);
   const int block = 128;
+  // The one-atom (thread-per-sim) kernel takes its stage slots as dynamic shared
+  // memory (on-chip, per block; not an allocation).
+  const size_t smem = n >= 2 ? 0 : ce::thread_smem_bytes(n, block);
   int per_sm = 0, sms = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, 0) != cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem) != cudaSuccess ||
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     return report(err, err_len, CE_ERR_CUDA, "ce_run_device_noalloc: device query failed");
   if (per_sm < 1) per_sm = 1;
@@ -169,7 +175,7 @@ extern "C" int ce_run_device_noalloc(int n, const double* mass_me, const double*
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   st = cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), s);  // the cursor must start at 0
   if (st != cudaSuccess) return report(err, err_len, CE_ERR_CUDA, "ce_run_device_noalloc: clearing the cursor failed");
-  fn<<<static_cast<unsigned>(grid), block, 0, s>>>(P, m);
+  fn<<<static_cast<unsigned>(grid), block, smem, s>>>(P, m);
   st = cudaGetLastError();
   if (st != cudaSuccess) {
     char msg[256];

@@ -103,7 +103,6 @@ struct V3 {
   float z;
   __device__ __forceinline__ float get(int c) const { return c == 0 ? xy.x : (c == 1 ? xy.y : z); }
 };
-__device__ __forceinline__ float2 bcast(float s) { return make_float2(s, s); }
 __device__ __forceinline__ V3 v3_zero() { return {make_float2(0.0f, 0.0f), 0.0f}; }
 // s * a + c
 __device__ __forceinline__ V3 v3_fma(float s, const V3& a, const V3& c) {
@@ -113,20 +112,6 @@ __device__ __forceinline__ V3 v3_mul(float s, const V3& a) { return {__fmul2_rn(
 __device__ __forceinline__ V3 v3_add(const V3& a, const V3& b) { return {__fadd2_rn(a.xy, b.xy), a.z + b.z}; }
 __device__ __forceinline__ V3 v3_sub(const V3& a, const V3& b) {
   return {__ffma2_rn(bcast(-1.0f), b.xy, a.xy), a.z - b.z};
-}
-
-// Approximate reciprocal and square root (PTX rcp.approx / sqrt.approx, flush
-// to zero): for the error-norm scales and the initial-step heuristic, where a
-// relative error of a few 1e-7 changes no decision the integrator relies on.
-__device__ __forceinline__ float rcp_approx(float x) {
-  float r;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-  return r;
-}
-__device__ __forceinline__ float sqrt_approx(float x) {
-  float r;
-  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-  return r;
 }
 
 template <int N, int MODE>

@@ -1,4 +1,4 @@
-// rk45_sim.cuh -- one Coulomb explosion per thread, entirely in registers.
+// rk45_sim.cuh -- one Coulomb explosion per thread (thread-per-sim layout).
 //
 // Device-side restatement of the reference's per-sim integration:
 //   pair force / potential         src/system.cpp:5-41, include/coulomb/batched_force.hpp:31-110
@@ -13,10 +13,29 @@
 // evaluation (x_7 is x_new, FSAL), and because every simulation starts at rest
 // the Hairer Euler probe has x_1 = x_0 exactly, so its force evaluation equals
 // k1 and is not recomputed.
+//
+// Compact attempt loop. The six stage evaluations run in one rolled loop with a
+// single inlined force evaluation, so the loop body (a few thousand bytes of
+// code for CH4) stays resident in the instruction cache; a fully unrolled
+// attempt (six inlined force evaluations) was bound by instruction fetch. The
+// loop's stage index is warp-uniform (every thread of a warp runs the same
+// stage), so the Butcher coefficients are constant-bank loads at a uniform
+// index. Stage accelerations k2..k7 live in shared memory, one private
+// 16-byte-chunked slot per thread and stage laid out [stage][chunk][thread], so
+// a warp's 16-byte accesses touch consecutive addresses (no bank conflicts);
+// k1 (the FSAL acceleration), x and v stay in registers.
+//
+// In-register order of a 3N-vector: the N (x, y) pairs first, then the N z
+// components, padded with zeros to whole 16-byte chunks. Every x/y update of the
+// pair force and every stage combination then runs on packed FP32x2
+// instructions (FFMA2 / FMUL2 / FADD2, per-element IEEE rounding, so results
+// equal the scalar formulation).
 #pragma once
 
 #include <cstdint>
 #include <type_traits>
+
+#include <cuda_runtime.h>
 
 #include "ce_gpu.h"
 #include "dp45_tableau.cuh"
@@ -57,18 +76,117 @@ struct RunParams {
   int32_t skip_empty;  // mixed batches: rows with n_atoms == 0 are left untouched (no outputs written)
 };
 
+
+// Packed-FP32x2 helpers (sm_100: FFMA2 / FMUL2 / FADD2; every element rounds
+// exactly like the scalar instruction) and the approximate MUFU forms.
+__device__ __forceinline__ float2 bcast(float s) { return make_float2(s, s); }
+
+// Approximate reciprocal and square root (PTX rcp.approx / sqrt.approx, flush
+// to zero): for the error-norm scales and the initial-step heuristic, where a
+// relative error of a few 1e-7 changes no decision the integrator relies on.
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float r;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// Register and shared-memory shape of one simulation in the thread-per-sim layout.
+template <int N>
+struct ThreadShape {
+  static constexpr int NF = 3 * N;         // floats of a 3N-vector
+  static constexpr int NC = (NF + 3) / 4;  // 16-byte chunks per stage slot
+  static constexpr int NP = 2 * NC;        // float2 register pairs (zero-padded)
+  static constexpr int kSlots = 6;         // k2..k6 and k7 (k1 stays in registers)
+  // Blocks of kThreadMaxBlock threads per SM the register allocator aims for:
+  // 128 registers a thread for CH4-sized molecules, more for larger N (whose
+  // shared-memory slots allow fewer blocks anyway).
+  static constexpr int kMinBlocks = N <= 5 ? 4 : (N <= 7 ? 3 : 2);
+};
+
+constexpr int kThreadMaxBlock = 128;
+
+// Dynamic shared memory of one thread-per-sim block: six stage slots of NC
+// 16-byte chunks for each of its threads.
+__host__ __device__ constexpr size_t thread_smem_bytes(int n, int block) {
+  return static_cast<size_t>(6) * static_cast<size_t>((3 * n + 3) / 4) * 16u * static_cast<size_t>(block);
+}
+
+// Flat float f of a register 3N-vector (x_i at 2i, y_i at 2i + 1, z_i at 2N + i);
+// f is a compile-time index after unrolling (values, never addresses, so the
+// arrays stay in registers).
+template <int NP>
+__device__ __forceinline__ void fl_set(float2 (&r)[NP], int f, float val) {
+  const float2 t = r[f >> 1];
+  r[f >> 1] = (f & 1) ? make_float2(t.x, val) : make_float2(val, t.y);
+}
+template <int NP>
+__device__ __forceinline__ float flc(const float2 (&r)[NP], int f) {
+  const float2 t = r[f >> 1];  // select between values, not addresses
+  return (f & 1) ? t.y : t.x;
+}
+__device__ __forceinline__ constexpr int flat_of(int n, int i, int c) { return c < 2 ? 2 * i + c : 2 * n + i; }
+
+// a_i = (1/m_i) sum_j k q_i q_j r_ij / |r_ij|^3 with Newton's third law, and
+// (if want_pe) pe += sum_{i<j} k q_i q_j / |r_ij|. Pairs in i < j order, each
+// acceleration accumulated from zero in that order (the order of
+// src/system.cpp:5-25); the x/y halves of every update are one FFMA2.
+template <int N, typename TPE>
+__device__ __forceinline__ void thread_forces(const float2 (&x)[ThreadShape<N>::NP],
+                                              float2 (&a)[ThreadShape<N>::NP], const FixedMol& M,
+                                              bool want_pe, TPE& pe) {
+  constexpr int NP = ThreadShape<N>::NP;
+  float2 axy[N];
+  float az[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    axy[i] = make_float2(0.0f, 0.0f);
+    az[i] = 0.0f;
+  }
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      if (j <= i) continue;  // constant trip count: the unrolled pair loop keeps every array in registers
+      const float2 rxy = __ffma2_rn(bcast(-1.0f), x[j], x[i]);
+      const float rz = flc<NP>(x, 2 * N + i) - flc<NP>(x, 2 * N + j);
+      const float d2 = fmaf(rxy.x, rxy.x, fmaf(rxy.y, rxy.y, rz * rz));
+      const float rinv = rsqrtf(d2);
+      const float u = M.pc[i * N + j] * rinv;  // pair potential k q_i q_j / r
+      if (want_pe) pe += static_cast<TPE>(u);
+      const float sc = u * (rinv * rinv);      // k q_i q_j / r^3
+      axy[i] = __ffma2_rn(rxy, bcast(sc), axy[i]);
+      az[i] = fmaf(rz, sc, az[i]);
+      axy[j] = __ffma2_rn(rxy, bcast(-sc), axy[j]);
+      az[j] = fmaf(-rz, sc, az[j]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    a[i] = __fmul2_rn(axy[i], bcast(M.inv_m[i]));
+    fl_set<NP>(a, 2 * N + i, az[i] * M.inv_m[i]);
+  }
+#pragma unroll
+  for (int f = 3 * N; f < 2 * NP; ++f) fl_set<NP>(a, f, 0.0f);
+}
+
 template <int N, int MODE>
-struct Sim {
+struct ThreadSim {
   static constexpr bool kKahan = (MODE & CE_PREC_KAHAN) != 0;
   static constexpr bool kF64 = (MODE & CE_PREC_FP64) != 0;
-  static constexpr int KC = kKahan ? N : 1;
+  static constexpr int NP = ThreadShape<N>::NP;
+  static constexpr int KP = kKahan ? NP : 1;
   using Acc = typename std::conditional<kF64, double, float>::type;
 
-  float x[N][3];
-  float v[N][3];
-  float k[6][N][3];  // k[0] = a(x) (FSAL), k[1..5] = stage accelerations 2..6
-  float cx[KC][3];   // Kahan compensation of the committed x / v updates
-  float cv[KC][3];
+  float2 x[NP];
+  float2 v[NP];
+  float2 k0[NP];  // k1 = a(x) (FSAL)
+  float2 cx[KP];  // Kahan compensation of the committed x / v updates
+  float2 cv[KP];
   float h;
   Acc t;
   Acc e0;
@@ -78,298 +196,276 @@ struct Sim {
   unsigned long long sim;
 };
 
-// a_i = (1/m_i) sum_j k q_i q_j r_ij / |r_ij|^3 with Newton's third law, and
-// (if WITH_PE) pe += sum_{i<j} k q_i q_j / |r_ij|.
-template <int N, bool WITH_PE, typename TPE>
-__device__ __forceinline__ void pair_forces(const float (&x)[N][3], float (&a)[N][3],
-                                            const FixedMol& M, TPE& pe) {
-#pragma unroll
-  for (int i = 0; i < N; ++i) a[i][0] = a[i][1] = a[i][2] = 0.0f;
-#pragma unroll
-  for (int i = 0; i < N; ++i) {
-#pragma unroll
-    for (int j = i + 1; j < N; ++j) {
-      const float rx = x[i][0] - x[j][0];
-      const float ry = x[i][1] - x[j][1];
-      const float rz = x[i][2] - x[j][2];
-      const float d2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
-      const float rinv = rsqrtf(d2);
-      const float u = M.pc[i * N + j] * rinv;  // pair potential k q_i q_j / r
-      if (WITH_PE) pe += static_cast<TPE>(u);
-      const float s = u * (rinv * rinv);       // k q_i q_j / r^3
-      a[i][0] = fmaf(rx, s, a[i][0]);
-      a[i][1] = fmaf(ry, s, a[i][1]);
-      a[i][2] = fmaf(rz, s, a[i][2]);
-      a[j][0] = fmaf(-rx, s, a[j][0]);
-      a[j][1] = fmaf(-ry, s, a[j][1]);
-      a[j][2] = fmaf(-rz, s, a[j][2]);
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < N; ++i) {
-    a[i][0] *= M.inv_m[i];
-    a[i][1] *= M.inv_m[i];
-    a[i][2] *= M.inv_m[i];
-  }
-}
-
-// FP64 finalize: KE, s = sqrt(E0/KE), p_i = (m_i s) v_i, KER; then the per-sim
-// output record. A converged sim with non-finite momenta is CE_SIM_NONFINITE.
+// FP64 finalize: KE, s = sqrt(E0/KE), p_i = (m_i s) v_i, KER = s^2 KE; then the
+// per-sim output record. A converged sim with non-finite momenta is
+// CE_SIM_NONFINITE.
 template <int N, int MODE>
-__device__ __forceinline__ void finalize(const Sim<N, MODE>& s, int status, double pe_final,
-                                         const RunParams& P, const FixedMol& M) {
+__device__ __forceinline__ void thread_finalize(const ThreadSim<N, MODE>& s, int status, double pe_final,
+                                                const RunParams& P, const FixedMol& M) {
+  constexpr int NP = ThreadShape<N>::NP;
   double ke = 0.0;
   bool finite = true;
 #pragma unroll
   for (int i = 0; i < N; ++i) {
-    const double vx = s.v[i][0], vy = s.v[i][1], vz = s.v[i][2];
+    const double vx = s.v[i].x, vy = s.v[i].y, vz = flc<NP>(s.v, 2 * N + i);
     ke += 0.5 * M.mass[i] * (vx * vx + vy * vy + vz * vz);
     finite = finite && isfinite(vx) && isfinite(vy) && isfinite(vz);
   }
   if (status == CE_SIM_OK && !finite) status = CE_SIM_NONFINITE;
-  const double sc = (P.redistribute && ke > 0.0) ? sqrt(static_cast<double>(s.e0) / ke) : 1.0;
-  double ker = 0.0;
+  const double e0d = static_cast<double>(s.e0);
+  const double sc =
+      (P.redistribute && ke > 0.0) ? (e0d > 0.0 ? e0d * rsqrt(e0d * ke) : sqrt(e0d / ke)) : 1.0;
   float* dst = P.momenta + s.sim * (3ull * N);
 #pragma unroll
   for (int i = 0; i < N; ++i) {
     const double mm = M.mass[i] * sc;
-    const double px = mm * static_cast<double>(s.v[i][0]);
-    const double py = mm * static_cast<double>(s.v[i][1]);
-    const double pz = mm * static_cast<double>(s.v[i][2]);
-    dst[i * 3 + 0] = static_cast<float>(px);
-    dst[i * 3 + 1] = static_cast<float>(py);
-    dst[i * 3 + 2] = static_cast<float>(pz);
-    ker += (px * px + py * py + pz * pz) / (2.0 * M.mass[i]);
+    dst[i * 3 + 0] = static_cast<float>(mm * static_cast<double>(s.v[i].x));
+    dst[i * 3 + 1] = static_cast<float>(mm * static_cast<double>(s.v[i].y));
+    dst[i * 3 + 2] = static_cast<float>(mm * static_cast<double>(flc<NP>(s.v, 2 * N + i)));
   }
-  if (P.ker) P.ker[s.sim] = ker;
+  if (P.ker) P.ker[s.sim] = (sc * sc) * ke;
   if (P.steps) P.steps[s.sim] = s.steps;
   if (P.status) P.status[s.sim] = static_cast<uint8_t>(status);
   if (P.rejects) P.rejects[s.sim] = s.rejects;
   if (P.t_final) P.t_final[s.sim] = static_cast<double>(s.t);
   if (P.pe_final) P.pe_final[s.sim] = pe_final;
   if (P.ke_before) P.ke_before[s.sim] = ke;
-  if (P.e0) P.e0[s.sim] = static_cast<double>(s.e0);
+  if (P.e0) P.e0[s.sim] = e0d;
   if (P.positions) {
     float* xp = P.positions + s.sim * (3ull * N);
 #pragma unroll
     for (int i = 0; i < N; ++i) {
-      xp[i * 3 + 0] = s.x[i][0];
-      xp[i * 3 + 1] = s.x[i][1];
-      xp[i * 3 + 2] = s.x[i][2];
+      xp[i * 3 + 0] = s.x[i].x;
+      xp[i * 3 + 1] = s.x[i].y;
+      xp[i * 3 + 2] = flc<NP>(s.x, 2 * N + i);
     }
   }
 }
 
-// Hairer's initial step from rest (src/integrators.cpp:197-250 with v0 = 0:
-// every velocity term is 0, sv = atol, and the probe accelerations equal k1).
+// Load sim `sim`, evaluate k1 and PE0 and choose the first step (Hairer's
+// heuristic from rest, src/integrators.cpp:197-250 with v0 = 0: every velocity
+// term is 0, sv = atol, and the probe accelerations equal k1; its quotients use
+// the fast forms, as the initial step is a heuristic). Returns false when the
+// sim is already finished (written out).
 template <int N, int MODE>
-__device__ __forceinline__ float initial_step(const Sim<N, MODE>& s, const RunParams& P) {
-  float d0_sq = 0.0f, d1_sq = 0.0f, d2_sq = 0.0f;
-#pragma unroll
-  for (int i = 0; i < N; ++i) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const float sx = P.atol + P.rtol * fabsf(s.x[i][c]);
-      const float r0 = s.x[i][c] / sx;
-      const float r1 = s.k[0][i][c] / P.atol;
-      d0_sq += r0 * r0;
-      d1_sq += r1 * r1;
-    }
-  }
-  const float denom = static_cast<float>(6 * N);
-  const float d0 = sqrtf(d0_sq / denom);
-  const float d1 = sqrtf(d1_sq / denom);
-  const float h0 = (static_cast<double>(d0) < 1e-5 || static_cast<double>(d1) < 1e-5)
-                       ? 1e-6f
-                       : 0.01f * d0 / d1;
-#pragma unroll
-  for (int i = 0; i < N; ++i) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const float sx = P.atol + P.rtol * fabsf(s.x[i][c]);
-      const float r = (s.k[0][i][c] * h0) / sx;  // (v1 - v0) / sx; (a1 - a0) = 0
-      d2_sq += r * r;
-    }
-  }
-  const float d2 = sqrtf(d2_sq / denom) / h0;
-  const float h1 = (static_cast<double>(d1) <= 1e-15 && static_cast<double>(d2) <= 1e-15)
-                       ? fmaxf(1e-6f, h0 * 1e-3f)
-                       : powf(0.01f / fmaxf(d1, d2), 0.2f);
-  float hmin = 100.0f * h0;
-  if (h1 < hmin) hmin = h1;
-  if (P.max_dt < hmin) hmin = P.max_dt;
-  return hmin;
-}
-
-// Load sim `sim` and prepare its first step. Returns false when the sim is
-// already finished (written out) and the lane stays idle.
-template <int N, int MODE>
-__device__ __forceinline__ bool init_sim(Sim<N, MODE>& s, unsigned long long sim,
-                                         const RunParams& P, const FixedMol& M) {
-  using Acc = typename Sim<N, MODE>::Acc;
+__device__ __forceinline__ bool thread_init(ThreadSim<N, MODE>& s, unsigned long long sim, const RunParams& P,
+                                            const FixedMol& M) {
+  using S = ThreadSim<N, MODE>;
+  using Acc = typename S::Acc;
+  constexpr int NP = ThreadShape<N>::NP;
   s.sim = sim;
   const float* src = P.pos + sim * (3ull * N);
 #pragma unroll
-  for (int i = 0; i < N; ++i) {
+  for (int p = 0; p < NP; ++p) s.x[p] = s.v[p] = make_float2(0.0f, 0.0f);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      s.x[i][c] = __ldg(src + i * 3 + c);
-      s.v[i][c] = 0.0f;
-    }
+  for (int i = 0; i < N; ++i) {
+    s.x[i] = make_float2(__ldg(src + 3 * i), __ldg(src + 3 * i + 1));
+    fl_set<NP>(s.x, 2 * N + i, __ldg(src + 3 * i + 2));
   }
 #pragma unroll
-  for (int i = 0; i < Sim<N, MODE>::KC; ++i)
-#pragma unroll
-    for (int c = 0; c < 3; ++c) s.cx[i][c] = s.cv[i][c] = 0.0f;
+  for (int p = 0; p < S::KP; ++p) s.cx[p] = s.cv[p] = make_float2(0.0f, 0.0f);
   Acc pe0 = Acc(0);
-  pair_forces<N, true>(s.x, s.k[0], M, pe0);
+  thread_forces<N, Acc>(s.x, s.k0, M, true, pe0);
   s.t = Acc(0);
-  s.steps = 0;
-  s.rejects = 0;
-  s.rej_in_step = 0;
+  s.steps = s.rejects = s.rej_in_step = 0u;
   s.rej_once = false;
   s.e0 = pe0;  // E_0 = PE_0 + KE_0, KE_0 = 0 (batched_integrator.hpp:137)
-  if (Sim<N, MODE>::kF64)
+  if (S::kF64)
     s.pe_stop = static_cast<Acc>(P.pe_stop_d * static_cast<double>(pe0));
   else
     s.pe_stop = static_cast<Acc>(P.pe_stop_f * static_cast<float>(pe0));
-  if (!isfinite(static_cast<double>(pe0))) {
-    finalize(s, CE_SIM_NONFINITE, static_cast<double>(pe0), P, M);
+  int fin = -1;
+  if (!isfinite(static_cast<double>(pe0))) fin = CE_SIM_NONFINITE;
+  else if (!(pe0 > s.pe_stop)) fin = CE_SIM_OK;  // already at or below the stop (driver.cpp:19)
+  else if (P.max_steps == 0u) fin = CE_SIM_MAX_STEPS;
+  if (fin >= 0) {
+    thread_finalize(s, fin, static_cast<double>(pe0), P, M);
     return false;
   }
-  if (!(pe0 > s.pe_stop)) {  // already at or below the stop (driver.cpp:19)
-    finalize(s, CE_SIM_OK, static_cast<double>(pe0), P, M);
-    return false;
+  float d0_sq = 0.0f, d1_sq = 0.0f;
+  const float inv_atol = __frcp_rn(P.atol);
+#pragma unroll
+  for (int f = 0; f < 3 * N; ++f) {
+    const float xf = flc<NP>(s.x, f);
+    const float r0 = __fdividef(xf, P.atol + P.rtol * fabsf(xf));
+    const float r1 = flc<NP>(s.k0, f) * inv_atol;
+    d0_sq += r0 * r0;
+    d1_sq += r1 * r1;
   }
-  if (P.max_steps == 0u) {
-    finalize(s, CE_SIM_MAX_STEPS, static_cast<double>(pe0), P, M);
-    return false;
+  constexpr float inv_denom = 1.0f / static_cast<float>(6 * N);
+  const float d0 = sqrt_approx(d0_sq * inv_denom);
+  const float d1 = sqrt_approx(d1_sq * inv_denom);
+  const float h0 = (static_cast<double>(d0) < 1e-5 || static_cast<double>(d1) < 1e-5) ? 1e-6f
+                                                                                         : __fdividef(0.01f * d0, d1);
+  float d2_sq = 0.0f;
+#pragma unroll
+  for (int f = 0; f < 3 * N; ++f) {
+    const float xf = flc<NP>(s.x, f);
+    const float r = __fdividef(flc<NP>(s.k0, f) * h0, P.atol + P.rtol * fabsf(xf));
+    d2_sq += r * r;
   }
-  s.h = initial_step(s, P);
+  const float d2 = __fdividef(sqrt_approx(d2_sq * inv_denom), h0);
+  const float h1 = (static_cast<double>(d1) <= 1e-15 && static_cast<double>(d2) <= 1e-15)
+                       ? fmaxf(1e-6f, h0 * 1e-3f)
+                       : __powf(__fdividef(0.01f, fmaxf(d1, d2)), 0.2f);
+  float hm = 100.0f * h0;
+  if (h1 < hm) hm = h1;
+  if (P.max_dt < hm) hm = P.max_dt;
+  s.h = hm;
   return true;
 }
 
 // One DP5(4) attempt (src/integrators.cpp:83-146) plus, on acceptance, the
-// driver's stop test (src/driver.cpp:19-30). Returns false once the sim is
-// finished and written out.
+// driver's stop test (src/driver.cpp:19-30). `ks` is this thread's first stage
+// chunk in shared memory; chunk c of stage slot l is ks[(l * NC + c) * B].
+// Returns false once the sim is finished and written out.
 template <int N, int MODE>
-__device__ __forceinline__ bool attempt(Sim<N, MODE>& s, const RunParams& P, const FixedMol& M) {
-  using S = Sim<N, MODE>;
+__device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE>& s, const RunParams& P, const FixedMol& M,
+                                               float4* ks, int B) {
+  using S = ThreadSim<N, MODE>;
   using Acc = typename S::Acc;
+  constexpr int NC = ThreadShape<N>::NC;
+  constexpr int NP = ThreadShape<N>::NP;
+  constexpr int NF = ThreadShape<N>::NF;
   const float hh = (P.max_dt < s.h) ? P.max_dt : s.h;  // std::min(h_, max_dt)
 
-  // Stages 2..6: x_s = x + h (c_s v + h sum_l abar_sl k_l); k_s = a(x_s).
-  {
-    float xs[N][3];
-#pragma unroll
-    for (int si = 1; si <= 5; ++si) {
-#pragma unroll
-      for (int i = 0; i < N; ++i) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          float sum = 0.0f;
-#pragma unroll
-          for (int l = 0; l + 1 < si; ++l) sum = fmaf(c_abar[si + 1][l + 1], s.k[l][i][c], sum);
-          const float inner = fmaf(hh, sum, c_c[si + 1] * s.v[i][c]);
-          xs[i][c] = fmaf(hh, inner, s.x[i][c]);
-        }
-      }
-      Acc unused = Acc(0);
-      pair_forces<N, false>(xs, s.k[si], M, unused);
-    }
-  }
-
-  // Stage 7 (row = 5th-order weights): x_new, v_new, the position half of the
-  // error and the k1..k6 part of the velocity error, before k7 is known.
-  float xn[N][3], vn[N][3], evp[N][3];
-  float cxn[S::KC][3], cvn[S::KC][3];
-  float err_sq = 0.0f;
-#pragma unroll
-  for (int i = 0; i < N; ++i) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      float sx = 0.0f, sv = 0.0f, se = 0.0f, sev = 0.0f;
-#pragma unroll
-      for (int l = 0; l < 6; ++l) {
-        if (l < 5) sx = fmaf(c_abar[7][l + 1], s.k[l][i][c], sx);
-        if (l != 1) sv = fmaf(c_b[l + 1], s.k[l][i][c], sv);  // b_2 = 0
-        se = fmaf(c_ebar[l + 1], s.k[l][i][c], se);
-        if (l != 1) sev = fmaf(c_e[l + 1], s.k[l][i][c], sev);  // E_2 = 0
-      }
-      const float incx = hh * fmaf(hh, sx, s.v[i][c]);  // c_7 = 1
-      const float incv = hh * sv;
-      if (S::kKahan) {
-        const float yx = incx - s.cx[i][c];
-        xn[i][c] = s.x[i][c] + yx;
-        cxn[i][c] = (xn[i][c] - s.x[i][c]) - yx;
-        const float yv = incv - s.cv[i][c];
-        vn[i][c] = s.v[i][c] + yv;
-        cvn[i][c] = (vn[i][c] - s.v[i][c]) - yv;
-      } else {
-        xn[i][c] = s.x[i][c] + incx;
-        vn[i][c] = s.v[i][c] + incv;
-      }
-      evp[i][c] = sev;
-      const float ex = (hh * hh) * se;
-      const float scx = fmaf(P.rtol, fmaxf(fabsf(s.x[i][c]), fabsf(xn[i][c])), P.atol);
-      const float r = __fdividef(ex, scx);
-      err_sq = fmaf(r, r, err_sq);
-    }
-  }
-  float k7[N][3];
+  // Stages 2..7: x_s = x + h (c_s v + h sum_l abar_sl k_l); k_s = a(x_s) into
+  // slot s - 2. Stage 7 (5th-order weights) gives x_new and, FSAL, k7 and PE.
+  float2 xs[NP], a[NP];
+  float2 cxn[S::KP];
   Acc pe_new = Acc(0);
-  pair_forces<N, true>(xn, k7, M, pe_new);
+#pragma unroll 1
+  for (int si = 1; si <= 6; ++si) {
+    const float cc = c_c[si + 1];
+    float2 sum[NP];
+    {
+      const float a1 = c_abar[si + 1][1];
 #pragma unroll
-  for (int i = 0; i < N; ++i) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const float ev = hh * fmaf(c_e[7], k7[i][c], evp[i][c]);
-      const float scv = fmaf(P.rtol, fmaxf(fabsf(s.v[i][c]), fabsf(vn[i][c])), P.atol);
-      const float r = __fdividef(ev, scv);
-      err_sq = fmaf(r, r, err_sq);
+      for (int p = 0; p < NP; ++p) sum[p] = __fmul2_rn(bcast(a1), s.k0[p]);
     }
+#pragma unroll 1
+    for (int l = 1; l + 1 < si; ++l) {
+      const float al = c_abar[si + 1][l + 1];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const float4 q = ks[((l - 1) * NC + c) * B];
+        sum[2 * c] = __ffma2_rn(bcast(al), make_float2(q.x, q.y), sum[2 * c]);
+        sum[2 * c + 1] = __ffma2_rn(bcast(al), make_float2(q.z, q.w), sum[2 * c + 1]);
+      }
+    }
+    if (S::kKahan && si == 6) {
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        const float2 inc = __fmul2_rn(bcast(hh), __ffma2_rn(bcast(hh), sum[p], __fmul2_rn(bcast(cc), s.v[p])));
+        const float2 y = __ffma2_rn(bcast(-1.0f), s.cx[p < S::KP ? p : 0], inc);
+        xs[p] = __fadd2_rn(s.x[p], y);
+        cxn[p < S::KP ? p : 0] = __ffma2_rn(bcast(-1.0f), y, __ffma2_rn(bcast(-1.0f), s.x[p], xs[p]));
+      }
+    } else {
+#pragma unroll
+      for (int p = 0; p < NP; ++p)
+        xs[p] = __ffma2_rn(bcast(hh), __ffma2_rn(bcast(hh), sum[p], __fmul2_rn(bcast(cc), s.v[p])), s.x[p]);
+    }
+    thread_forces<N, Acc>(xs, a, M, si == 6, pe_new);
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+      ks[((si - 1) * NC + c) * B] = make_float4(a[2 * c].x, a[2 * c].y, a[2 * c + 1].x, a[2 * c + 1].y);
   }
-  const float en = sqrtf(err_sq * (1.0f / static_cast<float>(6 * N)));
 
-  if (en <= 1.0f) {
+  // x_new = xs. Velocity update and error estimate, one chunk at a time (stage
+  // slots 0..4 hold k2..k6, slot 5 k7): v_new = v + h sum b_l k_l, position
+  // error h^2 sum ebar_l k_l, velocity error h sum E_l k_l (b_2 = E_2 = 0).
+  float2 vn[NP];
+  float2 cvn[S::KP];
+  float err_sq = 0.0f;
+  const float hh2 = hh * hh;
 #pragma unroll
-    for (int i = 0; i < N; ++i) {
+  for (int c = 0; c < NC; ++c) {
+    float4 q[6];
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        s.x[i][c] = xn[i][c];
-        s.v[i][c] = vn[i][c];
-        s.k[0][i][c] = k7[i][c];
-        if (S::kKahan) {
-          s.cx[i][c] = cxn[i][c];
-          s.cv[i][c] = cvn[i][c];
+    for (int l = 0; l < 6; ++l) q[l] = ks[(l * NC + c) * B];
+#pragma unroll
+    for (int hp = 0; hp < 2; ++hp) {
+      const int p = 2 * c + hp;
+      float2 sv = __fmul2_rn(bcast(c_b[1]), s.k0[p]);
+      float2 se = __fmul2_rn(bcast(c_ebar[1]), s.k0[p]);
+      float2 sev = __fmul2_rn(bcast(c_e[1]), s.k0[p]);
+#pragma unroll
+      for (int l = 1; l < 6; ++l) {
+        const float2 kl = hp == 0 ? make_float2(q[l - 1].x, q[l - 1].y) : make_float2(q[l - 1].z, q[l - 1].w);
+        if (l != 1) sv = __ffma2_rn(bcast(c_b[l + 1]), kl, sv);
+        se = __ffma2_rn(bcast(c_ebar[l + 1]), kl, se);
+        if (l != 1) sev = __ffma2_rn(bcast(c_e[l + 1]), kl, sev);
+      }
+      const float2 incv = __fmul2_rn(bcast(hh), sv);
+      if (S::kKahan) {
+        const float2 y = __ffma2_rn(bcast(-1.0f), s.cv[p < S::KP ? p : 0], incv);
+        vn[p] = __fadd2_rn(s.v[p], y);
+        cvn[p < S::KP ? p : 0] = __ffma2_rn(bcast(-1.0f), y, __ffma2_rn(bcast(-1.0f), s.v[p], vn[p]));
+      } else {
+        vn[p] = __fadd2_rn(s.v[p], incv);
+      }
+      const float2 ex = __fmul2_rn(bcast(hh2), se);
+      const float2 k7 = hp == 0 ? make_float2(q[5].x, q[5].y) : make_float2(q[5].z, q[5].w);
+      const float2 ev = __fmul2_rn(bcast(hh), __ffma2_rn(bcast(c_e[7]), k7, sev));
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        if (2 * p + e < NF) {
+          const float exe = e ? ex.y : ex.x, eve = e ? ev.y : ev.x;
+          const float x0 = e ? s.x[p].y : s.x[p].x, x1 = e ? xs[p].y : xs[p].x;
+          const float v0 = e ? s.v[p].y : s.v[p].x, v1 = e ? vn[p].y : vn[p].x;
+          const float rx = exe * rcp_approx(fmaf(P.rtol, fmaxf(fabsf(x0), fabsf(x1)), P.atol));
+          const float rv = eve * rcp_approx(fmaf(P.rtol, fmaxf(fabsf(v0), fabsf(v1)), P.atol));
+          err_sq = fmaf(rv, rv, fmaf(rx, rx, err_sq));
         }
       }
     }
-    float factor = (en == 0.0f) ? kMaxFactor : fminf(kMaxFactor, kSafety * __powf(en, kExponent));
+  }
+  // RMS norm squared: en <= 1 exactly when en^2 <= 1, and the controller's
+  // en^-1/5 is (en^2)^-1/10, so no square root is taken.
+  const float en2 = err_sq * (1.0f / static_cast<float>(6 * N));
+  if (en2 <= 1.0f) {
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      s.x[p] = xs[p];
+      s.v[p] = vn[p];
+    }
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const float4 q = ks[(5 * NC + c) * B];  // k7 becomes k1 (FSAL)
+      s.k0[2 * c] = make_float2(q.x, q.y);
+      s.k0[2 * c + 1] = make_float2(q.z, q.w);
+    }
+    if (S::kKahan) {
+#pragma unroll
+      for (int p = 0; p < S::KP; ++p) {
+        s.cx[p] = cxn[p];
+        s.cv[p] = cvn[p];
+      }
+    }
+    float factor = (en2 == 0.0f) ? kMaxFactor : fminf(kMaxFactor, kSafety * __powf(en2, 0.5f * kExponent));
     if (s.rej_once) factor = fminf(factor, 1.0f);
     const float hn = hh * factor;
     s.h = (P.max_dt < hn) ? P.max_dt : hn;
     s.t += static_cast<Acc>(hh);
     s.steps += 1u;
-    s.rej_in_step = 0;
+    s.rej_in_step = 0u;
     s.rej_once = false;
-    if (!(pe_new > s.pe_stop)) {
-      finalize(s, CE_SIM_OK, static_cast<double>(pe_new), P, M);
-      return false;
-    }
-    if (s.steps >= P.max_steps) {
-      finalize(s, CE_SIM_MAX_STEPS, static_cast<double>(pe_new), P, M);
+    int fin = -1;
+    if (!(pe_new > s.pe_stop)) fin = CE_SIM_OK;
+    else if (s.steps >= P.max_steps) fin = CE_SIM_MAX_STEPS;
+    if (fin >= 0) {
+      thread_finalize(s, fin, static_cast<double>(pe_new), P, M);
       return false;
     }
     return true;
   }
-  const float factor = fmaxf(kMinFactor, kSafety * __powf(en, kExponent));
-  s.h = hh * factor;
+  s.h = hh * fmaxf(kMinFactor, kSafety * __powf(en2, 0.5f * kExponent));
   s.rej_once = true;
   s.rejects += 1u;
   s.rej_in_step += 1u;
   if (s.rej_in_step > static_cast<uint32_t>(kMaxRejections)) {
-    finalize(s, CE_SIM_REJECT_LIMIT, static_cast<double>(pe_new), P, M);
+    thread_finalize(s, CE_SIM_REJECT_LIMIT, static_cast<double>(pe_new), P, M);
     return false;
   }
   return true;
@@ -377,18 +473,23 @@ __device__ __forceinline__ bool attempt(Sim<N, MODE>& s, const RunParams& P, con
 
 // Persistent kernel: each warp keeps its 32 lanes busy by pulling sim indices
 // from a global cursor (one warp-aggregated atomicAdd per refill) whenever at
-// least `refill_threshold` lanes are idle; no lane waits on another lane's sim.
+// least `refill_threshold` lanes are idle (or all of them). Launched with
+// thread_smem_bytes(N, blockDim.x) bytes of dynamic shared memory and at most
+// kThreadMaxBlock threads per block.
 template <int N, int MODE>
-__global__ void __launch_bounds__(256) rk45_fixed_kernel(const RunParams P, const FixedMol M) {
-  Sim<N, MODE> s;
+__global__ void __launch_bounds__(kThreadMaxBlock, ThreadShape<N>::kMinBlocks)
+    rk45_fixed_kernel(const RunParams P, const FixedMol M) {
+  extern __shared__ float4 ce_stage_slots[];
+  ThreadSim<N, MODE> s;
   bool active = false;
   bool queue_empty = false;
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lt_mask = (1u << lane) - 1u;
+  float4* ks = ce_stage_slots + threadIdx.x;
+  const int B = static_cast<int>(blockDim.x);
   for (;;) {
     const unsigned idle = __ballot_sync(0xffffffffu, !active);
-    if (!queue_empty && idle != 0u &&
-        (idle == 0xffffffffu || __popc(idle) >= P.refill_threshold)) {
+    if (!queue_empty && idle != 0u && (idle == 0xffffffffu || __popc(idle) >= P.refill_threshold)) {
       const int cnt = __popc(idle);
       const int leader = __ffs(idle) - 1;
       unsigned long long base = 0ull;
@@ -397,14 +498,14 @@ __global__ void __launch_bounds__(256) rk45_fixed_kernel(const RunParams P, cons
       queue_empty = (base + static_cast<unsigned long long>(cnt) >= P.S);
       if (!active) {
         const unsigned long long sim = base + static_cast<unsigned long long>(__popc(idle & lt_mask));
-        if (sim < P.S) active = init_sim(s, sim, P, M);
+        if (sim < P.S) active = thread_init(s, sim, P, M);
       }
     }
     if (!__any_sync(0xffffffffu, active)) {
       if (queue_empty) break;
       continue;
     }
-    if (active) active = attempt(s, P, M);
+    if (active) active = thread_attempt(s, P, M, ks, B);
   }
 }
 

@@ -110,8 +110,8 @@ typedef struct ce_outputs {
 /* Launch-shape knobs (0 = autotuned value if any, else the engine default). */
 typedef struct ce_tuning {
   int32_t block_threads;    /* threads per block, multiple of 32 up to 256; the     *
-                             * lane-per-atom and mixed-batch kernels run at most     *
-                             * 128 and clamp a larger request to 128                 */
+                             * integration kernels run at most 128 threads per      *
+                             * block and clamp a larger request to 128              */
   int32_t blocks_per_sm;    /* persistent grid = SMs * this (0: occupancy limit)    */
   int32_t refill_threshold; /* refill a warp once this many sims are idle (1..32;   *
                              * 0: a default per molecule size)                       */
@@ -232,7 +232,9 @@ int ce_autotune_mixed(ce_engine* e, uint64_t S, const ce_mixed_batch* dev_in, do
  * Limits: 1 <= n <= 10 atoms and S <= 2^40 sims; anything outside is rejected
  * with CE_ERR_INVALID before a launch. The first call on a device (that device
  * current) resolves the array's address once, so make it before any stream
- * capture. All calls share the cursor: each call clears it on `stream` first, and
+ * capture. The address is kept for the life of the process: a cudaDeviceReset
+ * (or any teardown of the device's primary context) between calls is not
+ * supported, as the array may then move. All calls share the cursor: each call clears it on `stream` first, and
  * calls that overlap on the GPU race on it. `err` (may be NULL) receives a
  * message of at most err_len bytes on failure. */
 int ce_run_device_noalloc(int n, const double* mass_me, const double* charge, double coulomb_k,

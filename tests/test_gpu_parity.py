@@ -50,6 +50,32 @@ def test_ch4_tight_matches_reference_engine(engine, ce, wl, golden_ch4, mode):
     assert abs(r.steps.mean() - steps_ref.mean()) <= 0.03 * steps_ref.mean()
 
 
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
+@pytest.mark.parametrize("point", ["prod", "tight"])
+def test_ch4_thread_per_sim_layout_matches_reference_engine(engine, ce, wl, golden_ch4, mode, point):
+    """The thread-per-sim kernel (rolled stage loop, stages in shared memory) on
+    the CH4 golden set, every precision mode, both tolerance points."""
+    g = golden_ch4
+    engine.set_tuning(lanes_per_sim=1)
+    try:
+        r = run(engine, ce, g["masses"], g["charges"], g["pos"], wl.TIGHT if point == "tight" else wl.PRODUCTION,
+                mode)
+    finally:
+        engine.set_tuning()
+    assert (r.status == 0).all()
+    if point == "tight":
+        for bits in (32, 64):
+            err = ol.config_norm_error(r.momenta, g[f"p_tight_f{bits}"])
+            assert err.max() <= TIGHT_MAX, (bits, err.max())
+        steps_ref = g["steps_tight_f32"].astype(float)
+    else:
+        err = ol.config_norm_error(r.momenta, g["p_prod_f32"])
+        assert np.median(err) <= PROD_MEDIAN and np.percentile(err, 99) <= PROD_P99 and err.max() <= PROD_MAX, (
+            np.median(err), np.percentile(err, 99), err.max())
+        steps_ref = g["steps_prod_f32"].astype(float)
+    assert abs(r.steps.mean() - steps_ref.mean()) <= 0.03 * steps_ref.mean()
+
+
 def test_ch4_tight_matches_scipy_oracle(engine, ce, wl, golden_ch4):
     g = golden_ch4
     n = len(g["p_scipy"])

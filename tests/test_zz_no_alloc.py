@@ -73,6 +73,26 @@ def test_noalloc_entry_point_matches_ce_run_device(ce, wl):
         np.testing.assert_array_equal(got["status"].cpu().numpy(), ref["status"].cpu().numpy())
         np.testing.assert_allclose(got["ker"].cpu().numpy(), ref["ker"].cpu().numpy(), rtol=TOL)
 
+    # The same two calls on a side stream (not torch's current stream), ordered by
+    # that stream alone: the cursor is cleared on the caller's stream, so stream
+    # order is all a caller needs to serialise calls.
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    outs = []
+    with torch.cuda.stream(side):
+        for call in range(2):
+            got = _device_buffers(torch, S, mol.n)
+            rc = lib.ce_run_device_noalloc(mol.n, m.ctypes.data, q.ctypes.data, 1.0, S, pos.data_ptr(), C.byref(c),
+                                           C.byref(_outputs(ce, got)), side.cuda_stream, err, len(err))
+            assert rc == ce.CE_OK, err.value.decode()
+            outs.append(got)
+    side.synchronize()
+    for call, got in enumerate(outs):
+        e = ol.config_norm_error(got["momenta"].cpu().numpy(), ref["momenta"].cpu().numpy())
+        assert e.max() <= TOL, ("side stream", call, e.max())
+        np.testing.assert_array_equal(got["steps"].cpu().numpy(), ref["steps"].cpu().numpy())
+        np.testing.assert_array_equal(got["status"].cpu().numpy(), ref["status"].cpu().numpy())
+
     # Sizes beyond the supported maximum are rejected before any launch.
     rc = lib.ce_run_device_noalloc(11, m.ctypes.data, q.ctypes.data, 1.0, S, pos.data_ptr(), C.byref(c),
                                    C.byref(_outputs(ce, ref)), stream, err, len(err))
