@@ -1195,8 +1195,9 @@ def main():
     # DRAM traffic of one integration launch, from the committed ncu summary of
     # this workload (dram__bytes_read.sum + dram__bytes_write.sum).
     traffic = None
-    tp = ROOT / "profiles" / f"rk45_atom_{args.molecule}_1e6.md"
-    if tp.exists() and S == S_DEFAULT and args.molecule == "ch4":
+    layout = "thread" if eng.get_tuning()["lanes_per_sim"] == 1 else "atom"
+    tp = ROOT / "profiles" / f"rk45_{layout}_{args.molecule}_1e6.md"
+    if tp.exists() and S == S_DEFAULT and args.molecule == "ch4" and args.mode == 0:
         import re
 
         m = re.search(r"traffic_bytes_per_launch:\s*([0-9]+)", tp.read_text())

@@ -19,15 +19,16 @@ namespace {
 
 // Launch shape for one run: explicit tuning fields win, then the autotuned
 // entry for this atom count, then the defaults (128 threads, occupancy-limited
-// grid, the per-size refill granularity of default_refill, one lane per atom for
-// N >= 2 -- measured faster on B200 than one thread per sim for CH4 and N = 10).
-ce_tuning effective_tuning(const ce_engine* e, int n) {
+// grid, the layout of default_lanes for this precision mode, the per-size refill
+// granularity of default_refill).
+ce_tuning effective_tuning(const ce_engine* e, int n, int mode) {
   ce_tuning t = e->tuning;
   const ce_tuned_entry& a = e->tuned_fixed[n];
   if (t.block_threads == 0) t.block_threads = a.valid && a.t.block_threads ? a.t.block_threads : 128;
   if (t.blocks_per_sm == 0 && a.valid) t.blocks_per_sm = a.t.blocks_per_sm;
   if (t.refill_threshold == 0 && a.valid) t.refill_threshold = a.t.refill_threshold;
-  if (t.lanes_per_sim == 0) t.lanes_per_sim = a.valid && a.t.lanes_per_sim ? a.t.lanes_per_sim : (n >= 2 ? n : 1);
+  if (t.lanes_per_sim == 0)
+    t.lanes_per_sim = a.valid && a.t.lanes_per_sim ? a.t.lanes_per_sim : ce::default_lanes(n, mode);
   if (n < 2) t.lanes_per_sim = 1;
   if (t.refill_threshold == 0) t.refill_threshold = ce::default_refill(n, t.lanes_per_sim);
   return t;
@@ -144,7 +145,7 @@ int ce_set_tuning(ce_engine* e, const ce_tuning* t) {
 
 int ce_get_tuning(const ce_engine* e, ce_tuning* t) {
   if (!e || !t) return CE_ERR_INVALID;
-  *t = e->has_mol ? effective_tuning(e, e->n) : e->tuning;
+  *t = e->has_mol ? effective_tuning(e, e->n, 0) : e->tuning;
   return CE_OK;
 }
 
@@ -177,12 +178,13 @@ int launch_fixed(ce_engine* e, uint64_t S, const float* pos, const ce_run_config
                  cudaStream_t s, unsigned long long* cursor) {
   cudaError_t st;
 
-  const ce_tuning t = effective_tuning(e, e->n);
+  const ce_tuning t = effective_tuning(e, e->n, cfg->precision_mode);
   const bool atom = t.lanes_per_sim >= 2;
   const ce::FixedKernelFn fn = atom ? ce::select_atom_kernel(e->n, cfg->precision_mode)
                                     : ce::select_fixed_kernel(e->n, cfg->precision_mode);
   if (!fn) return ce::fail(e, CE_ERR_INVALID, "ce_run: no kernel for this atom count");
-  const int block = std::min(t.block_threads, atom ? ce::kAtomMaxBlock : ce::kThreadMaxBlock);
+  // The thread-per-sim kernel's shared-memory offsets assume exactly kThreadMaxBlock threads.
+  const int block = atom ? std::min(t.block_threads, ce::kAtomMaxBlock) : ce::kThreadMaxBlock;
   const uint64_t sims_per_block =
       atom ? static_cast<uint64_t>(block / 32) * static_cast<uint64_t>(32 / e->n) : static_cast<uint64_t>(block);
   // The thread-per-sim kernel keeps its stage accelerations in dynamic shared memory.
@@ -191,6 +193,12 @@ int launch_fixed(ce_engine* e, uint64_t S, const float* pos, const ce_run_config
     st = cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
                               static_cast<int>(smem));
     if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaFuncSetAttribute(max dynamic shared memory)");
+    // All of the SM's unified L1 / shared storage as shared memory: the kernel
+    // reads almost nothing through L1, and CH4's seven stage slots per thread
+    // need 56 KB per block for four blocks per SM.
+    st = cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributePreferredSharedMemoryCarveout,
+                              cudaSharedmemCarveoutMaxShared);
+    if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaFuncSetAttribute(shared memory carveout)");
   }
   int per_sm = t.blocks_per_sm;
   if (per_sm == 0) {

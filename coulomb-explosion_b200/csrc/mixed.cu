@@ -515,9 +515,10 @@ int ce_autotune_fixed(ce_engine* e, uint64_t S, const float* pos_dev, const ce_r
   e->tuned_fixed[e->n].valid = false;
   std::vector<int> layouts = {1};
   if (e->n >= 2) layouts.push_back(e->n);
-  const int blocks_sim[] = {64, 128, 256};
-  const int blocks_atom[] = {64, 96, ce::kAtomMaxBlock};
-  const int refills[] = {0, 1, 2, 4};  // 0: the per-size default
+  // The thread-per-sim kernel always runs kThreadMaxBlock threads per block.
+  const std::vector<int> blocks_sim = {ce::kThreadMaxBlock};
+  const std::vector<int> blocks_atom = {64, 96, ce::kAtomMaxBlock};
+  const int refills[] = {0, 1, 2, 4, 8};  // 0: the per-size default
   double best = -1.0;
   ce_tuning best_t{};
   int count = 0;

@@ -73,10 +73,10 @@ int scratch_address(int dev, unsigned long long** addr, char* err, size_t err_le
   return CE_OK;
 }
 
-// The kernel ce_run_device launches by default: one lane per atom for n >= 2,
-// one thread per simulation for a single atom.
+// The kernel ce_run_device launches by default (ce::default_lanes): one thread
+// per simulation, or one lane per atom.
 ce::FixedKernelFn kernel_for(int n, int mode) {
-  if (n >= 2) {
+  if (ce::default_lanes(n, mode) >= 2) {
     switch (mode & 3) {
       case 0: return ce::atom_kernel_m0(n);
       case 1: return ce::atom_kernel_m1(n);
@@ -135,15 +135,21 @@ extern "C" int ce_run_device_noalloc(int n, const double* mass_me, const double*
 
   const ce::FixedKernelFn fn = kernel_for(n, cfg->precision_mode);
   const int block = 128;
-  // The one-atom (thread-per-sim) kernel takes its stage slots as dynamic shared
-  // memory (on-chip, per block; not an allocation).
-  const size_t smem = n >= 2 ? 0 : ce::thread_smem_bytes(n, block);
+  const int lanes = ce::default_lanes(n, cfg->precision_mode);
+  // The thread-per-sim kernel takes its stage slots as dynamic shared memory
+  // (on-chip, per block; not an allocation).
+  const size_t smem = lanes >= 2 ? 0 : ce::thread_smem_bytes(n, block);
+  if (smem > 0 &&
+      (cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            static_cast<int>(smem)) != cudaSuccess ||
+       cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributePreferredSharedMemoryCarveout,
+                            cudaSharedmemCarveoutMaxShared) != cudaSuccess))
+    return report(err, err_len, CE_ERR_CUDA, "ce_run_device_noalloc: shared-memory attribute failed");
   int per_sm = 0, sms = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem) != cudaSuccess ||
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     return report(err, err_len, CE_ERR_CUDA, "ce_run_device_noalloc: device query failed");
   if (per_sm < 1) per_sm = 1;
-  const int lanes = n >= 2 ? n : 1;
   const uint64_t sims_per_block =
       lanes >= 2 ? static_cast<uint64_t>(block / 32) * static_cast<uint64_t>(32 / n) : static_cast<uint64_t>(block);
   const uint64_t need = (S + sims_per_block - 1) / sims_per_block;

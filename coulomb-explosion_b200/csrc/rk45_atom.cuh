@@ -49,10 +49,23 @@ constexpr int kAtomMaxBlock = 128;
 // layout, a warp refills once floor((G - 1) / 3) of its groups are idle, at
 // least one (measured: CH4, G = 6: 1 beats 2 and 3 by 0.5 % and 1.5 %; stiff
 // H2O, G = 10: 3 beats 2 and 4 by 0.3 % and 3.7 %; N = 10, G = 3: 1).
-// Thread-per-sim refills at once. A refill threshold of 0 in RunParams or
-// ce_tuning means this per-size default.
+// Thread-per-sim refills once 4 of a warp's 32 sims are idle (CH4: 4 beats 1,
+// 2, 6 and 8 by 0.2 to 6 %); a single atom finishes at once, so 1. A refill
+// threshold of 0 in RunParams or ce_tuning means this per-size default.
 __host__ __device__ constexpr int default_refill(int n, int lanes_per_sim) {
-  return (lanes_per_sim < 2 || n < 2) ? 1 : ((32 / n - 1) / 3 > 1 ? (32 / n - 1) / 3 : 1);
+  return n < 2 ? 1 : (lanes_per_sim < 2 ? 4 : ((32 / n - 1) / 3 > 1 ? (32 / n - 1) / 3 : 1));
+}
+
+// Default layout of a fixed-molecule run (ce_tuning::lanes_per_sim): one thread
+// per sim for up to kThreadMaxAtoms atoms in the precision modes without Kahan
+// compensation, else one lane per atom. Measured on CH4 at the tight point:
+// 2.60e8 against 2.15e8 explosions/s (plain FP32); stiff H2O 5.05e8 against
+// 4.66e8; at 10 atoms the seven stage slots allow one 128-thread block per SM
+// and the lane layout wins (6.3e7 against 4.4e7); with the compensation terms
+// the thread layout spills (CH4, full precision form: 1.57e8 against 2.00e8).
+constexpr int kThreadMaxAtoms = 6;
+__host__ __device__ constexpr int default_lanes(int n, int mode) {
+  return n < 2 ? 1 : (((mode & CE_PREC_KAHAN) == 0 && n <= kThreadMaxAtoms) ? 1 : n);
 }
 
 template <int N>

@@ -20,10 +20,14 @@
 // attempt (six inlined force evaluations) was bound by instruction fetch. The
 // loop's stage index is warp-uniform (every thread of a warp runs the same
 // stage), so the Butcher coefficients are constant-bank loads at a uniform
-// index. Stage accelerations k2..k7 live in shared memory, one private
+// index; stage 7 (x_new, with the potential for the stop test) is peeled out of
+// the loop. Stage accelerations live in shared memory, one private
 // 16-byte-chunked slot per thread and stage laid out [stage][chunk][thread], so
-// a warp's 16-byte accesses touch consecutive addresses (no bank conflicts);
-// k1 (the FSAL acceleration), x and v stay in registers.
+// a warp's 16-byte accesses touch consecutive addresses (no bank conflicts):
+// slots 0..4 hold k2..k6, and k1 and k7 alternate between slots 5 and 6, so the
+// FSAL hand-over k1 <- k7 of an accepted step is a slot swap, not a copy. Only x
+// and v stay in registers (with k1 there too, CH4 needed more than 128
+// registers and spilled).
 //
 // In-register order of a 3N-vector: the N (x, y) pairs first, then the N z
 // components, padded with zeros to whole 16-byte chunks. Every x/y update of the
@@ -101,7 +105,7 @@ struct ThreadShape {
   static constexpr int NF = 3 * N;         // floats of a 3N-vector
   static constexpr int NC = (NF + 3) / 4;  // 16-byte chunks per stage slot
   static constexpr int NP = 2 * NC;        // float2 register pairs (zero-padded)
-  static constexpr int kSlots = 6;         // k2..k6 and k7 (k1 stays in registers)
+  static constexpr int kSlots = 7;         // k2..k6, and k1 / k7 alternating between two slots
   // Blocks of kThreadMaxBlock threads per SM the register allocator aims for:
   // 128 registers a thread for CH4-sized molecules, more for larger N (whose
   // shared-memory slots allow fewer blocks anyway).
@@ -110,10 +114,10 @@ struct ThreadShape {
 
 constexpr int kThreadMaxBlock = 128;
 
-// Dynamic shared memory of one thread-per-sim block: six stage slots of NC
+// Dynamic shared memory of one thread-per-sim block: seven stage slots of NC
 // 16-byte chunks for each of its threads.
 __host__ __device__ constexpr size_t thread_smem_bytes(int n, int block) {
-  return static_cast<size_t>(6) * static_cast<size_t>((3 * n + 3) / 4) * 16u * static_cast<size_t>(block);
+  return static_cast<size_t>(7) * static_cast<size_t>((3 * n + 3) / 4) * 16u * static_cast<size_t>(block);
 }
 
 // Flat float f of a register 3N-vector (x_i at 2i, y_i at 2i + 1, z_i at 2N + i);
@@ -184,7 +188,7 @@ struct ThreadSim {
 
   float2 x[NP];
   float2 v[NP];
-  float2 k0[NP];  // k1 = a(x) (FSAL)
+  int k1s;        // stage slot holding k1 = a(x) (FSAL): 5 or 6; k7 goes to the other
   float2 cx[KP];  // Kahan compensation of the committed x / v updates
   float2 cv[KP];
   float h;
@@ -242,14 +246,14 @@ __device__ __forceinline__ void thread_finalize(const ThreadSim<N, MODE>& s, int
   }
 }
 
-// Load sim `sim`, evaluate k1 and PE0 and choose the first step (Hairer's
+// Load sim `sim`, evaluate k1 (into stage slot 5) and PE0 and choose the first step (Hairer's
 // heuristic from rest, src/integrators.cpp:197-250 with v0 = 0: every velocity
 // term is 0, sv = atol, and the probe accelerations equal k1; its quotients use
 // the fast forms, as the initial step is a heuristic). Returns false when the
 // sim is already finished (written out).
 template <int N, int MODE>
 __device__ __forceinline__ bool thread_init(ThreadSim<N, MODE>& s, unsigned long long sim, const RunParams& P,
-                                            const FixedMol& M) {
+                                            const FixedMol& M, float4* ks, int B) {
   using S = ThreadSim<N, MODE>;
   using Acc = typename S::Acc;
   constexpr int NP = ThreadShape<N>::NP;
@@ -265,7 +269,12 @@ __device__ __forceinline__ bool thread_init(ThreadSim<N, MODE>& s, unsigned long
 #pragma unroll
   for (int p = 0; p < S::KP; ++p) s.cx[p] = s.cv[p] = make_float2(0.0f, 0.0f);
   Acc pe0 = Acc(0);
-  thread_forces<N, Acc>(s.x, s.k0, M, true, pe0);
+  float2 k0[NP];
+  thread_forces<N, Acc>(s.x, k0, M, true, pe0);
+  s.k1s = 5;
+#pragma unroll
+  for (int c = 0; c < ThreadShape<N>::NC; ++c)
+    ks[(5 * ThreadShape<N>::NC + c) * B] = make_float4(k0[2 * c].x, k0[2 * c].y, k0[2 * c + 1].x, k0[2 * c + 1].y);
   s.t = Acc(0);
   s.steps = s.rejects = s.rej_in_step = 0u;
   s.rej_once = false;
@@ -288,7 +297,7 @@ __device__ __forceinline__ bool thread_init(ThreadSim<N, MODE>& s, unsigned long
   for (int f = 0; f < 3 * N; ++f) {
     const float xf = flc<NP>(s.x, f);
     const float r0 = __fdividef(xf, P.atol + P.rtol * fabsf(xf));
-    const float r1 = flc<NP>(s.k0, f) * inv_atol;
+    const float r1 = flc<NP>(k0, f) * inv_atol;
     d0_sq += r0 * r0;
     d1_sq += r1 * r1;
   }
@@ -301,7 +310,7 @@ __device__ __forceinline__ bool thread_init(ThreadSim<N, MODE>& s, unsigned long
 #pragma unroll
   for (int f = 0; f < 3 * N; ++f) {
     const float xf = flc<NP>(s.x, f);
-    const float r = __fdividef(flc<NP>(s.k0, f) * h0, P.atol + P.rtol * fabsf(xf));
+    const float r = __fdividef(flc<NP>(k0, f) * h0, P.atol + P.rtol * fabsf(xf));
     d2_sq += r * r;
   }
   const float d2 = __fdividef(sqrt_approx(d2_sq * inv_denom), h0);
@@ -317,59 +326,90 @@ __device__ __forceinline__ bool thread_init(ThreadSim<N, MODE>& s, unsigned long
 
 // One DP5(4) attempt (src/integrators.cpp:83-146) plus, on acceptance, the
 // driver's stop test (src/driver.cpp:19-30). `ks` is this thread's first stage
-// chunk in shared memory; chunk c of stage slot l is ks[(l * NC + c) * B].
+// chunk in shared memory; chunk c of stage slot l is ks[(l * NC + c) * B], B =
+// the block's thread count (a run-time value: with it a compile-time constant
+// the compiler hoisted the slot loads and CH4 spilled, 20 % slower).
 // Returns false once the sim is finished and written out.
 template <int N, int MODE>
 __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE>& s, const RunParams& P, const FixedMol& M,
-                                               float4* ks, int B) {
+                                               float4* ks) {
   using S = ThreadSim<N, MODE>;
   using Acc = typename S::Acc;
   constexpr int NC = ThreadShape<N>::NC;
   constexpr int NP = ThreadShape<N>::NP;
   constexpr int NF = ThreadShape<N>::NF;
+  const int B = static_cast<int>(blockDim.x);
   const float hh = (P.max_dt < s.h) ? P.max_dt : s.h;  // std::min(h_, max_dt)
 
-  // Stages 2..7: x_s = x + h (c_s v + h sum_l abar_sl k_l); k_s = a(x_s) into
-  // slot s - 2. Stage 7 (5th-order weights) gives x_new and, FSAL, k7 and PE.
+  // Stages 2..6: x_s = x + h (c_s v + h sum_l abar_sl k_l); k_s = a(x_s) into
+  // slot s - 2.
   float2 xs[NP], a[NP];
-  float2 cxn[S::KP];
-  Acc pe_new = Acc(0);
+  {
+    Acc no_pe = Acc(0);
 #pragma unroll 1
-  for (int si = 1; si <= 6; ++si) {
-    const float cc = c_c[si + 1];
-    float2 sum[NP];
-    {
-      const float a1 = c_abar[si + 1][1];
+    for (int si = 1; si <= 5; ++si) {
+      const float cc = c_c[si + 1];
+      float2 sum[NP];
+      {
+        const float a1 = c_abar[si + 1][1];
+        const float4* k1 = ks + s.k1s * NC * B;
 #pragma unroll
-      for (int p = 0; p < NP; ++p) sum[p] = __fmul2_rn(bcast(a1), s.k0[p]);
-    }
+        for (int c = 0; c < NC; ++c) {
+          const float4 q = k1[c * B];
+          sum[2 * c] = __fmul2_rn(bcast(a1), make_float2(q.x, q.y));
+          sum[2 * c + 1] = __fmul2_rn(bcast(a1), make_float2(q.z, q.w));
+        }
+      }
 #pragma unroll 1
-    for (int l = 1; l + 1 < si; ++l) {
-      const float al = c_abar[si + 1][l + 1];
+      for (int l = 1; l + 1 < si; ++l) {
+        const float al = c_abar[si + 1][l + 1];
+        const float4* kl = ks + (l - 1) * NC * B;
 #pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        const float4 q = ks[((l - 1) * NC + c) * B];
-        sum[2 * c] = __ffma2_rn(bcast(al), make_float2(q.x, q.y), sum[2 * c]);
-        sum[2 * c + 1] = __ffma2_rn(bcast(al), make_float2(q.z, q.w), sum[2 * c + 1]);
+        for (int c = 0; c < NC; ++c) {
+          const float4 q = kl[c * B];
+          sum[2 * c] = __ffma2_rn(bcast(al), make_float2(q.x, q.y), sum[2 * c]);
+          sum[2 * c + 1] = __ffma2_rn(bcast(al), make_float2(q.z, q.w), sum[2 * c + 1]);
+        }
       }
-    }
-    if (S::kKahan && si == 6) {
-#pragma unroll
-      for (int p = 0; p < NP; ++p) {
-        const float2 inc = __fmul2_rn(bcast(hh), __ffma2_rn(bcast(hh), sum[p], __fmul2_rn(bcast(cc), s.v[p])));
-        const float2 y = __ffma2_rn(bcast(-1.0f), s.cx[p < S::KP ? p : 0], inc);
-        xs[p] = __fadd2_rn(s.x[p], y);
-        cxn[p < S::KP ? p : 0] = __ffma2_rn(bcast(-1.0f), y, __ffma2_rn(bcast(-1.0f), s.x[p], xs[p]));
-      }
-    } else {
 #pragma unroll
       for (int p = 0; p < NP; ++p)
         xs[p] = __ffma2_rn(bcast(hh), __ffma2_rn(bcast(hh), sum[p], __fmul2_rn(bcast(cc), s.v[p])), s.x[p]);
+      thread_forces<N, Acc>(xs, a, M, false, no_pe);
+      float4* out = ks + (si - 1) * NC * B;
+#pragma unroll
+      for (int c = 0; c < NC; ++c)
+        out[c * B] = make_float4(a[2 * c].x, a[2 * c].y, a[2 * c + 1].x, a[2 * c + 1].y);
     }
-    thread_forces<N, Acc>(xs, a, M, si == 6, pe_new);
+  }
+
+  // Stage 7 (row = 5th-order weights, c_7 = 1): x_new, and FSAL k7 with the
+  // potential energy of x_new for the stop test.
+  float2 cxn[S::KP];
+  Acc pe_new = Acc(0);
+  {
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      // one chunk's k2..k6 at a time keeps the stage-7 sums' live range short
+      const float4 q1 = ks[(s.k1s * NC + (p >> 1)) * B];
+      float2 sum = __fmul2_rn(bcast(c_abar[7][1]), (p & 1) ? make_float2(q1.z, q1.w) : make_float2(q1.x, q1.y));
+#pragma unroll
+      for (int l = 1; l < 6; ++l) {
+        const float4 q = ks[((l - 1) * NC + (p >> 1)) * B];
+        sum = __ffma2_rn(bcast(c_abar[7][l + 1]), (p & 1) ? make_float2(q.z, q.w) : make_float2(q.x, q.y), sum);
+      }
+      const float2 inner = __ffma2_rn(bcast(hh), sum, __fmul2_rn(bcast(c_c[7]), s.v[p]));
+      if (S::kKahan) {
+        const float2 y = __ffma2_rn(bcast(-1.0f), s.cx[p < S::KP ? p : 0], __fmul2_rn(bcast(hh), inner));
+        xs[p] = __fadd2_rn(s.x[p], y);
+        cxn[p < S::KP ? p : 0] = __ffma2_rn(bcast(-1.0f), y, __ffma2_rn(bcast(-1.0f), s.x[p], xs[p]));
+      } else {
+        xs[p] = __ffma2_rn(bcast(hh), inner, s.x[p]);
+      }
+    }
+    thread_forces<N, Acc>(xs, a, M, true, pe_new);
 #pragma unroll
     for (int c = 0; c < NC; ++c)
-      ks[((si - 1) * NC + c) * B] = make_float4(a[2 * c].x, a[2 * c].y, a[2 * c + 1].x, a[2 * c + 1].y);
+      ks[((11 - s.k1s) * NC + c) * B] = make_float4(a[2 * c].x, a[2 * c].y, a[2 * c + 1].x, a[2 * c + 1].y);
   }
 
   // x_new = xs. Velocity update and error estimate, one chunk at a time (stage
@@ -383,13 +423,16 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE>& s, const RunP
   for (int c = 0; c < NC; ++c) {
     float4 q[6];
 #pragma unroll
-    for (int l = 0; l < 6; ++l) q[l] = ks[(l * NC + c) * B];
+    for (int l = 0; l < 5; ++l) q[l] = ks[(l * NC + c) * B];
+    q[5] = ks[((11 - s.k1s) * NC + c) * B];
+    const float4 q1 = ks[(s.k1s * NC + c) * B];
 #pragma unroll
     for (int hp = 0; hp < 2; ++hp) {
       const int p = 2 * c + hp;
-      float2 sv = __fmul2_rn(bcast(c_b[1]), s.k0[p]);
-      float2 se = __fmul2_rn(bcast(c_ebar[1]), s.k0[p]);
-      float2 sev = __fmul2_rn(bcast(c_e[1]), s.k0[p]);
+      const float2 k1 = hp == 0 ? make_float2(q1.x, q1.y) : make_float2(q1.z, q1.w);
+      float2 sv = __fmul2_rn(bcast(c_b[1]), k1);
+      float2 se = __fmul2_rn(bcast(c_ebar[1]), k1);
+      float2 sev = __fmul2_rn(bcast(c_e[1]), k1);
 #pragma unroll
       for (int l = 1; l < 6; ++l) {
         const float2 kl = hp == 0 ? make_float2(q[l - 1].x, q[l - 1].y) : make_float2(q[l - 1].z, q[l - 1].w);
@@ -430,12 +473,7 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE>& s, const RunP
       s.x[p] = xs[p];
       s.v[p] = vn[p];
     }
-#pragma unroll
-    for (int c = 0; c < NC; ++c) {
-      const float4 q = ks[(5 * NC + c) * B];  // k7 becomes k1 (FSAL)
-      s.k0[2 * c] = make_float2(q.x, q.y);
-      s.k0[2 * c + 1] = make_float2(q.z, q.w);
-    }
+    s.k1s = 11 - s.k1s;  // k7 becomes k1 (FSAL)
     if (S::kKahan) {
 #pragma unroll
       for (int p = 0; p < S::KP; ++p) {
@@ -474,8 +512,8 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE>& s, const RunP
 // Persistent kernel: each warp keeps its 32 lanes busy by pulling sim indices
 // from a global cursor (one warp-aggregated atomicAdd per refill) whenever at
 // least `refill_threshold` lanes are idle (or all of them). Launched with
-// thread_smem_bytes(N, blockDim.x) bytes of dynamic shared memory and at most
-// kThreadMaxBlock threads per block.
+// kThreadMaxBlock threads per block and thread_smem_bytes(N, kThreadMaxBlock)
+// bytes of dynamic shared memory.
 template <int N, int MODE>
 __global__ void __launch_bounds__(kThreadMaxBlock, ThreadShape<N>::kMinBlocks)
     rk45_fixed_kernel(const RunParams P, const FixedMol M) {
@@ -498,14 +536,14 @@ __global__ void __launch_bounds__(kThreadMaxBlock, ThreadShape<N>::kMinBlocks)
       queue_empty = (base + static_cast<unsigned long long>(cnt) >= P.S);
       if (!active) {
         const unsigned long long sim = base + static_cast<unsigned long long>(__popc(idle & lt_mask));
-        if (sim < P.S) active = thread_init(s, sim, P, M);
+        if (sim < P.S) active = thread_init(s, sim, P, M, ks, B);
       }
     }
     if (!__any_sync(0xffffffffu, active)) {
       if (queue_empty) break;
       continue;
     }
-    if (active) active = thread_attempt(s, P, M, ks, B);
+    if (active) active = thread_attempt(s, P, M, ks);
   }
 }
 

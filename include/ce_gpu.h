@@ -110,8 +110,8 @@ typedef struct ce_outputs {
 /* Launch-shape knobs (0 = autotuned value if any, else the engine default). */
 typedef struct ce_tuning {
   int32_t block_threads;    /* threads per block, multiple of 32 up to 256; the     *
-                             * integration kernels run at most 128 threads per      *
-                             * block and clamp a larger request to 128              */
+                             * lane-per-atom and mixed kernels run at most 128 and  *
+                             * clamp a larger request; thread-per-sim runs 128      */
   int32_t blocks_per_sm;    /* persistent grid = SMs * this (0: occupancy limit)    */
   int32_t refill_threshold; /* refill a warp once this many sims are idle (1..32;   *
                              * 0: a default per molecule size)                       */
@@ -131,6 +131,9 @@ const char* ce_version(void);
 int ce_set_molecule(ce_engine* e, int n, const double* mass_me, const double* charge,
                     double coulomb_k);
 int ce_set_tuning(ce_engine* e, const ce_tuning* t);
+/* The launch shape a plain-FP32 run of the current molecule uses (explicit
+ * fields, else the autotuned entry, else the defaults: one thread per sim up to
+ * 6 atoms without Kahan compensation, else one lane per atom). */
 int ce_get_tuning(const ce_engine* e, ce_tuning* t);
 
 /* Integrate S explosions of the fixed molecule from rest.

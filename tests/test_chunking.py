@@ -52,8 +52,8 @@ def test_chunks_cover_the_batch(schedule, min_chunk, max_chunks):
 
 def test_default_refill(schedule):
     # floor((G - 1) / 3) idle groups of G = 32 / n sims per warp, at least one;
-    # one thread per sim refills at once
+    # one thread per sim refills once 4 sims of the warp are idle (a lone atom at once)
     rows = schedule("refill")
     assert [r[0] for r in rows] == list(range(1, 11))
     assert {r[0]: r[1] for r in rows} == {1: 1, 2: 5, 3: 3, 4: 2, 5: 1, 6: 1, 7: 1, 8: 1, 9: 1, 10: 1}
-    assert all(r[2] == 1 for r in rows)
+    assert {r[0]: r[2] for r in rows} == {1: 1, **{n: 4 for n in range(2, 11)}}
