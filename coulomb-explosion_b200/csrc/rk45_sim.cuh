@@ -327,8 +327,7 @@ __device__ __forceinline__ bool thread_init(ThreadSim<N, MODE>& s, unsigned long
 // One DP5(4) attempt (src/integrators.cpp:83-146) plus, on acceptance, the
 // driver's stop test (src/driver.cpp:19-30). `ks` is this thread's first stage
 // chunk in shared memory; chunk c of stage slot l is ks[(l * NC + c) * B], B =
-// the block's thread count (a run-time value: with it a compile-time constant
-// the compiler hoisted the slot loads and CH4 spilled, 20 % slower).
+// kThreadMaxBlock, so every slot offset is an immediate.
 // Returns false once the sim is finished and written out.
 template <int N, int MODE>
 __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE>& s, const RunParams& P, const FixedMol& M,
@@ -338,17 +337,18 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE>& s, const RunP
   constexpr int NC = ThreadShape<N>::NC;
   constexpr int NP = ThreadShape<N>::NP;
   constexpr int NF = ThreadShape<N>::NF;
-  const int B = static_cast<int>(blockDim.x);
+  constexpr int B = kThreadMaxBlock;
   const float hh = (P.max_dt < s.h) ? P.max_dt : s.h;  // std::min(h_, max_dt)
 
-  // Stages 2..6: x_s = x + h (c_s v + h sum_l abar_sl k_l); k_s = a(x_s) into
-  // slot s - 2.
+  // Stages 2..6: x_s = x + (c_s h) v + h^2 sum_l abar_sl k_l; k_s = a(x_s)
+  // into slot s - 2.
+  const float hh2 = hh * hh;
   float2 xs[NP], a[NP];
   {
     Acc no_pe = Acc(0);
 #pragma unroll 1
     for (int si = 1; si <= 5; ++si) {
-      const float cc = c_c[si + 1];
+      const float chh = c_c[si + 1] * hh;
       float2 sum[NP];
       {
         const float a1 = c_abar[si + 1][1];
@@ -373,7 +373,7 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE>& s, const RunP
       }
 #pragma unroll
       for (int p = 0; p < NP; ++p)
-        xs[p] = __ffma2_rn(bcast(hh), __ffma2_rn(bcast(hh), sum[p], __fmul2_rn(bcast(cc), s.v[p])), s.x[p]);
+        xs[p] = __ffma2_rn(bcast(hh2), sum[p], __ffma2_rn(bcast(chh), s.v[p], s.x[p]));
       thread_forces<N, Acc>(xs, a, M, false, no_pe);
       float4* out = ks + (si - 1) * NC * B;
 #pragma unroll
@@ -397,13 +397,13 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE>& s, const RunP
         const float4 q = ks[((l - 1) * NC + (p >> 1)) * B];
         sum = __ffma2_rn(bcast(c_abar[7][l + 1]), (p & 1) ? make_float2(q.z, q.w) : make_float2(q.x, q.y), sum);
       }
-      const float2 inner = __ffma2_rn(bcast(hh), sum, __fmul2_rn(bcast(c_c[7]), s.v[p]));
       if (S::kKahan) {
-        const float2 y = __ffma2_rn(bcast(-1.0f), s.cx[p < S::KP ? p : 0], __fmul2_rn(bcast(hh), inner));
+        const float2 inc = __ffma2_rn(bcast(hh2), sum, __fmul2_rn(bcast(hh), s.v[p]));
+        const float2 y = __ffma2_rn(bcast(-1.0f), s.cx[p < S::KP ? p : 0], inc);
         xs[p] = __fadd2_rn(s.x[p], y);
         cxn[p < S::KP ? p : 0] = __ffma2_rn(bcast(-1.0f), y, __ffma2_rn(bcast(-1.0f), s.x[p], xs[p]));
       } else {
-        xs[p] = __ffma2_rn(bcast(hh), inner, s.x[p]);
+        xs[p] = __ffma2_rn(bcast(hh2), sum, __ffma2_rn(bcast(hh), s.v[p], s.x[p]));  // c_7 = 1
       }
     }
     thread_forces<N, Acc>(xs, a, M, true, pe_new);
@@ -417,8 +417,7 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE>& s, const RunP
   // error h^2 sum ebar_l k_l, velocity error h sum E_l k_l (b_2 = E_2 = 0).
   float2 vn[NP];
   float2 cvn[S::KP];
-  float err_sq = 0.0f;
-  const float hh2 = hh * hh;
+  float2 err2 = make_float2(0.0f, 0.0f);
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
     float4 q[6];
@@ -451,22 +450,30 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE>& s, const RunP
       const float2 ex = __fmul2_rn(bcast(hh2), se);
       const float2 k7 = hp == 0 ? make_float2(q[5].x, q[5].y) : make_float2(q[5].z, q[5].w);
       const float2 ev = __fmul2_rn(bcast(hh), __ffma2_rn(bcast(c_e[7]), k7, sev));
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        if (2 * p + e < NF) {
-          const float exe = e ? ex.y : ex.x, eve = e ? ev.y : ev.x;
-          const float x0 = e ? s.x[p].y : s.x[p].x, x1 = e ? xs[p].y : xs[p].x;
-          const float v0 = e ? s.v[p].y : s.v[p].x, v1 = e ? vn[p].y : vn[p].x;
-          const float rx = exe * rcp_approx(fmaf(P.rtol, fmaxf(fabsf(x0), fabsf(x1)), P.atol));
-          const float rv = eve * rcp_approx(fmaf(P.rtol, fmaxf(fabsf(v0), fabsf(v1)), P.atol));
-          err_sq = fmaf(rv, rv, fmaf(rx, rx, err_sq));
-        }
+      // Scaled errors e / (atol + rtol max(|y0|, |y1|)), both halves of the pair
+      // at once; a zero-padded half is left out (its scale could be 0).
+      if (2 * p + 1 < NF) {
+        const float2 sx = __ffma2_rn(bcast(P.rtol),
+                                     make_float2(fmaxf(fabsf(s.x[p].x), fabsf(xs[p].x)),
+                                                 fmaxf(fabsf(s.x[p].y), fabsf(xs[p].y))),
+                                     bcast(P.atol));
+        const float2 sv2 = __ffma2_rn(bcast(P.rtol),
+                                      make_float2(fmaxf(fabsf(s.v[p].x), fabsf(vn[p].x)),
+                                                  fmaxf(fabsf(s.v[p].y), fabsf(vn[p].y))),
+                                      bcast(P.atol));
+        const float2 rx = __fmul2_rn(ex, make_float2(rcp_approx(sx.x), rcp_approx(sx.y)));
+        const float2 rv = __fmul2_rn(ev, make_float2(rcp_approx(sv2.x), rcp_approx(sv2.y)));
+        err2 = __ffma2_rn(rv, rv, __ffma2_rn(rx, rx, err2));
+      } else if (2 * p < NF) {
+        const float rx = ex.x * rcp_approx(fmaf(P.rtol, fmaxf(fabsf(s.x[p].x), fabsf(xs[p].x)), P.atol));
+        const float rv = ev.x * rcp_approx(fmaf(P.rtol, fmaxf(fabsf(s.v[p].x), fabsf(vn[p].x)), P.atol));
+        err2.x = fmaf(rv, rv, fmaf(rx, rx, err2.x));
       }
     }
   }
   // RMS norm squared: en <= 1 exactly when en^2 <= 1, and the controller's
   // en^-1/5 is (en^2)^-1/10, so no square root is taken.
-  const float en2 = err_sq * (1.0f / static_cast<float>(6 * N));
+  const float en2 = (err2.x + err2.y) * (1.0f / static_cast<float>(6 * N));
   if (en2 <= 1.0f) {
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
