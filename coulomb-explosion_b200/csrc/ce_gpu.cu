@@ -172,50 +172,72 @@ int ensure_pipeline(ce_engine* e) {
 
 namespace {
 
-// One fixed-molecule launch on `s`, its work queue at `cursor` (reset to 0 on
-// `s` first). Arguments are checked by the callers.
-int launch_fixed(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg, const ce_outputs* out,
-                 cudaStream_t s, unsigned long long* cursor) {
-  cudaError_t st;
+// Launch shape of a fixed-molecule run: kernel, block, dynamic shared memory,
+// resident blocks per SM and simulations per block.
+struct FixedShape {
+  ce::FixedKernelFn fn = nullptr;
+  int block = 0;
+  size_t smem = 0;
+  int per_sm = 0;
+  uint64_t sims_per_block = 0;
+  int refill = 0;
+};
 
-  const ce_tuning t = effective_tuning(e, e->n, cfg->precision_mode);
+int fixed_shape(ce_engine* e, int mode, FixedShape* sh) {
+  cudaError_t st;
+  const ce_tuning t = effective_tuning(e, e->n, mode);
   const bool atom = t.lanes_per_sim >= 2;
-  const ce::FixedKernelFn fn = atom ? ce::select_atom_kernel(e->n, cfg->precision_mode)
-                                    : ce::select_fixed_kernel(e->n, cfg->precision_mode);
-  if (!fn) return ce::fail(e, CE_ERR_INVALID, "ce_run: no kernel for this atom count");
+  sh->fn = atom ? ce::select_atom_kernel(e->n, mode) : ce::select_fixed_kernel(e->n, mode);
+  if (!sh->fn) return ce::fail(e, CE_ERR_INVALID, "ce_run: no kernel for this atom count");
   // The thread-per-sim kernel's shared-memory offsets assume exactly kThreadMaxBlock threads.
-  const int block = atom ? std::min(t.block_threads, ce::kAtomMaxBlock) : ce::kThreadMaxBlock;
-  const uint64_t sims_per_block =
-      atom ? static_cast<uint64_t>(block / 32) * static_cast<uint64_t>(32 / e->n) : static_cast<uint64_t>(block);
+  sh->block = atom ? std::min(t.block_threads, ce::kAtomMaxBlock) : ce::kThreadMaxBlock;
+  sh->sims_per_block = atom ? static_cast<uint64_t>(sh->block / 32) * static_cast<uint64_t>(32 / e->n)
+                            : static_cast<uint64_t>(sh->block);
+  sh->refill = t.refill_threshold;
   // The thread-per-sim kernel keeps its stage accelerations in dynamic shared memory.
-  const size_t smem = atom ? 0 : ce::thread_smem_bytes(e->n, block);
-  if (smem > 0) {
-    st = cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              static_cast<int>(smem));
+  sh->smem = atom ? 0 : ce::thread_smem_bytes(e->n, sh->block);
+  if (sh->smem > 0) {
+    st = cudaFuncSetAttribute(reinterpret_cast<const void*>(sh->fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              static_cast<int>(sh->smem));
     if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaFuncSetAttribute(max dynamic shared memory)");
     // All of the SM's unified L1 / shared storage as shared memory: the kernel
     // reads almost nothing through L1, and CH4's seven stage slots per thread
     // need 56 KB per block for four blocks per SM.
-    st = cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributePreferredSharedMemoryCarveout,
+    st = cudaFuncSetAttribute(reinterpret_cast<const void*>(sh->fn), cudaFuncAttributePreferredSharedMemoryCarveout,
                               cudaSharedmemCarveoutMaxShared);
     if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaFuncSetAttribute(shared memory carveout)");
   }
-  int per_sm = t.blocks_per_sm;
-  if (per_sm == 0) {
-    st = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem);
+  sh->per_sm = t.blocks_per_sm;
+  if (sh->per_sm == 0) {
+    st = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh->per_sm, sh->fn, sh->block, sh->smem);
     if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-    if (per_sm < 1) per_sm = 1;
+    if (sh->per_sm < 1) sh->per_sm = 1;
   }
+  return CE_OK;
+}
+
+// One fixed-molecule launch on `s`, its work queue at `cursor` (reset to 0 on
+// `s` first). Arguments are checked by the callers.
+int launch_fixed(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg, const ce_outputs* out,
+                 cudaStream_t s, unsigned long long* cursor) {
+  FixedShape sh;
+  int rc = fixed_shape(e, cfg->precision_mode, &sh);
+  if (rc != CE_OK) return rc;
+  const ce::FixedKernelFn fn = sh.fn;
+  const int block = sh.block;
+  const size_t smem = sh.smem;
+  const int per_sm = sh.per_sm;
+  const uint64_t sims_per_block = sh.sims_per_block;
   const uint64_t need_blocks = (S + sims_per_block - 1) / sims_per_block;
   const uint64_t grid = std::min<uint64_t>(static_cast<uint64_t>(e->sms) * per_sm, need_blocks);
 
   ce::RunParams P{};
-  ce::fill_run_params(P, cfg, out, t.refill_threshold);
+  ce::fill_run_params(P, cfg, out, sh.refill);
   P.pos = pos;
   P.cursor = cursor;
   P.S = S;
 
-  st = cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), s);
+  cudaError_t st = cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), s);
   if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMemsetAsync(cursor)");
   fn<<<static_cast<unsigned>(grid), block, smem, s>>>(P, e->mol);
   st = cudaGetLastError();
@@ -251,6 +273,8 @@ int ce_run_device(ce_engine* e, uint64_t S, const float* pos, const ce_run_confi
 // integrate on two compute streams with a work-queue cursor each, so a chunk's
 // persistent blocks take over SMs as the previous chunk's blocks retire instead
 // of waiting for its last simulation.
+constexpr uint64_t kResidentPerChunk = 2;
+
 int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
            const ce_outputs* out) {
   if (!e) return CE_ERR_INVALID;
@@ -266,10 +290,19 @@ int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
   rc = ce::ensure_pipeline(e);
   if (rc != CE_OK) return rc;
 
-  // chunking: one chunk below 2^17 sims, else up to 16 chunks of at least 2^16
-  // (measured on CH4 1e6: 8 chunks 1.79e8/s end to end, 16 1.85e8, 32 1.75e8)
+  // Chunking: up to 16 chunks, each at least kResidentPerChunk times the sims the
+  // persistent grid holds at once (and 2^16), so a chunk's last simulations are
+  // a small part of its run. One chunk below twice that. Measured on CH4 1e6
+  // with the thread-per-sim kernel (75,776 sims resident), end to end: 1x the
+  // resident count 2.29e8/s, 2x 2.47e8, 3x 2.25e8, 4x 2.19e8 (device-resident
+  // 2.74e8); with a fixed 2^16 minimum 2.24e8.
+  FixedShape sh;
+  rc = fixed_shape(e, cfg->precision_mode, &sh);
+  if (rc != CE_OK) return rc;
+  const uint64_t resident = static_cast<uint64_t>(e->sms) * static_cast<uint64_t>(sh.per_sm) * sh.sims_per_block;
+  const uint64_t min_chunk = std::max<uint64_t>(1ull << 16, kResidentPerChunk * resident);
   uint64_t bnd[17], C = 0;
-  const uint64_t nchunks = ce::chunk_bounds(S, 1ull << 16, 16, bnd, &C);
+  const uint64_t nchunks = ce::chunk_bounds(S, min_chunk, 16, bnd, &C);
   auto bound = [&](uint64_t k) -> uint64_t { return bnd[k]; };
   const size_t n3 = static_cast<size_t>(e->n) * 3;
   auto al = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
