@@ -907,6 +907,55 @@ def run_stream(args):
                 gph.close()
     acc, fbk = clo.counts()
 
+    # ---- kernel-level rooflines, event-timed outside the stream: the plain
+    # integration of chunk 0 (FP32 CUDA cores, algorithmic FLOPs from its own
+    # step counts at N = 10, P = 45) and the closure network's fused forward on
+    # C_ rows (tensor cores, against the measured bf16 peak)
+    d0 = slots[0]
+    assert lib.ce_sample_ball_device(10, 0, C_, ctypes.byref(bcfg), ctypes.c_void_p(d0["batch"].pos.data_ptr()),
+                                     None, ctypes.c_void_p(cs)) == 0
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(4)]
+    for a_, b_ in evs:
+        a_.record(compute)
+        eng.run_mixed_device(C_, d0["cb"], cfg, d0["out"], sched, cs)
+        b_.record(compute)
+    torch.cuda.synchronize()
+    int_ms = float(np.median([a_.elapsed_time(b_) for a_, b_ in evs[1:]]))
+    int_flops = float(flops_per_sim(d0["steps"].cpu().numpy().astype(np.uint32), 10).sum())
+    fp32 = measure_fp32_peak(torch, dev)
+    int_tf = int_flops / (int_ms / 1e3) / 1e12
+    rows = cl.pad128(C_)
+    gx = torch.Generator(device=dev)
+    gx.manual_seed(seed)
+    xf = torch.randn((rows, ce.CLOSURE_FEATURES), generator=gx, device=dev).to(torch.bfloat16)
+    of = torch.empty((rows, ce.CLOSURE_OUTPUTS), dtype=torch.float32, device=dev)
+    for a_, b_ in evs:
+        a_.record(compute)
+        net.forward(xf, of, rows, cs)
+        b_.record(compute)
+    torch.cuda.synchronize()
+    net.check(cs)
+    fwd_ms = float(np.median([a_.elapsed_time(b_) for a_, b_ in evs[1:]]))
+    fl_row = 2 * (ce.CLOSURE_FEATURES * net.hidden + (net.depth - 1) * net.hidden * net.hidden + net.hidden * 32)
+    fwd_tf = fl_row * rows / (fwd_ms / 1e3) / 1e12
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    bf16_peak = peaks.get("bf16_tflops") or 1590.0
+    del xf, of
+
+    # ---- the reference's SIMD batched engine on this host, same molecule and
+    # tolerance point, on a bounded sample of the stream's geometries
+    cpu = None
+    if not args.no_cpu:
+        n_cpu = 1 << 17
+        x_cpu, _, fl_cpu = sp.sample_ball_host(mol, n_cpu, seed=seed, first_sim=0)
+        assert not fl_cpu.any()
+        cpu = cpu_batched_baseline(x_cpu.astype(np.float64), mol, TIGHT, all_steps=3, single_reps=5,
+                                   single_sample=4096, scalar_sample=1024)
+        if cpu:
+            cpu["sample"] = f"{n_cpu} sims of the stream (first chunk's geometries), " + cpu["sample"].split(", ", 1)[1]
+            cpu["gpu_e2e_speedup_vs_all_cores"] = res["plain"]["explosions_per_s"] / cpu["value"]
+            cpu["gpu_e2e_speedup_vs_single_core"] = res["plain"]["explosions_per_s"] / cpu["single_core_value"]
+
     # accuracy on the first chunk: closure vs plain, both vs the FP64 oracle on a subset
     pc = firsts["closure"]["momenta"].double()
     pp = firsts["plain"]["momenta"].double()
@@ -945,6 +994,19 @@ def run_stream(args):
         "closure_last_chunk": {"accepted": acc, "fallback": fbk},
         "gate": {"tol_energy": gate.tol_energy, "tol_momentum": gate.tol_momentum,
                  "tol_correction": gate.tol_correction},
+        "e2e": {"value": res["closure"]["explosions_per_s"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": d2h_bytes * (total // C_),
+                "path": "whole stream, first geometry to last host byte: geometries drawn on the device (no input "
+                        "copy), every chunk's results copied into pinned host memory"},
+        "roofline": {"bound": "fp32", "kernel": "plain integration of one 1e6-sim chunk (mixed-batch kernels, "
+                                                "N = 10), event-timed outside the stream",
+                     "achieved": int_tf, "peak": fp32["tflops"], "unit": "TFLOP/s", "frac": int_tf / fp32["tflops"],
+                     "peak_source": fp32["source"], "flops_per_chunk": int_flops, "chunk_ms": int_ms},
+        "roofline_network": {"bound": "tensor", "kernel": f"fused closure-network forward, {rows} rows",
+                             "achieved": fwd_tf, "peak": bf16_peak, "unit": "TFLOP/s", "frac": fwd_tf / bf16_peak,
+                             "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback 1590",
+                             "chunk_ms": fwd_ms},
+        "cpu_baseline": cpu,
         "rel_err_vs_plain_first_chunk": dist_t(e_cp),
         "rel_err_vs_fp64": {"subset": n_sub, "closure": dist_n(e64_c), "plain": dist_n(e64_p),
                             "fp64": "oracle f64, rtol 1e-10, atol 1e-16, pe_stop 1e-11"},
