@@ -427,8 +427,9 @@ def run_precision(args):
     >= 0.3), 1e6 sims each, every precision mode at the production and tight
     points. Errors against the FP64 reference (oracle f64 at rtol 1e-12 /
     atol 1e-20 / pe_stop 1e-13) on a 1e4 subset: per-atom |dp_i| / |p_i| and the
-    per-sim config norm; energy drift |KE + PE_final - E0| / E0 before
-    redistribution; accepted steps per sim."""
+    per-sim config norm; the config norm against the FP64 scipy oracle (the
+    reference's simulate_explosion, restated) on the same subset; energy drift
+    |KE + PE_final - E0| / E0 before redistribution; accepted steps per sim."""
     import importlib
 
     import torch
@@ -441,10 +442,12 @@ def run_precision(args):
     sys.path.insert(0, str(ROOT / "tests"))
     import oracle_lib as ol
 
+    so = _scipy_oracle()
     S = args.sims
     n_sub = min(10_000, S)
     eng = ce.Engine(0)
     rows = []
+    scipy_check = {}
     for name, mol in (("CH4", wl.CH4), ("H2O-stiff", wl.H2O_STIFF)):
         pos, pos64, flags = sp.sample_ball_host(mol, S, seed=SEED)
         assert not flags.any()
@@ -452,6 +455,11 @@ def run_precision(args):
         ref = ol.run_batch(pos[sub].astype(np.float64), mol.masses_me, mol.charge_array, bits=64, rtol=1e-12,
                            atol=1e-20, pe_stop=1e-13)
         pe0 = np.array([ol.potential(x, mol.charge_array) for x in pos[sub].astype(np.float64)])
+        t_sci = time.perf_counter()
+        sci = so.run_many(pos[sub].astype(np.float64), mol.masses_me, mol.charge_array)
+        e_rs = ol.config_norm_error(ref["momenta"], sci)
+        scipy_check[name] = {"fp64_reference_vs_scipy": {"median": float(np.median(e_rs)), "max": float(e_rs.max())},
+                             "scipy_seconds": time.perf_counter() - t_sci}
         eng.set_molecule(mol.masses_me, mol.charge_array)
         x_d = torch.from_numpy(pos).cuda()
         for point_name, (rtol, atol, pes) in (("production", wl.PRODUCTION), ("tight", wl.TIGHT)):
@@ -477,6 +485,7 @@ def run_precision(args):
                 p = mom.cpu().numpy()[sub].astype(np.float64)
                 atom_err = np.linalg.norm(p - ref["momenta"], axis=2) / np.linalg.norm(ref["momenta"], axis=2)
                 cn = ol.config_norm_error(p, ref["momenta"])
+                cs_ = ol.config_norm_error(p, sci)
                 drift = np.abs(keb.cpu().numpy()[sub] + pef.cpu().numpy()[sub] - pe0) / pe0
                 rows.append({
                     "molecule": name, "point": point_name, "rtol": rtol, "atol": atol, "pe_stop": pes,
@@ -486,13 +495,17 @@ def run_precision(args):
                                      "max": float(atom_err.max())},
                     "config_rel_err": {"median": float(np.median(cn)), "p99": float(np.percentile(cn, 99)),
                                        "max": float(cn.max())},
+                    "config_rel_err_vs_scipy": {"median": float(np.median(cs_)), "p99": float(np.percentile(cs_, 99)),
+                                                "max": float(cs_.max())},
                     "energy_drift": {"median": float(np.median(drift)), "max": float(drift.max())},
                     "mean_steps": float(stp.cpu().numpy().mean()),
                     "status_ok_frac": float((sts.cpu().numpy() == 0).mean()),
                 })
     eng.close()
     print(json.dumps({"metric": "precision study (CH4 and stiff H2O, every precision mode)", "sims_per_case": S, "fp64_subset": n_sub,
-                      "fp64_reference": "oracle f64, rtol 1e-12, atol 1e-20, pe_stop 1e-13", "rows": rows}))
+                      "fp64_reference": "oracle f64, rtol 1e-12, atol 1e-20, pe_stop 1e-13",
+                      "fp64_scipy": "solve_ivp RK45 to t = 1e10, rtol 1e-8, atol 1e-16 (the reference's Python oracle, "
+                                    "restated), same subset", "scipy_check": scipy_check, "rows": rows}))
     return 0
 
 
