@@ -81,6 +81,13 @@ class CeMixedBatch(C.Structure):
     _fields_ = [("n_atoms", C.c_void_p), ("mass_me", C.c_void_p), ("charge", C.c_void_p), ("pos", C.c_void_p)]
 
 
+class CeSimState(C.Structure):
+    """ce_sim_state: a run's saved integrator state, or the state a resumed run
+    continues from (device pointers, mixed layout)."""
+    _fields_ = [("positions", C.c_void_p), ("velocities", C.c_void_p), ("h", C.c_void_p), ("t", C.c_void_p),
+                ("steps", C.c_void_p), ("rejects", C.c_void_p), ("e0", C.c_void_p), ("comp", C.c_void_p)]
+
+
 class CeTuneResult(C.Structure):
     _fields_ = [("t", CeTuning), ("sims_per_s", C.c_double), ("schedule", C.c_int32)]
 
@@ -138,6 +145,11 @@ _SIGNATURES = {
                               C.c_int),
     "ce_probe_bounded_wait": ([C.c_int, C.c_uint, C.POINTER(C.c_int)], C.c_int),
     "ce_reserve_mixed": ([C.c_void_p, C.c_uint64], C.c_int),
+    "ce_run_mixed_device_state": (
+        [C.c_void_p, C.c_uint64, C.POINTER(CeMixedBatch), C.c_double, C.POINTER(CeRunConfig), C.POINTER(CeSimState),
+         C.POINTER(CeSimState), C.POINTER(CeOutputs), C.c_int, C.c_void_p],
+        C.c_int,
+    ),
     "ce_run_mixed_device": (
         [C.c_void_p, C.c_uint64, C.POINTER(CeMixedBatch), C.c_double, C.POINTER(CeRunConfig), C.POINTER(CeOutputs),
          C.c_int, C.c_void_p],
@@ -401,6 +413,16 @@ class Engine:
         c = cfg.to_c()
         self._check(self.lib.ce_run_mixed(self.h, S, C.byref(batch), float(coulomb_k), C.byref(c), C.byref(out)))
         return r
+
+    def run_mixed_device_state(self, S: int, batch: CeMixedBatch, cfg: RunConfig, out: CeOutputs,
+                               resume: "CeSimState | None" = None, save: "CeSimState | None" = None,
+                               schedule: int = CE_SCHEDULE_ONE_LAUNCH, stream: int = 0, coulomb_k: float = 1.0):
+        """ce_run_mixed_device_state: save the integrator state of every sim it
+        finishes and / or continue sims from a saved state."""
+        c = cfg.to_c()
+        self._check(self.lib.ce_run_mixed_device_state(
+            self.h, int(S), C.byref(batch), float(coulomb_k), C.byref(c), C.byref(resume) if resume else None,
+            C.byref(save) if save else None, C.byref(out), int(schedule), C.c_void_p(stream)))
 
     def run_mixed_device(self, S: int, batch: CeMixedBatch, cfg: RunConfig, out: CeOutputs,
                          schedule: int = CE_SCHEDULE_ONE_LAUNCH, stream: int = 0, coulomb_k: float = 1.0):

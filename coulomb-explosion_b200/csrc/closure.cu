@@ -493,6 +493,11 @@ struct ce_closure {
   double *e0 = nullptr, *pef = nullptr;
   uint8_t* st = nullptr;
   uint32_t* steps = nullptr;
+  // the rest of the integrator state at the loose stop, from which the sims the
+  // gate sends back continue
+  float *vel = nullptr, *h = nullptr, *comp = nullptr;
+  double* t = nullptr;
+  uint32_t* rej = nullptr;
   // network
   bf16* feats = nullptr;
   float *out = nullptr, *pbase = nullptr, *pscale = nullptr;
@@ -584,7 +589,9 @@ int ce_closure_create(ce_closure** out, ce_engine* e, ce_mlp* net, uint64_t max_
   auto al = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
   const size_t sizes[] = {al(S * 3 * kA * 4), al(S * 3 * kA * 4), al(S * 8), al(S * 8), al(S), al(S * 4),
                           al(Sp * kFeat * 2), al(Sp * kOut * 4), al(S * 3 * kA * 4), al(S * 4),
-                          al(S), al(S * 3 * kA * 4), al(S * 8), al(S * 4), al(S), al(2 * 8)};
+                          al(S), al(S * 3 * kA * 4), al(S * 8), al(S * 4), al(S), al(2 * 8),
+                          al(S * 3 * kA * 4), al(S * 4), al(S * 6 * kA * 4), al(S * 8), al(S * 4)};
+  constexpr int kSlots = sizeof(sizes) / sizeof(sizes[0]);
   size_t total = 0;
   for (size_t b : sizes) total += b;
   if (cudaSetDevice(e->device) != cudaSuccess || cudaMalloc(&c->arena, total) != cudaSuccess) {
@@ -592,8 +599,8 @@ int ce_closure_create(ce_closure** out, ce_engine* e, ce_mlp* net, uint64_t max_
     return CE_ERR_CUDA;
   }
   char* p = static_cast<char*>(c->arena);
-  void* slot[16];
-  for (int i = 0; i < 16; ++i) {
+  void* slot[kSlots];
+  for (int i = 0; i < kSlots; ++i) {
     slot[i] = p;
     p += sizes[i];
   }
@@ -613,6 +620,11 @@ int ce_closure_create(ce_closure** out, ce_engine* e, ce_mlp* net, uint64_t max_
   c->fb_steps = static_cast<uint32_t*>(slot[13]);
   c->fb_st = static_cast<uint8_t*>(slot[14]);
   c->counts = static_cast<unsigned long long*>(slot[15]);
+  c->vel = static_cast<float*>(slot[16]);
+  c->h = static_cast<float*>(slot[17]);
+  c->comp = static_cast<float*>(slot[18]);
+  c->t = static_cast<double*>(slot[19]);
+  c->rej = static_cast<uint32_t*>(slot[20]);
   // padded network rows stay finite
   cudaMemset(c->out, 0, sizes[7]);
   const int rc = ce_reserve_mixed(e, max_sims);
@@ -650,19 +662,18 @@ int ce_closure_serve(ce_closure* c, uint64_t S, const ce_mixed_batch* in, double
   if (cudaMemsetAsync(c->counts, 0, 2 * sizeof(unsigned long long), s) != cudaSuccess)
     return cfail(c, CE_ERR_CUDA, "memset counts");
 
-  // 1. integrate every sim to the loose stop, without the energy rescale
+  // 1. integrate every sim to the loose stop, without the energy rescale, and
+  // keep its integrator state there
   ce_run_config loose = *cfg;
   loose.pe_stop_fraction = loose_pe_stop;
   loose.redistribute_energy = 0;
   ce_outputs lo{};
   lo.momenta = c->ps;
-  lo.positions = c->xs;
-  lo.e0 = c->e0;
   lo.pe_final = c->pef;
   lo.status = c->st;
-  lo.steps = c->steps;
+  const ce_sim_state saved{c->xs, c->vel, c->h, c->t, c->steps, c->rej, c->e0, c->comp};
   const int sched = c->e->tuned_schedule;
-  int rc = ce_run_mixed_device(c->e, S, in, coulomb_k, &loose, &lo, sched, stream);
+  int rc = ce::run_mixed_device(c->e, S, in, coulomb_k, &loose, &lo, sched, stream, false, nullptr, &saved);
   if (rc != CE_OK) return cfail(c, rc, std::string("loose run: ") + ce_last_error(c->e));
 
   // 2. features and the ballistic base
@@ -684,14 +695,16 @@ int ce_closure_serve(ce_closure* c, uint64_t S, const ce_mixed_batch* in, double
   rc = ce_closure_apply(S, in, &st, c->steps, c->pbase, c->pscale, c->out, gate, out, c->fb, c->counts, stream);
   if (rc != CE_OK) return cfail(c, rc, "apply launch");
 
-  // 5. plain RK45 from the initial geometry for the marked sims (n = 0 for the rest)
+  // 5. plain RK45 for the marked sims (n = 0 for the rest), continued from the
+  // loose-stop state: bit for bit the result of an uninterrupted plain run. A
+  // sim whose loose run did not finish CE_SIM_OK (saved h = 0) restarts from rest.
   const ce_mixed_batch fbin{c->fb, in->mass_me, in->charge, in->pos};
   ce_outputs fo{};
   fo.momenta = c->fb_m;
   fo.ker = c->fb_ker;
   fo.steps = c->fb_steps;
   fo.status = c->fb_st;
-  rc = ce::run_mixed_device(c->e, S, &fbin, coulomb_k, cfg, &fo, sched, stream, /*skip_empty=*/true);
+  rc = ce::run_mixed_device(c->e, S, &fbin, coulomb_k, cfg, &fo, sched, stream, /*skip_empty=*/true, &saved, nullptr);
   if (rc != CE_OK) return cfail(c, rc, std::string("fallback run: ") + ce_last_error(c->e));
   MergeArgs M{S, c->fb, c->fb_m, c->fb_ker, c->fb_steps, c->fb_st, out->momenta, out->ker, out->steps, out->status};
   closure_merge_kernel<<<grid_for(S, c->e->device), 128, 0, s>>>(M);

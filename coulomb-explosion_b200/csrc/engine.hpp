@@ -119,11 +119,12 @@ inline MixedKernelFn select_mixed_kernel(int n, int mode) {
   }
 }
 
-// ce_run_mixed_device with one extra switch: skip_empty leaves rows with
+// ce_run_mixed_device_state with one extra switch: skip_empty leaves rows with
 // n_atoms == 0 untouched instead of writing CE_SIM_BAD_INPUT outputs (the
-// closure's plain rerun of the sims its gate sent back). Defined in mixed.cu.
+// closure's plain continuation of the sims its gate sent back). Defined in mixed.cu.
 int run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coulomb_k, const ce_run_config* cfg,
-                     const ce_outputs* out, int schedule, void* stream, bool skip_empty);
+                     const ce_outputs* out, int schedule, void* stream, bool skip_empty, const ce_sim_state* resume,
+                     const ce_sim_state* save);
 
 
 // Chunk bounds of the pipelined host-buffer paths: nchunks = 1 below

@@ -111,6 +111,20 @@ __global__ void bucket_scatter_kernel(const uint8_t* __restrict__ n_per, uint64_
         const float* x0 = P.pos + i * (3ull * ce::kMixedStride);
         for (int c = 0; c < 3 * ce::kMixedStride; ++c) xp[c] = bin == 1 ? x0[c] : 0.0f;
       }
+      if (P.save_h) {  // saved state of a sim that needs no integration: restart from rest
+        const float* x0 = P.pos + i * (3ull * ce::kMixedStride);
+        for (int c = 0; c < 3 * ce::kMixedStride; ++c) {
+          P.save_pos[i * (3ull * ce::kMixedStride) + c] = bin == 1 ? x0[c] : 0.0f;
+          P.save_vel[i * (3ull * ce::kMixedStride) + c] = 0.0f;
+        }
+        if (P.save_comp)
+          for (int c = 0; c < 6 * ce::kMixedStride; ++c) P.save_comp[i * (6ull * ce::kMixedStride) + c] = 0.0f;
+        P.save_h[i] = 0.0f;
+        P.save_t[i] = 0.0;
+        P.save_steps[i] = 0u;
+        P.save_rejects[i] = 0u;
+        P.save_e0[i] = 0.0;
+      }
     }
     __syncthreads();
   }
@@ -168,7 +182,13 @@ int ce_reserve_mixed(ce_engine* e, uint64_t S) {
 
 int ce_run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coulomb_k,
                         const ce_run_config* cfg, const ce_outputs* out, int schedule, void* stream) {
-  return ce::run_mixed_device(e, S, in, coulomb_k, cfg, out, schedule, stream, false);
+  return ce::run_mixed_device(e, S, in, coulomb_k, cfg, out, schedule, stream, false, nullptr, nullptr);
+}
+
+int ce_run_mixed_device_state(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coulomb_k,
+                              const ce_run_config* cfg, const ce_sim_state* resume, const ce_sim_state* save,
+                              const ce_outputs* out, int schedule, void* stream) {
+  return ce::run_mixed_device(e, S, in, coulomb_k, cfg, out, schedule, stream, false, resume, save);
 }
 
 }  // extern "C"
@@ -176,13 +196,22 @@ int ce_run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, doub
 namespace ce {
 
 int run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coulomb_k, const ce_run_config* cfg,
-                     const ce_outputs* out, int schedule, void* stream, bool skip_empty) {
+                     const ce_outputs* out, int schedule, void* stream, bool skip_empty, const ce_sim_state* resume,
+                     const ce_sim_state* save) {
   if (!e) return CE_ERR_INVALID;
   e->last_launches = 0;
   int rc = check_mixed_args(e, S, in, coulomb_k, cfg, out);
   if (rc != CE_OK || S == 0) return rc;
+  const bool kahan = (cfg->precision_mode & CE_PREC_KAHAN) != 0;
+  for (const ce_sim_state* st : {resume, save})
+    if (st && (!st->positions || !st->velocities || !st->h || !st->t || !st->steps || !st->rejects || !st->e0 ||
+               (kahan && !st->comp)))
+      return ce::fail(e, CE_ERR_INVALID, "ce_run_mixed_device_state: a state pointer is NULL");
   if (schedule != CE_SCHEDULE_ONE_LAUNCH && schedule != CE_SCHEDULE_PER_SIZE)
     return ce::fail(e, CE_ERR_INVALID, "ce_run_mixed: unknown schedule");
+  // Saving and resuming integrator state is built into the per-size kernels only
+  // (in the one-launch kernel the extra registers cost 6 %).
+  if (resume || save) schedule = CE_SCHEDULE_PER_SIZE;
   cudaError_t st = cudaSetDevice(e->device);
   if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaSetDevice");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -201,6 +230,26 @@ int run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double 
   P.skip_empty = skip_empty ? 1 : 0;
   P.pos = in->pos;
   P.cursor = nullptr;
+  if (save) {
+    P.save_pos = save->positions;
+    P.save_vel = save->velocities;
+    P.save_h = save->h;
+    P.save_t = save->t;
+    P.save_steps = save->steps;
+    P.save_rejects = save->rejects;
+    P.save_e0 = save->e0;
+    P.save_comp = save->comp;
+  }
+  if (resume) {
+    P.res_pos = resume->positions;
+    P.res_vel = resume->velocities;
+    P.res_h = resume->h;
+    P.res_t = resume->t;
+    P.res_steps = resume->steps;
+    P.res_rejects = resume->rejects;
+    P.res_e0 = resume->e0;
+    P.res_comp = resume->comp;
+  }
   P.S = S;
   ce::MixedIn X{in->n_atoms, in->mass_me, in->charge, coulomb_k};
   ce::Buckets B{T.perm, T.off, T.cnt, T.cursor};

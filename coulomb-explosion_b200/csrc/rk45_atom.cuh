@@ -22,7 +22,7 @@
 // The stage loop is unrolled: a lane carries three components, so the six
 // force loops stay small and every coefficient is a compile-time operand.
 //
-// One warp loop (atom_loop<N, MODE, MIXED>) serves three kernels:
+// One warp loop (atom_loop<N, MODE, MIXED, STATE>) serves three kernels:
 //   rk45_atom_kernel<N, MODE>    one fixed molecule (include/ce_gpu.h ce_run*)
 //   rk45_mixed_kernel<MODE>      mixed 2..10-atom molecules, one persistent
 //                                launch walking the size buckets 10 -> 2
@@ -214,7 +214,7 @@ __device__ __forceinline__ void lane_force(const int (&nbr)[N - 1], const int (&
 // FP64 finalize, executed by every lane of the warp (the reductions are full-warp
 // shuffles); lanes with status < 0 compute but write nothing. Each finishing
 // lane writes its atom's momentum, lane i = 0 of the group the per-sim scalars.
-template <int N, int MODE, int STRIDE>
+template <int N, int MODE, int STRIDE, bool STATE>
 __device__ __forceinline__ void atom_finalize(const AtomLane<N, MODE>& s, int status, double pe_final,
                                               const AtomConsts& ac, int ai, int base, const RunParams& P) {
   const double vx = s.v.xy.x, vy = s.v.xy.y, vz = s.v.z;
@@ -245,6 +245,31 @@ __device__ __forceinline__ void atom_finalize(const AtomLane<N, MODE>& s, int st
     xp[2] = s.x.z;
   }
   if (ai == 0 && P.e0) P.e0[s.sim] = static_cast<double>(s.e0);
+  if (STATE && P.save_h) {  // the integrator state this sim stopped in (a resumable run's input)
+    const unsigned long long row = s.sim * (3ull * STRIDE) + 3 * ai;
+    P.save_pos[row] = s.x.xy.x;
+    P.save_pos[row + 1] = s.x.xy.y;
+    P.save_pos[row + 2] = s.x.z;
+    P.save_vel[row] = s.v.xy.x;
+    P.save_vel[row + 1] = s.v.xy.y;
+    P.save_vel[row + 2] = s.v.z;
+    if (AtomLane<N, MODE>::kKahan && P.save_comp) {
+      float* c = P.save_comp + s.sim * (6ull * STRIDE) + 6 * ai;
+      c[0] = s.cx.xy.x;
+      c[1] = s.cx.xy.y;
+      c[2] = s.cx.z;
+      c[3] = s.cv.xy.x;
+      c[4] = s.cv.xy.y;
+      c[5] = s.cv.z;
+    }
+    if (ai == 0) {
+      P.save_h[s.sim] = status == CE_SIM_OK ? s.h : 0.0f;
+      P.save_t[s.sim] = static_cast<double>(s.t);
+      P.save_steps[s.sim] = s.steps;
+      P.save_rejects[s.sim] = s.rejects;
+      P.save_e0[s.sim] = static_cast<double>(s.e0);
+    }
+  }
   if (ai == 0) {
     if (P.ker) P.ker[s.sim] = ker;
     if (P.steps) P.steps[s.sim] = s.steps;
@@ -260,7 +285,7 @@ __device__ __forceinline__ void atom_finalize(const AtomLane<N, MODE>& s, int st
 // drawn from one work queue (cursor over [0, count), mapped through perm when
 // non-null) until the queue is empty and every group has finished. MIXED reads
 // each sim's masses and charges from X; otherwise the fixed molecule M.
-template <int N, int MODE, bool MIXED>
+template <int N, int MODE, bool MIXED, bool STATE>
 __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M, const MixedIn& X,
                                           unsigned long long* cursor, unsigned long long count,
                                           const uint32_t* perm) {
@@ -337,10 +362,21 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
     // ---- init of freshly claimed sims (all lanes take part in the exchange) ----
     if (__ballot_sync(0xffffffffu, fresh) != 0u) {
       int fin_st = -1;
+      bool resumed = false;  // continue from a saved state (res_h > 0) instead of from rest
       if (fresh) {
-        const float* src = P.pos + s.sim * (3ull * STRIDE) + 3 * ai;
+        if (STATE && P.res_h) resumed = __ldg(P.res_h + s.sim) > 0.0f;
+        const unsigned long long row = s.sim * (3ull * STRIDE) + 3 * ai;
+        const float* src = (resumed ? P.res_pos : P.pos) + row;
         s.x = {make_float2(__ldg(src), __ldg(src + 1)), __ldg(src + 2)};
         s.v = s.cx = s.cv = v3_zero();
+        if (resumed) {
+          s.v = {make_float2(__ldg(P.res_vel + row), __ldg(P.res_vel + row + 1)), __ldg(P.res_vel + row + 2)};
+          if (L::kKahan) {
+            const float* c = P.res_comp + s.sim * (6ull * STRIDE) + 6 * ai;
+            s.cx = {make_float2(__ldg(c), __ldg(c + 1)), __ldg(c + 2)};
+            s.cv = {make_float2(__ldg(c + 3), __ldg(c + 4)), __ldg(c + 5)};
+          }
+        }
       }
       if (MIXED) {
         // This sim's constants: pair constants (k q_i) q_j formed in double and
@@ -391,7 +427,27 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
         d2p += r * r;
       }
       const float d2 = __fdividef(sqrt_approx(gsum<N>(d2p, base) * inv_denom), h0);
-      if (fresh) {
+      if (STATE && fresh && resumed) {
+        // The saved state follows an accepted step: k1 = a(x) is bit for bit the
+        // k7 of that step, and the driver's stop test runs again on the current
+        // potential (src/driver.cpp:19-30), as the uninterrupted run would.
+        s.k[0] = a0;
+        s.h = __ldg(P.res_h + s.sim);
+        s.t = static_cast<Acc>(P.res_t[s.sim]);
+        s.steps = P.res_steps[s.sim];
+        s.rejects = P.res_rejects[s.sim];
+        s.rej_in_step = 0u;
+        s.rej_once = false;
+        s.e0 = static_cast<Acc>(P.res_e0[s.sim]);
+        if (L::kF64)
+          s.pe_stop = static_cast<Acc>(P.pe_stop_d * static_cast<double>(s.e0));
+        else
+          s.pe_stop = static_cast<Acc>(P.pe_stop_f * static_cast<float>(s.e0));
+        active = true;
+        if (!(pe0 > s.pe_stop)) fin_st = CE_SIM_OK;
+        else if (s.steps >= P.max_steps) fin_st = CE_SIM_MAX_STEPS;
+        if (fin_st >= 0) active = false;
+      } else if (fresh) {
         s.k[0] = a0;
         const float h1 = (static_cast<double>(d1) <= 1e-15 && static_cast<double>(d2) <= 1e-15)
                              ? fmaxf(1e-6f, h0 * 1e-3f)
@@ -415,7 +471,7 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
         if (fin_st >= 0) active = false;
       }
       if (__ballot_sync(0xffffffffu, fin_st >= 0) != 0u)
-        atom_finalize<N, MODE, STRIDE>(s, fin_st, static_cast<double>(pe0), ac, ai, base, P);
+        atom_finalize<N, MODE, STRIDE, STATE>(s, fin_st, static_cast<double>(pe0), ac, ai, base, P);
     }
     if (__ballot_sync(0xffffffffu, active) == 0u) {
       if (queue_empty) break;
@@ -519,7 +575,7 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
       if (fin_st >= 0) active = false;
     }
     if (__ballot_sync(0xffffffffu, fin_st >= 0) != 0u)
-      atom_finalize<N, MODE, STRIDE>(s, fin_st, static_cast<double>(pe_new), ac, ai, base, P);
+      atom_finalize<N, MODE, STRIDE, STATE>(s, fin_st, static_cast<double>(pe_new), ac, ai, base, P);
   }
 }
 
@@ -528,7 +584,7 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
 template <int N, int MODE>
 __global__ void __launch_bounds__(kAtomMaxBlock) rk45_atom_kernel(const RunParams P, const FixedMol M) {
   const MixedIn none{};
-  atom_loop<N, MODE, false>(P, M, none, P.cursor, P.S, nullptr);
+  atom_loop<N, MODE, false, false>(P, M, none, P.cursor, P.S, nullptr);
 }
 
 // One size bucket of the one-launch mixed kernel, kept out of line so each
@@ -538,7 +594,7 @@ template <int N, int MODE>
 __device__ __noinline__ void mixed_bucket(const RunParams P, const MixedIn X, unsigned long long* cur,
                                           unsigned long long cnt, const uint32_t* perm) {
   const FixedMol none{};
-  atom_loop<N, MODE, true>(P, none, X, cur, cnt, perm);
+  atom_loop<N, MODE, true, false>(P, none, X, cur, cnt, perm);
 }
 
 // Mixed molecules in one persistent launch: every warp walks the size buckets
@@ -571,11 +627,12 @@ __global__ void __launch_bounds__(kAtomMaxBlock, 4) rk45_mixed_kernel(const RunP
   }
 }
 
-// One size bucket of a mixed batch (the per-size launch schedule).
+// One size bucket of a mixed batch (the per-size launch schedule); the only
+// kernel that saves and resumes integrator state (RunParams save_* / res_*).
 template <int N, int MODE>
 __global__ void __launch_bounds__(kAtomMaxBlock) rk45_bucket_kernel(const RunParams P, const MixedIn X, const Buckets B) {
   const FixedMol none{};
-  atom_loop<N, MODE, true>(P, none, X, B.cursor + N, B.cnt[N], B.perm + B.off[N]);
+  atom_loop<N, MODE, true, true>(P, none, X, B.cursor + N, B.cnt[N], B.perm + B.off[N]);
 }
 
 using AtomKernelFn = void (*)(RunParams, FixedMol);

@@ -78,6 +78,27 @@ struct RunParams {
   int32_t redistribute;
   int32_t refill_threshold;
   int32_t skip_empty;  // mixed batches: rows with n_atoms == 0 are left untouched (no outputs written)
+  // Integrator state (lane-per-atom kernels). save_*: written when a sim
+  // finishes, the state it stopped in (save_h = 0 unless it finished
+  // CE_SIM_OK). res_*: when res_h is non-null, a sim whose res_h > 0 starts
+  // from that state (positions res_pos) instead of from rest, and continues
+  // exactly as the run that saved it would have; the others start from rest.
+  float* save_pos;     // [S][stride][3]
+  float* save_vel;     // [S][stride][3] v (not m v)
+  float* save_h;       // [S] next step size
+  double* save_t;      // [S]
+  uint32_t* save_steps;
+  uint32_t* save_rejects;
+  double* save_e0;
+  float* save_comp;    // [S][stride][6] Kahan compensation of x (0..2) and v (3..5)
+  const float* res_pos;
+  const float* res_vel;
+  const float* res_h;
+  const double* res_t;
+  const uint32_t* res_steps;
+  const uint32_t* res_rejects;
+  const double* res_e0;
+  const float* res_comp;
 };
 
 

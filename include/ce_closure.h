@@ -124,9 +124,11 @@ int ce_closure_apply(uint64_t S, const ce_mixed_batch* in, const ce_closure_stat
                      const ce_outputs* out, uint8_t* fallback, unsigned long long* counts, void* stream);
 
 /* Serving pipeline bound to one engine and one network (in_dim 128, out_dim 32):
- * loose run (cfg with pe_stop_fraction = loose_pe_stop and no rescale) ->
- * features -> network -> gate -> plain run (cfg) of the sims sent back ->
- * merge. Device pointers, stream-ordered, no host synchronisation and no
+ * loose run (cfg with pe_stop_fraction = loose_pe_stop and no rescale, keeping
+ * each sim's integrator state, ce_sim_state) -> features -> network -> gate ->
+ * plain RK45 (cfg) for the sims sent back, continued from their loose-stop
+ * state, so their results are bit for bit those of plain RK45 (a sim whose loose
+ * run failed restarts from rest) -> merge. Device pointers, stream-ordered, no host synchronisation and no
  * allocation (scratch for max_sims sims is allocated by ce_closure_create), so
  * a call can be captured in a CUDA graph. out->momenta/ker/steps/status are
  * written (other fields ignored). */

@@ -190,6 +190,33 @@ typedef struct ce_mixed_batch {
 int ce_reserve_mixed(ce_engine* e, uint64_t S);
 int ce_run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coulomb_k,
                         const ce_run_config* cfg, const ce_outputs* out, int schedule, void* stream);
+/* Integrator state of each sim, mixed layout (device pointers). No counterpart
+ * in the reference, whose integrators keep this state in the object between
+ * steps (src/integrators.cpp:63-147). A run given `save` writes, for every sim
+ * it finishes, the state it stopped in: positions, velocities v (not m v), the
+ * next step size h (0 unless the sim finished CE_SIM_OK), time, accepted steps,
+ * rejected attempts, E0, and in the Kahan modes the compensation terms. A run
+ * given `resume` (same precision mode and tolerances, a smaller pe_stop_fraction)
+ * continues every sim whose saved h > 0 from that state, bit for bit as one
+ * uninterrupted run would have; sims with h = 0 start from rest at in->pos. Its
+ * steps / rejects / t outputs count from the start of the first run. Every
+ * pointer is required, `comp` only in the Kahan modes. */
+typedef struct ce_sim_state {
+  float* positions;  /* [S][10][3] */
+  float* velocities; /* [S][10][3] */
+  float* h;          /* [S] */
+  double* t;         /* [S] */
+  uint32_t* steps;   /* [S] */
+  uint32_t* rejects; /* [S] */
+  double* e0;        /* [S] */
+  float* comp;       /* [S][10][6]: x then v compensation (CE_PREC_KAHAN) */
+} ce_sim_state;
+/* ce_run_mixed_device with state: `resume` and `save` may each be NULL (and may
+ * not share buffers). With either, the per-size schedule runs whatever
+ * `schedule` says. */
+int ce_run_mixed_device_state(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double coulomb_k,
+                              const ce_run_config* cfg, const ce_sim_state* resume, const ce_sim_state* save,
+                              const ce_outputs* out, int schedule, void* stream);
 /* Host buffers, synchronous; one-launch schedule unless ce_autotune_mixed found
  * the per-size schedule faster. Up to 8 chunks whose copies overlap the
  * neighbouring chunks' integration when the host buffers are pinned. Whole rows

@@ -225,3 +225,57 @@ def test_autotuner_picks_a_measured_candidate_and_keeps_results(ce, wl):
     # get_tuning reports the resolved shape: refill 0 is CH4's default of 1 in both layouts
     assert (t["block_threads"], t["refill_threshold"], t["lanes_per_sim"]) == (
         best_f["block_threads"], best_f["refill_threshold"] or 1, best_f["lanes_per_sim"])
+
+
+def _state(torch, ce, S):
+    d = dict(x=torch.zeros((S, 10, 3), dtype=torch.float32, device="cuda"),
+             v=torch.zeros((S, 10, 3), dtype=torch.float32, device="cuda"),
+             h=torch.zeros(S, dtype=torch.float32, device="cuda"),
+             t=torch.zeros(S, dtype=torch.float64, device="cuda"),
+             s=torch.zeros(S, dtype=torch.int32, device="cuda"),
+             r=torch.zeros(S, dtype=torch.int32, device="cuda"),
+             e=torch.zeros(S, dtype=torch.float64, device="cuda"),
+             c=torch.zeros((S, 10, 6), dtype=torch.float32, device="cuda"))
+    st = ce.CeSimState(*(d[k].data_ptr() for k in ("x", "v", "h", "t", "s", "r", "e", "c")))
+    return d, st
+
+
+@pytest.mark.parametrize("schedule", ["one", "per_size"])
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
+def test_saved_state_resumes_bit_for_bit(engine, ce, wl, mode, schedule):
+    """A run to a loose stop that saves each sim's integrator state, then a run
+    that continues from it, equals one uninterrupted run bit for bit (momenta,
+    KER, steps, rejects, status); sims whose saved step is 0 restart from rest
+    and equal it too. The closure continues the sims its gate sends back this way."""
+    torch = pytest.importorskip("torch")
+    sch = ce.CE_SCHEDULE_ONE_LAUNCH if schedule == "one" else ce.CE_SCHEDULE_PER_SIZE
+    S = 6000
+    n_per, m, q, pos = wl.sample_mixed(S, seed=61)
+    keep, batch = _device_batch(torch, ce, n_per, m, q, pos)
+    cfg = tight(ce, wl, mode)
+    loose = tight(ce, wl, mode, redistribute_energy=False)
+    loose.pe_stop_fraction = 0.01
+
+    def outputs():
+        d, o = _device_out(torch, ce, S)
+        d["r"] = torch.zeros(S, dtype=torch.int32, device="cuda")
+        d["tf"] = torch.zeros(S, dtype=torch.float64, device="cuda")
+        o.rejects, o.t_final = d["r"].data_ptr(), d["tf"].data_ptr()
+        return d, o
+
+    dp, op = outputs()
+    engine.run_mixed_device(S, batch, cfg, op, sch)
+    dl, ol_ = outputs()
+    ds, st = _state(torch, ce, S)
+    engine.run_mixed_device_state(S, batch, loose, ol_, save=st, schedule=sch)
+    torch.cuda.synchronize()
+    assert (dl["t"].cpu().numpy() == 0).all()
+    h = ds["h"].cpu().numpy()
+    assert (h > 0).all() and (ds["s"].cpu().numpy() > 0).all()
+    ds["h"][::7] = 0.0  # these restart from rest
+    dr, orr = outputs()
+    engine.run_mixed_device_state(S, batch, cfg, orr, resume=st, schedule=sch)
+    torch.cuda.synchronize()
+    for k in ("m", "k", "s", "t", "r", "tf"):
+        np.testing.assert_array_equal(dr[k].cpu().numpy(), dp[k].cpu().numpy(), err_msg=k)
+    assert (dp["t"].cpu().numpy() == 0).all()
