@@ -553,7 +553,7 @@ def run_closure(args):
     g = torch.Generator(device=dev)
     g.manual_seed(seed)
     perm = torch.randperm(S_train, generator=g, device=dev)
-    n_val = max(mb, S_train // 50)
+    n_val = max(mb, int(S_train * args.val_frac))
     val_rows, train_rows = perm[:n_val], perm[n_val:]
     train_rows = train_rows[ts.valid[train_rows]]
 
@@ -653,17 +653,6 @@ def run_closure(args):
     c_lo = ce.CeOutputs(lo_m.data_ptr(), None, lo_s.data_ptr(), lo_st.data_ptr(), None, None, lo_d[1].data_ptr(),
                         None, lo_x.data_ptr(), lo_d[2].data_ptr())
     ms_loose = timed(lambda: eng.run_mixed_device(S, batch_c, lcfg, c_lo, sched, stream.cuda_stream))
-    # the plain rerun of the sims the gate sent back, on those rows alone (the serve
-    # skips the accepted rows; it also sorts all S rows, which stays in "rest")
-    idx = torch.nonzero(fbf).squeeze(1)
-    n_fb = int(idx.numel())
-    ms_fb = 0.0
-    if n_fb:
-        fb = cl.DeviceBatch(fbf[idx].contiguous(), sb.mass[idx].contiguous(), sb.charge[idx].contiguous(),
-                            sb.pos[idx].contiguous())
-        fb_c = fb.c()
-        ms_fb = timed(lambda: eng.run_mixed_device(n_fb, fb_c, cfg, c_lo, sched, stream.cuda_stream))
-        del fb
     del lo_m, lo_x, lo_d, lo_s, lo_st
 
     # network forward alone (tensor-core roofline of the learned part)
@@ -728,8 +717,8 @@ def run_closure(args):
         "plain": {"value": S / (ms_plain / 1e3), "unit": UNIT, "ms_per_step": ms_plain,
                   "mean_steps": float(op["steps"].double().mean())},
         "speedup_vs_plain": ms_plain / ms_clo,
-        "breakdown_ms": {"loose_run": ms_loose, "network_forward": None, "fallback_run": ms_fb,
-                         "rest (features, gate, merge)": None},
+        "breakdown_ms": {"loose_run": ms_loose, "network_forward": None,
+                         "rest (features, gate, continuation of the sims sent back, merge)": None},
         "accepted_frac": acc / max(1, acc + fbk), "fallback_sims": fbk,
         "mean_steps_closure_path": float(steps_c[accepted].mean()) if bool(accepted.any()) else None,
         "gate": {"tol_energy": gate.tol_energy, "tol_momentum": gate.tol_momentum,
@@ -751,7 +740,8 @@ def run_closure(args):
         "clocks": clk.summary(),
     }
     line["breakdown_ms"]["network_forward"] = ms_fwd
-    line["breakdown_ms"]["rest (features, gate, merge)"] = ms_clo - ms_loose - ms_fwd - ms_fb
+    line["breakdown_ms"]["rest (features, gate, continuation of the sims sent back, merge)"] = (
+        ms_clo - ms_loose - ms_fwd)
     print(json.dumps(line))
     clo.close()
     net.close()
@@ -1115,6 +1105,8 @@ def main():
     ap.add_argument("--minibatch", type=int, default=8192, help="closure: rows per training step")
     ap.add_argument("--lr", type=float, default=1e-3, help="closure: peak Adam learning rate")
     ap.add_argument("--gate-quantile", type=float, default=0.99, help="closure: gate bounds quantile")
+    ap.add_argument("--val-frac", type=float, default=0.02,
+                    help="closure: fraction of the training sims held out to validate and calibrate the gate")
     ap.add_argument("--fp64-subset", type=int, default=300, help="closure: sims checked against the FP64 oracle")
     ap.add_argument("--total", type=int, default=100_000_000, help="stream: explosions in the whole stream")
     ap.add_argument("--gate-target-err", type=float, default=0.0,
