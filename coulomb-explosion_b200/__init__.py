@@ -117,6 +117,7 @@ CLOSURE_OUTPUTS = 32
 CE_SIM_BAD_INPUT = 4
 CE_SCHEDULE_ONE_LAUNCH = 0
 CE_SCHEDULE_PER_SIZE = 1
+CE_SCHEDULE_OVERLAP = 2
 MAX_ATOMS = 10
 
 

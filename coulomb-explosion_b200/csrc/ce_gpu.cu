@@ -82,7 +82,7 @@ void ce_destroy(ce_engine* e) {
   if (!e) return;
   cudaSetDevice(e->device);
   if (e->stream) cudaStreamSynchronize(e->stream);
-  for (cudaStream_t x : {e->s_in, e->s_out, e->s_comp2})
+  for (cudaStream_t x : {e->s_in, e->s_out, e->s_comp2, e->s_mix2})
     if (x) {
       cudaStreamSynchronize(x);
       cudaStreamDestroy(x);
@@ -90,6 +90,8 @@ void ce_destroy(ce_engine* e) {
   for (int i = 0; i < 2; ++i)
     for (cudaEvent_t ev : {e->ev_loaded[i], e->ev_computed[i], e->ev_copied[i]})
       if (ev) cudaEventDestroy(ev);
+  for (cudaEvent_t ev : {e->ev_mix_fork, e->ev_mix_join})
+    if (ev) cudaEventDestroy(ev);
   if (e->d_arena) cudaFree(e->d_arena);
   if (e->d_mixed) cudaFree(e->d_mixed);
   if (e->d_cursor) cudaFree(e->d_cursor);

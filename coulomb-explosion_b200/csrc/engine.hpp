@@ -42,6 +42,9 @@ struct ce_engine {
   // Mixed-batch scratch: 4 x 11 u64 bucket tables, then the S-entry permutation.
   void* d_mixed = nullptr;
   size_t mixed_bytes = 0;
+  // CE_SCHEDULE_OVERLAP: a side stream and its fork / join events
+  cudaStream_t s_mix2 = nullptr;
+  cudaEvent_t ev_mix_fork = nullptr, ev_mix_join = nullptr;
   int last_launches = 0;
   std::string err;
 };

@@ -162,15 +162,30 @@ struct ce_graph {
   int device = 0;
 };
 
+namespace {
+// The side stream and events of CE_SCHEDULE_OVERLAP, created once (outside any capture).
+int ensure_overlap_stream(ce_engine* e) {
+  if (e->s_mix2) return CE_OK;
+  cudaError_t st;
+  if ((st = cudaStreamCreateWithFlags(&e->s_mix2, cudaStreamNonBlocking)) != cudaSuccess ||
+      (st = cudaEventCreateWithFlags(&e->ev_mix_fork, cudaEventDisableTiming)) != cudaSuccess ||
+      (st = cudaEventCreateWithFlags(&e->ev_mix_join, cudaEventDisableTiming)) != cudaSuccess)
+    return ce::cuda_fail(e, st, "overlap schedule stream");
+  return CE_OK;
+}
+}  // namespace
+
 extern "C" {
 
 int ce_reserve_mixed(ce_engine* e, uint64_t S) {
   if (!e) return CE_ERR_INVALID;
   if (S >= (1ull << 32)) return ce::fail(e, CE_ERR_INVALID, "ce_reserve_mixed: S must be below 2^32");
-  const size_t need = mixed_scratch_bytes(S);
-  if (need <= e->mixed_bytes) return CE_OK;
   cudaError_t st = cudaSetDevice(e->device);
   if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaSetDevice");
+  int rc = ensure_overlap_stream(e);
+  if (rc != CE_OK) return rc;
+  const size_t need = mixed_scratch_bytes(S);
+  if (need <= e->mixed_bytes) return CE_OK;
   if (e->d_mixed) cudaFree(e->d_mixed);
   e->d_mixed = nullptr;
   e->mixed_bytes = 0;
@@ -207,15 +222,15 @@ int run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double 
     if (st && (!st->positions || !st->velocities || !st->h || !st->t || !st->steps || !st->rejects || !st->e0 ||
                (kahan && !st->comp)))
       return ce::fail(e, CE_ERR_INVALID, "ce_run_mixed_device_state: a state pointer is NULL");
-  if (schedule != CE_SCHEDULE_ONE_LAUNCH && schedule != CE_SCHEDULE_PER_SIZE)
+  if (schedule != CE_SCHEDULE_ONE_LAUNCH && schedule != CE_SCHEDULE_PER_SIZE && schedule != CE_SCHEDULE_OVERLAP)
     return ce::fail(e, CE_ERR_INVALID, "ce_run_mixed: unknown schedule");
   // Saving and resuming integrator state is built into the per-size kernels only
   // (in the one-launch kernel the extra registers cost 6 %).
-  if (resume || save) schedule = CE_SCHEDULE_PER_SIZE;
+  if ((resume || save) && schedule == CE_SCHEDULE_ONE_LAUNCH) schedule = CE_SCHEDULE_PER_SIZE;
   cudaError_t st = cudaSetDevice(e->device);
   if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaSetDevice");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (mixed_scratch_bytes(S) > e->mixed_bytes) {
+  if (mixed_scratch_bytes(S) > e->mixed_bytes || !e->s_mix2) {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (s && cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone)
       return ce::fail(e, CE_ERR_STATE, "ce_run_mixed: scratch too small during graph capture (ce_reserve_mixed first)");
@@ -279,7 +294,18 @@ int run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double 
     fn<<<static_cast<unsigned>(std::max<uint64_t>(grid, 1)), block, 0, s>>>(P, X, B);
     ++launches;
   } else {
+    // Per size, 10 atoms down to 2; with CE_SCHEDULE_OVERLAP the launches
+    // alternate between the call's stream and the engine's side stream (forked
+    // after the sort, joined at the end), so a bucket's blocks take over SMs as
+    // the previous bucket's last blocks retire.
+    const bool overlap = schedule == CE_SCHEDULE_OVERLAP;
+    if (overlap) {
+      if ((st = cudaEventRecord(e->ev_mix_fork, s)) != cudaSuccess ||
+          (st = cudaStreamWaitEvent(e->s_mix2, e->ev_mix_fork, 0)) != cudaSuccess)
+        return ce::cuda_fail(e, st, "overlap schedule fork");
+    }
     for (int n = CE_MAX_ATOMS; n >= 2; --n) {
+      const cudaStream_t sn = (overlap && (n & 1)) ? e->s_mix2 : s;
       const ce::MixedKernelFn fn = ce::select_mixed_kernel(n, cfg->precision_mode);
       int per_sm = t.blocks_per_sm;
       if (per_sm == 0) {
@@ -291,8 +317,13 @@ int run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double 
       const uint64_t grid = std::min<uint64_t>(static_cast<uint64_t>(e->sms) * per_sm, (S + sims_per_block - 1) / sims_per_block);
       ce::RunParams Pn = P;
       if (t.refill_threshold == 0) Pn.refill_threshold = ce::default_refill(n, n);
-      fn<<<static_cast<unsigned>(std::max<uint64_t>(grid, 1)), block, 0, s>>>(Pn, X, B);
+      fn<<<static_cast<unsigned>(std::max<uint64_t>(grid, 1)), block, 0, sn>>>(Pn, X, B);
       ++launches;
+    }
+    if (overlap) {
+      if ((st = cudaEventRecord(e->ev_mix_join, e->s_mix2)) != cudaSuccess ||
+          (st = cudaStreamWaitEvent(s, e->ev_mix_join, 0)) != cudaSuccess)
+        return ce::cuda_fail(e, st, "overlap schedule join");
     }
   }
   st = cudaGetLastError();
@@ -608,7 +639,7 @@ int ce_autotune_mixed(ce_engine* e, uint64_t S, const ce_mixed_batch* dev_in, do
   e->tuned_mixed.valid = false;
   const int blocks[] = {64, 96, ce::kAtomMaxBlock};
   const int refills[] = {0, 1, 2, 4};  // 0: each size's default
-  const int schedules[] = {CE_SCHEDULE_ONE_LAUNCH, CE_SCHEDULE_PER_SIZE};
+  const int schedules[] = {CE_SCHEDULE_ONE_LAUNCH, CE_SCHEDULE_PER_SIZE, CE_SCHEDULE_OVERLAP};
   double best = -1.0;
   ce_tuning best_t{};
   int best_s = CE_SCHEDULE_ONE_LAUNCH;

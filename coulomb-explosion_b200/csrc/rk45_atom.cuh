@@ -288,7 +288,7 @@ __device__ __forceinline__ void atom_finalize(const AtomLane<N, MODE>& s, int st
 template <int N, int MODE, bool MIXED, bool STATE>
 __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M, const MixedIn& X,
                                           unsigned long long* cursor, unsigned long long count,
-                                          const uint32_t* perm) {
+                                          const uint32_t* perm, int refill) {
   using L = AtomLane<N, MODE>;
   using Acc = typename L::Acc;
   constexpr int G = AtomShape<N>::G;
@@ -344,7 +344,7 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
     bool fresh = false;
     const unsigned idle = __ballot_sync(0xffffffffu, leader && !active);
     if (!queue_empty && idle != 0u &&
-        (__popc(idle) >= P.refill_threshold || __ballot_sync(0xffffffffu, active) == 0u)) {
+        (__popc(idle) >= refill || __ballot_sync(0xffffffffu, active) == 0u)) {
       const int cnt = __popc(idle);
       const int first = __ffs(idle) - 1;
       unsigned long long b0 = 0ull;
@@ -584,17 +584,17 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
 template <int N, int MODE>
 __global__ void __launch_bounds__(kAtomMaxBlock) rk45_atom_kernel(const RunParams P, const FixedMol M) {
   const MixedIn none{};
-  atom_loop<N, MODE, false, false>(P, M, none, P.cursor, P.S, nullptr);
+  atom_loop<N, MODE, false, false>(P, M, none, P.cursor, P.S, nullptr, P.refill_threshold);
 }
 
 // One size bucket of the one-launch mixed kernel, kept out of line so each
 // size gets its own register allocation (inlined into one function, the nine
 // loops together needed ~230 registers; apart, the largest needs 128).
 template <int N, int MODE>
-__device__ __noinline__ void mixed_bucket(const RunParams P, const MixedIn X, unsigned long long* cur,
+__device__ __noinline__ void mixed_bucket(const RunParams& P, int refill, const MixedIn X, unsigned long long* cur,
                                           unsigned long long cnt, const uint32_t* perm) {
   const FixedMol none{};
-  atom_loop<N, MODE, true, false>(P, none, X, cur, cnt, perm);
+  atom_loop<N, MODE, true, false>(P, none, X, cur, cnt, perm, refill);
 }
 
 // Mixed molecules in one persistent launch: every warp walks the size buckets
@@ -604,25 +604,26 @@ __device__ __noinline__ void mixed_bucket(const RunParams P, const MixedIn X, un
 // blocks per SM are asked for: left free, the nine out-of-line bucket loops
 // take 166 registers and only three blocks fit.
 template <int MODE>
-__global__ void __launch_bounds__(kAtomMaxBlock, 4) rk45_mixed_kernel(const RunParams P, const MixedIn X, const Buckets B) {
+__global__ void __launch_bounds__(kAtomMaxBlock, 4)
+    rk45_mixed_kernel(const __grid_constant__ RunParams P, const MixedIn X, const Buckets B) {
 #pragma unroll 1
   for (int n = CE_MAX_ATOMS; n >= 2; --n) {
     const unsigned long long cnt = B.cnt[n];
     if (cnt == 0ull) continue;
     const uint32_t* perm = B.perm + B.off[n];
     unsigned long long* cur = B.cursor + n;
-    RunParams Pn = P;
-    if (Pn.refill_threshold == 0) Pn.refill_threshold = default_refill(n, n);
+    // the parameters by reference (no per-bucket copy of the kernel arguments)
+    const int refill = P.refill_threshold == 0 ? default_refill(n, n) : P.refill_threshold;
     switch (n) {
-      case 10: mixed_bucket<10, MODE>(Pn, X, cur, cnt, perm); break;
-      case 9: mixed_bucket<9, MODE>(Pn, X, cur, cnt, perm); break;
-      case 8: mixed_bucket<8, MODE>(Pn, X, cur, cnt, perm); break;
-      case 7: mixed_bucket<7, MODE>(Pn, X, cur, cnt, perm); break;
-      case 6: mixed_bucket<6, MODE>(Pn, X, cur, cnt, perm); break;
-      case 5: mixed_bucket<5, MODE>(Pn, X, cur, cnt, perm); break;
-      case 4: mixed_bucket<4, MODE>(Pn, X, cur, cnt, perm); break;
-      case 3: mixed_bucket<3, MODE>(Pn, X, cur, cnt, perm); break;
-      default: mixed_bucket<2, MODE>(Pn, X, cur, cnt, perm); break;
+      case 10: mixed_bucket<10, MODE>(P, refill, X, cur, cnt, perm); break;
+      case 9: mixed_bucket<9, MODE>(P, refill, X, cur, cnt, perm); break;
+      case 8: mixed_bucket<8, MODE>(P, refill, X, cur, cnt, perm); break;
+      case 7: mixed_bucket<7, MODE>(P, refill, X, cur, cnt, perm); break;
+      case 6: mixed_bucket<6, MODE>(P, refill, X, cur, cnt, perm); break;
+      case 5: mixed_bucket<5, MODE>(P, refill, X, cur, cnt, perm); break;
+      case 4: mixed_bucket<4, MODE>(P, refill, X, cur, cnt, perm); break;
+      case 3: mixed_bucket<3, MODE>(P, refill, X, cur, cnt, perm); break;
+      default: mixed_bucket<2, MODE>(P, refill, X, cur, cnt, perm); break;
     }
   }
 }
@@ -632,7 +633,7 @@ __global__ void __launch_bounds__(kAtomMaxBlock, 4) rk45_mixed_kernel(const RunP
 template <int N, int MODE>
 __global__ void __launch_bounds__(kAtomMaxBlock) rk45_bucket_kernel(const RunParams P, const MixedIn X, const Buckets B) {
   const FixedMol none{};
-  atom_loop<N, MODE, true, true>(P, none, X, B.cursor + N, B.cnt[N], B.perm + B.off[N]);
+  atom_loop<N, MODE, true, true>(P, none, X, B.cursor + N, B.cnt[N], B.perm + B.off[N], P.refill_threshold);
 }
 
 using AtomKernelFn = void (*)(RunParams, FixedMol);

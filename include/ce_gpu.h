@@ -183,6 +183,10 @@ typedef struct ce_mixed_batch {
 
 #define CE_SCHEDULE_ONE_LAUNCH 0 /* one persistent launch walks the size buckets 10 -> 2 */
 #define CE_SCHEDULE_PER_SIZE 1   /* one launch per size bucket, in sequence            */
+#define CE_SCHEDULE_OVERLAP 2    /* the per-size launches alternating between the call's *
+                                  * stream and an engine side stream, so each bucket's   *
+                                  * last simulations overlap the next bucket's start;    *
+                                  * results equal the other schedules' bit for bit       */
 
 /* Size the engine's mixed-batch scratch (bucket tables + a 4-byte-per-sim
  * permutation) for up to S sims, so later calls, and graph captures, allocate

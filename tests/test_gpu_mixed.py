@@ -169,13 +169,28 @@ def test_schedules_and_graph_replay_are_bit_identical(engine, ce, wl):
     cfg = tight(ce, wl)
     stream = torch.cuda.Stream()
     outs = []
-    for sched in (ce.CE_SCHEDULE_ONE_LAUNCH, ce.CE_SCHEDULE_PER_SIZE):
+    for sched in (ce.CE_SCHEDULE_ONE_LAUNCH, ce.CE_SCHEDULE_PER_SIZE, ce.CE_SCHEDULE_OVERLAP):
         d, o = _device_out(torch, ce, S)
         engine.run_mixed_device(S, batch, cfg, o, sched, stream.cuda_stream)
         stream.synchronize()
         outs.append({k: v.cpu().numpy() for k, v in d.items()})
-    for k in outs[0]:
-        np.testing.assert_array_equal(outs[0][k], outs[1][k])
+    for other in outs[1:]:
+        for k in outs[0]:
+            np.testing.assert_array_equal(outs[0][k], other[k])
+    # the overlapped per-size schedule (two streams, fork / join) captured and replayed
+    engine.reserve_mixed(S)
+    d, o = _device_out(torch, ce, S)
+    engine.graph_begin(stream.cuda_stream)
+    engine.run_mixed_device(S, batch, cfg, o, ce.CE_SCHEDULE_OVERLAP, stream.cuda_stream)
+    g = engine.graph_end(stream.cuda_stream)
+    try:
+        d["m"].zero_()
+        torch.cuda.synchronize()
+        g.launch(stream.cuda_stream)
+        stream.synchronize()
+        np.testing.assert_array_equal(d["m"].cpu().numpy(), outs[0]["m"])
+    finally:
+        g.close()
     # capture the one-launch call into a graph and replay it twice
     engine.reserve_mixed(S)
     d, o = _device_out(torch, ce, S)
@@ -206,9 +221,9 @@ def test_autotuner_picks_a_measured_candidate_and_keeps_results(ce, wl):
     engine.run_mixed_device(S, batch, cfg, o0, ce.CE_SCHEDULE_ONE_LAUNCH, stream.cuda_stream)
     stream.synchronize()
     report, best = engine.autotune_mixed(S, batch, cfg)
-    # 2 schedules x 3 block sizes x 4 refill thresholds (0 = each size's default)
-    assert len(report) == 24 and all(r["sims_per_s"] > 0 for r in report)
-    assert best in (ce.CE_SCHEDULE_ONE_LAUNCH, ce.CE_SCHEDULE_PER_SIZE)
+    # 3 schedules x 3 block sizes x 4 refill thresholds (0 = each size's default)
+    assert len(report) == 36 and all(r["sims_per_s"] > 0 for r in report)
+    assert best in (ce.CE_SCHEDULE_ONE_LAUNCH, ce.CE_SCHEDULE_PER_SIZE, ce.CE_SCHEDULE_OVERLAP)
     d1, o1 = _device_out(torch, ce, S)
     engine.run_mixed_device(S, batch, cfg, o1, best, stream.cuda_stream)
     stream.synchronize()
@@ -240,7 +255,7 @@ def _state(torch, ce, S):
     return d, st
 
 
-@pytest.mark.parametrize("schedule", ["one", "per_size"])
+@pytest.mark.parametrize("schedule", ["one", "per_size", "overlap"])
 @pytest.mark.parametrize("mode", [0, 1, 2, 3])
 def test_saved_state_resumes_bit_for_bit(engine, ce, wl, mode, schedule):
     """A run to a loose stop that saves each sim's integrator state, then a run
@@ -248,7 +263,8 @@ def test_saved_state_resumes_bit_for_bit(engine, ce, wl, mode, schedule):
     KER, steps, rejects, status); sims whose saved step is 0 restart from rest
     and equal it too. The closure continues the sims its gate sends back this way."""
     torch = pytest.importorskip("torch")
-    sch = ce.CE_SCHEDULE_ONE_LAUNCH if schedule == "one" else ce.CE_SCHEDULE_PER_SIZE
+    sch = {"one": ce.CE_SCHEDULE_ONE_LAUNCH, "per_size": ce.CE_SCHEDULE_PER_SIZE,
+           "overlap": ce.CE_SCHEDULE_OVERLAP}[schedule]
     S = 6000
     n_per, m, q, pos = wl.sample_mixed(S, seed=61)
     keep, batch = _device_batch(torch, ce, n_per, m, q, pos)
