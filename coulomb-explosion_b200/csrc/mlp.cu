@@ -416,6 +416,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) mlp_forward_fused_kernel(const
   uint64_t* act_ready = bars + 8;     // [2] tile's layer input written (256 arrivals)
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 10);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 11);
+  uint64_t* drain = bars + 12;        // completion of every MMA this CTA issued
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int ntiles = A.rows / kTM;
   const int npairs = (ntiles + 1) / 2;
@@ -428,6 +429,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) mlp_forward_fused_kernel(const
       umma::mbar_init(&acc_full[t], 1);
       umma::mbar_init(&act_ready[t], kFwdGroups * kTM);  // the tile's epilogue threads
     }
+    umma::mbar_init(drain, 1);
     *abort_flag = 0;
   }
   if (warp == 1) umma::tmem_alloc(tslot, kFwdTmemCols);
@@ -462,6 +464,11 @@ __global__ void __launch_bounds__(kFwdThreads, 1) mlp_forward_fused_kernel(const
             }
         }
       }
+      // Drain (matters after an abort): the last copies issued into each slot
+      // must have landed before the CTA's shared memory is released. In a normal
+      // run their phases are already complete and these waits return at once.
+      for (uint32_t j = k > static_cast<uint32_t>(kFwdSlots) ? k - kFwdSlots : 0u; j < k; ++j)
+        umma::mbar_wait(&full[j % kFwdSlots], (j / kFwdSlots) & 1u, A.err, 3);
     }
   } else if (warp == 1) {
     // ---- MMA issuer ----
@@ -495,6 +502,10 @@ __global__ void __launch_bounds__(kFwdThreads, 1) mlp_forward_fused_kernel(const
           }
         }
       }
+      // Drain (matters after an abort): every MMA issued must have finished
+      // writing TMEM before it is freed. In a normal run they all have.
+      umma::mma_commit(drain);
+      umma::mbar_wait(drain, 0u, A.err, 3);
     }
   } else {
     // ---- epilogue: 12 warps a tile; each warp one lane quarter (warp % 4, the
