@@ -221,6 +221,23 @@ struct ThreadSim {
   unsigned long long sim;
 };
 
+// Stores K contiguous floats (K compile-time) with float2 stores: an 8-byte
+// aligned start writes pairs (and a trailing single when K is odd), a start 4
+// bytes past alignment writes one single first.
+template <int K>
+__device__ __forceinline__ void store_record(float* dst, const float (&v)[K]) {
+  if ((reinterpret_cast<uintptr_t>(dst) & 7u) == 0u) {
+#pragma unroll
+    for (int f = 0; f + 1 < K; f += 2) *reinterpret_cast<float2*>(dst + f) = make_float2(v[f], v[f + 1]);
+    if (K & 1) dst[K - 1] = v[K - 1];
+  } else {
+    dst[0] = v[0];
+#pragma unroll
+    for (int f = 1; f + 1 < K; f += 2) *reinterpret_cast<float2*>(dst + f) = make_float2(v[f], v[f + 1]);
+    if (!(K & 1)) dst[K - 1] = v[K - 1];
+  }
+}
+
 // FP64 finalize: KE, s = sqrt(E0/KE), p_i = (m_i s) v_i, KER = s^2 KE; then the
 // per-sim output record. A converged sim with non-finite momenta is
 // CE_SIM_NONFINITE.
@@ -240,14 +257,17 @@ __device__ __forceinline__ void thread_finalize(const ThreadSim<N, MODE>& s, int
   const double e0d = static_cast<double>(s.e0);
   const double sc =
       (P.redistribute && ke > 0.0) ? (e0d > 0.0 ? e0d * rsqrt(e0d * ke) : sqrt(e0d / ke)) : 1.0;
-  float* dst = P.momenta + s.sim * (3ull * N);
+  // The sim's 3N momenta, written as one contiguous record with 8-byte stores
+  // (a record starts 8-byte aligned or 4 bytes past it, depending on the sim).
+  float pm[3 * N];
 #pragma unroll
   for (int i = 0; i < N; ++i) {
     const double mm = M.mass[i] * sc;
-    dst[i * 3 + 0] = static_cast<float>(mm * static_cast<double>(s.v[i].x));
-    dst[i * 3 + 1] = static_cast<float>(mm * static_cast<double>(s.v[i].y));
-    dst[i * 3 + 2] = static_cast<float>(mm * static_cast<double>(flc<NP>(s.v, 2 * N + i)));
+    pm[i * 3 + 0] = static_cast<float>(mm * static_cast<double>(s.v[i].x));
+    pm[i * 3 + 1] = static_cast<float>(mm * static_cast<double>(s.v[i].y));
+    pm[i * 3 + 2] = static_cast<float>(mm * static_cast<double>(flc<NP>(s.v, 2 * N + i)));
   }
+  store_record<3 * N>(P.momenta + s.sim * (3ull * N), pm);
   if (P.ker) P.ker[s.sim] = (sc * sc) * ke;
   if (P.steps) P.steps[s.sim] = s.steps;
   if (P.status) P.status[s.sim] = static_cast<uint8_t>(status);
