@@ -192,7 +192,9 @@ __device__ __forceinline__ void thread_forces(const float2 (&x)[ThreadShape<N>::
   }
 #pragma unroll
   for (int i = 0; i < N; ++i) {
-    a[i] = __fmul2_rn(axy[i], bcast(M.inv_m[i]));
+    // scalar products with the constant-bank 1/m_i (a packed product would first
+    // copy it into a register pair)
+    a[i] = make_float2(axy[i].x * M.inv_m[i], axy[i].y * M.inv_m[i]);
     fl_set<NP>(a, 2 * N + i, az[i] * M.inv_m[i]);
   }
 #pragma unroll
@@ -389,32 +391,32 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE>& s, const RunP
     Acc no_pe = Acc(0);
 #pragma unroll 1
     for (int si = 1; si <= 5; ++si) {
+      // x + (c_s h) v first, then each stage's h^2 abar_sl k_l added on
+      // (stage 2 has no k term)
       const float chh = c_c[si + 1] * hh;
-      float2 sum[NP];
-      {
-        const float a1 = c_abar[si + 1][1];
+#pragma unroll
+      for (int p = 0; p < NP; ++p) xs[p] = __ffma2_rn(bcast(chh), s.v[p], s.x[p]);
+      if (si > 1) {
+        const float a1 = c_abar[si + 1][1] * hh2;
         const float4* k1 = ks + s.k1s * NC * B;
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
           const float4 q = k1[c * B];
-          sum[2 * c] = __fmul2_rn(bcast(a1), make_float2(q.x, q.y));
-          sum[2 * c + 1] = __fmul2_rn(bcast(a1), make_float2(q.z, q.w));
+          xs[2 * c] = __ffma2_rn(bcast(a1), make_float2(q.x, q.y), xs[2 * c]);
+          xs[2 * c + 1] = __ffma2_rn(bcast(a1), make_float2(q.z, q.w), xs[2 * c + 1]);
         }
       }
 #pragma unroll 1
       for (int l = 1; l + 1 < si; ++l) {
-        const float al = c_abar[si + 1][l + 1];
+        const float al = c_abar[si + 1][l + 1] * hh2;
         const float4* kl = ks + (l - 1) * NC * B;
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
           const float4 q = kl[c * B];
-          sum[2 * c] = __ffma2_rn(bcast(al), make_float2(q.x, q.y), sum[2 * c]);
-          sum[2 * c + 1] = __ffma2_rn(bcast(al), make_float2(q.z, q.w), sum[2 * c + 1]);
+          xs[2 * c] = __ffma2_rn(bcast(al), make_float2(q.x, q.y), xs[2 * c]);
+          xs[2 * c + 1] = __ffma2_rn(bcast(al), make_float2(q.z, q.w), xs[2 * c + 1]);
         }
       }
-#pragma unroll
-      for (int p = 0; p < NP; ++p)
-        xs[p] = __ffma2_rn(bcast(hh2), sum[p], __ffma2_rn(bcast(chh), s.v[p], s.x[p]));
       thread_forces<N, Acc>(xs, a, M, false, no_pe);
       float4* out = ks + (si - 1) * NC * B;
 #pragma unroll
