@@ -197,7 +197,7 @@ int fixed_shape(ce_engine* e, int mode, FixedShape* sh) {
                             : static_cast<uint64_t>(sh->block);
   sh->refill = t.refill_threshold;
   // The thread-per-sim kernel keeps its stage accelerations in dynamic shared memory.
-  sh->smem = atom ? 0 : ce::thread_smem_bytes(e->n, sh->block);
+  sh->smem = atom ? 0 : ce::thread_smem_bytes(e->n, sh->block, mode);
   if (sh->smem > 0) {
     st = cudaFuncSetAttribute(reinterpret_cast<const void*>(sh->fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
                               static_cast<int>(sh->smem));

@@ -138,7 +138,7 @@ extern "C" int ce_run_device_noalloc(int n, const double* mass_me, const double*
   const int lanes = ce::default_lanes(n, cfg->precision_mode);
   // The thread-per-sim kernel takes its stage slots as dynamic shared memory
   // (on-chip, per block; not an allocation).
-  const size_t smem = lanes >= 2 ? 0 : ce::thread_smem_bytes(n, block);
+  const size_t smem = lanes >= 2 ? 0 : ce::thread_smem_bytes(n, block, cfg->precision_mode);
   if (smem > 0 &&
       (cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
                             static_cast<int>(smem)) != cudaSuccess ||

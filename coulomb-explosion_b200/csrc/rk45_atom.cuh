@@ -57,15 +57,17 @@ __host__ __device__ constexpr int default_refill(int n, int lanes_per_sim) {
 }
 
 // Default layout of a fixed-molecule run (ce_tuning::lanes_per_sim): one thread
-// per sim for up to kThreadMaxAtoms atoms in the precision modes without Kahan
-// compensation, else one lane per atom. Measured on CH4 at the tight point:
-// 2.60e8 against 2.15e8 explosions/s (plain FP32); stiff H2O 5.05e8 against
-// 4.66e8; at 10 atoms the seven stage slots allow one 128-thread block per SM
-// and the lane layout wins (6.3e7 against 4.4e7); with the compensation terms
-// the thread layout spills (CH4, full precision form: 1.57e8 against 2.00e8).
+// per sim for up to kThreadMaxAtoms atoms, and with Kahan compensation (whose
+// terms take four more stage slots, so fewer blocks fit) from 4 atoms up;
+// otherwise one lane per atom. Measured at the tight point, 1e6 sims: CH4 plain
+// FP32 2.78e8 against 2.15e8 explosions/s, full precision form (Kahan + FP64
+// t/E) 2.13e8 against 2.02e8; stiff H2O plain 5.22e8 against 4.66e8, full
+// precision 4.24e8 against 4.32e8 (lane wins); at 10 atoms the seven stage
+// slots allow one 128-thread block per SM and the lane layout wins (6.3e7
+// against 4.4e7).
 constexpr int kThreadMaxAtoms = 6;
 __host__ __device__ constexpr int default_lanes(int n, int mode) {
-  return n < 2 ? 1 : (((mode & CE_PREC_KAHAN) == 0 && n <= kThreadMaxAtoms) ? 1 : n);
+  return n < 2 ? 1 : ((n <= kThreadMaxAtoms && ((mode & CE_PREC_KAHAN) == 0 || n >= 4)) ? 1 : n);
 }
 
 template <int N>

@@ -133,12 +133,23 @@ struct ThreadShape {
   static constexpr int kMinBlocks = N <= 5 ? 4 : (N <= 7 ? 3 : 2);
 };
 
+// Stage slots per thread: k2..k6 and k1 / k7 (7); with Kahan compensation also
+// cx and cv, each alternating between two slots like k1 / k7 (11).
+__host__ __device__ constexpr int thread_slots(int mode) { return (mode & CE_PREC_KAHAN) ? 11 : 7; }
+// Blocks per SM the register allocator aims for; with the Kahan slots the
+// shared memory allows fewer blocks, so more registers a thread.
+template <int N, int MODE>
+__host__ __device__ constexpr int thread_min_blocks() {
+  return (MODE & CE_PREC_KAHAN) ? (N <= 4 ? 3 : 2) : ThreadShape<N>::kMinBlocks;
+}
+
 constexpr int kThreadMaxBlock = 128;
 
-// Dynamic shared memory of one thread-per-sim block: seven stage slots of NC
-// 16-byte chunks for each of its threads.
-__host__ __device__ constexpr size_t thread_smem_bytes(int n, int block) {
-  return static_cast<size_t>(7) * static_cast<size_t>((3 * n + 3) / 4) * 16u * static_cast<size_t>(block);
+// Dynamic shared memory of one thread-per-sim block: thread_slots(mode) stage
+// slots of NC 16-byte chunks for each of its threads.
+__host__ __device__ constexpr size_t thread_smem_bytes(int n, int block, int mode) {
+  return static_cast<size_t>(thread_slots(mode)) * static_cast<size_t>((3 * n + 3) / 4) * 16u *
+         static_cast<size_t>(block);
 }
 
 // Flat float f of a register 3N-vector (x_i at 2i, y_i at 2i + 1, z_i at 2N + i);
@@ -206,14 +217,13 @@ struct ThreadSim {
   static constexpr bool kKahan = (MODE & CE_PREC_KAHAN) != 0;
   static constexpr bool kF64 = (MODE & CE_PREC_FP64) != 0;
   static constexpr int NP = ThreadShape<N>::NP;
-  static constexpr int KP = kKahan ? NP : 1;
+
   using Acc = typename std::conditional<kF64, double, float>::type;
 
   float2 x[NP];
   float2 v[NP];
   int k1s;        // stage slot holding k1 = a(x) (FSAL): 5 or 6; k7 goes to the other
-  float2 cx[KP];  // Kahan compensation of the committed x / v updates
-  float2 cv[KP];
+  int cxs, cvs;   // stage slots holding the Kahan compensation of x (7 or 8) and v (9 or 10)
   float h;
   Acc t;
   Acc e0;
@@ -310,7 +320,15 @@ __device__ __forceinline__ bool thread_init(ThreadSim<N, MODE>& s, unsigned long
     fl_set<NP>(s.x, 2 * N + i, __ldg(src + 3 * i + 2));
   }
 #pragma unroll
-  for (int p = 0; p < S::KP; ++p) s.cx[p] = s.cv[p] = make_float2(0.0f, 0.0f);
+  if (S::kKahan) {  // compensation terms start at zero
+    s.cxs = 7;
+    s.cvs = 9;
+#pragma unroll
+    for (int c = 0; c < ThreadShape<N>::NC; ++c) {
+      ks[(7 * ThreadShape<N>::NC + c) * B] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      ks[(9 * ThreadShape<N>::NC + c) * B] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+  }
   Acc pe0 = Acc(0);
   float2 k0[NP];
   thread_forces<N, Acc>(s.x, k0, M, true, pe0);
@@ -427,7 +445,6 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE>& s, const RunP
 
   // Stage 7 (row = 5th-order weights, c_7 = 1): x_new, and FSAL k7 with the
   // potential energy of x_new for the stop test.
-  float2 cxn[S::KP];
   Acc pe_new = Acc(0);
   {
 #pragma unroll
@@ -440,11 +457,13 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE>& s, const RunP
         const float4 q = ks[((l - 1) * NC + (p >> 1)) * B];
         sum = __ffma2_rn(bcast(c_abar[7][l + 1]), (p & 1) ? make_float2(q.z, q.w) : make_float2(q.x, q.y), sum);
       }
-      if (S::kKahan) {
+      if (S::kKahan) {  // compensated update; the new compensation goes to the other cx slot
         const float2 inc = __ffma2_rn(bcast(hh2), sum, __fmul2_rn(bcast(hh), s.v[p]));
-        const float2 y = __ffma2_rn(bcast(-1.0f), s.cx[p < S::KP ? p : 0], inc);
+        const float4 qc = ks[(s.cxs * NC + (p >> 1)) * B];
+        const float2 y = __ffma2_rn(bcast(-1.0f), (p & 1) ? make_float2(qc.z, qc.w) : make_float2(qc.x, qc.y), inc);
         xs[p] = __fadd2_rn(s.x[p], y);
-        cxn[p < S::KP ? p : 0] = __ffma2_rn(bcast(-1.0f), y, __ffma2_rn(bcast(-1.0f), s.x[p], xs[p]));
+        const float2 cn = __ffma2_rn(bcast(-1.0f), y, __ffma2_rn(bcast(-1.0f), s.x[p], xs[p]));
+        reinterpret_cast<float2*>(ks + ((15 - s.cxs) * NC + (p >> 1)) * B)[p & 1] = cn;
       } else {
         xs[p] = __ffma2_rn(bcast(hh2), sum, __ffma2_rn(bcast(hh), s.v[p], s.x[p]));  // c_7 = 1
       }
@@ -459,7 +478,6 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE>& s, const RunP
   // slots 0..4 hold k2..k6, slot 5 k7): v_new = v + h sum b_l k_l, position
   // error h^2 sum ebar_l k_l, velocity error h sum E_l k_l (b_2 = E_2 = 0).
   float2 vn[NP];
-  float2 cvn[S::KP];
   float2 err2 = make_float2(0.0f, 0.0f);
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
@@ -483,10 +501,12 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE>& s, const RunP
         if (l != 1) sev = __ffma2_rn(bcast(c_e[l + 1]), kl, sev);
       }
       const float2 incv = __fmul2_rn(bcast(hh), sv);
-      if (S::kKahan) {
-        const float2 y = __ffma2_rn(bcast(-1.0f), s.cv[p < S::KP ? p : 0], incv);
+      if (S::kKahan) {  // compensated update; the new compensation goes to the other cv slot
+        const float4 qc = ks[(s.cvs * NC + c) * B];
+        const float2 y = __ffma2_rn(bcast(-1.0f), hp == 0 ? make_float2(qc.x, qc.y) : make_float2(qc.z, qc.w), incv);
         vn[p] = __fadd2_rn(s.v[p], y);
-        cvn[p < S::KP ? p : 0] = __ffma2_rn(bcast(-1.0f), y, __ffma2_rn(bcast(-1.0f), s.v[p], vn[p]));
+        const float2 cn = __ffma2_rn(bcast(-1.0f), y, __ffma2_rn(bcast(-1.0f), s.v[p], vn[p]));
+        reinterpret_cast<float2*>(ks + ((19 - s.cvs) * NC + c) * B)[hp] = cn;
       } else {
         vn[p] = __fadd2_rn(s.v[p], incv);
       }
@@ -524,12 +544,9 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE>& s, const RunP
       s.v[p] = vn[p];
     }
     s.k1s = 11 - s.k1s;  // k7 becomes k1 (FSAL)
-    if (S::kKahan) {
-#pragma unroll
-      for (int p = 0; p < S::KP; ++p) {
-        s.cx[p] = cxn[p];
-        s.cv[p] = cvn[p];
-      }
+    if (S::kKahan) {  // the new compensation terms become current
+      s.cxs = 15 - s.cxs;
+      s.cvs = 19 - s.cvs;
     }
     float factor = (en2 == 0.0f) ? kMaxFactor : fminf(kMaxFactor, kSafety * __powf(en2, 0.5f * kExponent));
     if (s.rej_once) factor = fminf(factor, 1.0f);
@@ -565,7 +582,7 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE>& s, const RunP
 // kThreadMaxBlock threads per block and thread_smem_bytes(N, kThreadMaxBlock)
 // bytes of dynamic shared memory.
 template <int N, int MODE>
-__global__ void __launch_bounds__(kThreadMaxBlock, ThreadShape<N>::kMinBlocks)
+__global__ void __launch_bounds__(kThreadMaxBlock, (thread_min_blocks<N, MODE>()))
     rk45_fixed_kernel(const RunParams P, const FixedMol M) {
   extern __shared__ float4 ce_stage_slots[];
   ThreadSim<N, MODE> s;

@@ -133,7 +133,7 @@ int ce_set_molecule(ce_engine* e, int n, const double* mass_me, const double* ch
 int ce_set_tuning(ce_engine* e, const ce_tuning* t);
 /* The launch shape a plain-FP32 run of the current molecule uses (explicit
  * fields, else the autotuned entry, else the defaults: one thread per sim up to
- * 6 atoms without Kahan compensation, else one lane per atom). */
+ * 6 atoms (4 to 6 with Kahan compensation), else one lane per atom). */
 int ce_get_tuning(const ce_engine* e, ce_tuning* t);
 
 /* Integrate S explosions of the fixed molecule from rest.
