@@ -275,7 +275,7 @@ int ce_run_device(ce_engine* e, uint64_t S, const float* pos, const ce_run_confi
 // integrate on two compute streams with a work-queue cursor each, so a chunk's
 // persistent blocks take over SMs as the previous chunk's blocks retire instead
 // of waiting for its last simulation.
-constexpr uint64_t kResidentPerChunk = 2;
+constexpr uint64_t kResidentQuartersPerChunk = 8;  // 2x the resident sims
 
 int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
            const ce_outputs* out) {
@@ -292,17 +292,18 @@ int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
   rc = ce::ensure_pipeline(e);
   if (rc != CE_OK) return rc;
 
-  // Chunking: up to 16 chunks, each at least kResidentPerChunk times the sims the
-  // persistent grid holds at once (and 2^16), so a chunk's last simulations are
-  // a small part of its run. One chunk below twice that. Measured on CH4 1e6
-  // with the thread-per-sim kernel (75,776 sims resident), end to end: 1x the
-  // resident count 2.29e8/s, 2x 2.47e8, 3x 2.25e8, 4x 2.19e8 (device-resident
-  // 2.74e8); with a fixed 2^16 minimum 2.24e8.
+  // Chunking: up to 16 chunks, each at least kResidentQuartersPerChunk / 4
+  // times the sims the persistent grid holds at once (and 2^16), so a chunk's
+  // last simulations are a small part of its run. One chunk below twice that.
+  // Measured on CH4 1e6 with the thread-per-sim kernel (75,776 sims resident),
+  // end to end: 1x the resident count 2.29e8/s, 1.5x 2.37e8, 2x 2.40-2.47e8,
+  // 2.5x 2.27e8, 3x 2.25e8, 4x 2.19e8 (device-resident 2.74-2.78e8); with a
+  // fixed 2^16 minimum 2.24e8.
   FixedShape sh;
   rc = fixed_shape(e, cfg->precision_mode, &sh);
   if (rc != CE_OK) return rc;
   const uint64_t resident = static_cast<uint64_t>(e->sms) * static_cast<uint64_t>(sh.per_sm) * sh.sims_per_block;
-  const uint64_t min_chunk = std::max<uint64_t>(1ull << 16, kResidentPerChunk * resident);
+  const uint64_t min_chunk = std::max<uint64_t>(1ull << 16, kResidentQuartersPerChunk * resident / 4);
   uint64_t bnd[17], C = 0;
   const uint64_t nchunks = ce::chunk_bounds(S, min_chunk, 16, bnd, &C);
   auto bound = [&](uint64_t k) -> uint64_t { return bnd[k]; };
