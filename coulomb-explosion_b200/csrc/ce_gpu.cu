@@ -191,8 +191,8 @@ int fixed_shape(ce_engine* e, int mode, FixedShape* sh) {
   const bool atom = t.lanes_per_sim >= 2;
   sh->fn = atom ? ce::select_atom_kernel(e->n, mode) : ce::select_fixed_kernel(e->n, mode);
   if (!sh->fn) return ce::fail(e, CE_ERR_INVALID, "ce_run: no kernel for this atom count");
-  // The thread-per-sim kernel's shared-memory offsets assume exactly kThreadMaxBlock threads.
-  sh->block = atom ? std::min(t.block_threads, ce::kAtomMaxBlock) : ce::kThreadMaxBlock;
+  // The thread-per-sim kernel's shared-memory offsets assume exactly thread_block(n) threads.
+  sh->block = atom ? std::min(t.block_threads, ce::kAtomMaxBlock) : ce::thread_block(e->n);
   sh->sims_per_block = atom ? static_cast<uint64_t>(sh->block / 32) * static_cast<uint64_t>(32 / e->n)
                             : static_cast<uint64_t>(sh->block);
   sh->refill = t.refill_threshold;

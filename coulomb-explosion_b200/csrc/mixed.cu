@@ -595,8 +595,8 @@ int ce_autotune_fixed(ce_engine* e, uint64_t S, const float* pos_dev, const ce_r
   e->tuned_fixed[e->n].valid = false;
   std::vector<int> layouts = {1};
   if (e->n >= 2) layouts.push_back(e->n);
-  // The thread-per-sim kernel always runs kThreadMaxBlock threads per block.
-  const std::vector<int> blocks_sim = {ce::kThreadMaxBlock};
+  // The thread-per-sim kernel always runs thread_block(n) threads per block.
+  const std::vector<int> blocks_sim = {ce::thread_block(e->n)};
   const std::vector<int> blocks_atom = {64, 96, ce::kAtomMaxBlock};
   const int refills[] = {0, 1, 2, 4, 8};  // 0: the per-size default
   double best = -1.0;

@@ -134,8 +134,8 @@ extern "C" int ce_run_device_noalloc(int n, const double* mass_me, const double*
   if (rc != CE_OK) return rc;
 
   const ce::FixedKernelFn fn = kernel_for(n, cfg->precision_mode);
-  const int block = 128;
   const int lanes = ce::default_lanes(n, cfg->precision_mode);
+  const int block = lanes >= 2 ? 128 : ce::thread_block(n);
   // The thread-per-sim kernel takes its stage slots as dynamic shared memory
   // (on-chip, per block; not an allocation).
   const size_t smem = lanes >= 2 ? 0 : ce::thread_smem_bytes(n, block, cfg->precision_mode);

@@ -140,10 +140,13 @@ __host__ __device__ constexpr int thread_slots(int mode) { return (mode & CE_PRE
 // shared memory allows fewer blocks, so more registers a thread.
 template <int N, int MODE>
 __host__ __device__ constexpr int thread_min_blocks() {
-  return (MODE & CE_PREC_KAHAN) ? (N <= 4 ? 3 : 2) : ThreadShape<N>::kMinBlocks;
+  return N >= 8 ? 4 : ((MODE & CE_PREC_KAHAN) ? (N <= 4 ? 3 : 2) : ThreadShape<N>::kMinBlocks);
 }
 
 constexpr int kThreadMaxBlock = 128;
+// Threads per block of the thread-per-sim kernel: 128, and 64 from 8 atoms up,
+// where a 128-thread block's stage slots would leave room for one block per SM.
+__host__ __device__ constexpr int thread_block(int n) { return n >= 8 ? 64 : kThreadMaxBlock; }
 
 // Dynamic shared memory of one thread-per-sim block: thread_slots(mode) stage
 // slots of NC 16-byte chunks for each of its threads.
@@ -398,7 +401,7 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE>& s, const RunP
   constexpr int NC = ThreadShape<N>::NC;
   constexpr int NP = ThreadShape<N>::NP;
   constexpr int NF = ThreadShape<N>::NF;
-  constexpr int B = kThreadMaxBlock;
+  constexpr int B = thread_block(N);
   const float hh = (P.max_dt < s.h) ? P.max_dt : s.h;  // std::min(h_, max_dt)
 
   // Stages 2..6: x_s = x + (c_s h) v + h^2 sum_l abar_sl k_l; k_s = a(x_s)
@@ -579,10 +582,10 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE>& s, const RunP
 // Persistent kernel: each warp keeps its 32 lanes busy by pulling sim indices
 // from a global cursor (one warp-aggregated atomicAdd per refill) whenever at
 // least `refill_threshold` lanes are idle (or all of them). Launched with
-// kThreadMaxBlock threads per block and thread_smem_bytes(N, kThreadMaxBlock)
+// thread_block(N) threads per block and thread_smem_bytes(N, thread_block(N), MODE)
 // bytes of dynamic shared memory.
 template <int N, int MODE>
-__global__ void __launch_bounds__(kThreadMaxBlock, (thread_min_blocks<N, MODE>()))
+__global__ void __launch_bounds__(thread_block(N), (thread_min_blocks<N, MODE>()))
     rk45_fixed_kernel(const RunParams P, const FixedMol M) {
   extern __shared__ float4 ce_stage_slots[];
   ThreadSim<N, MODE> s;
