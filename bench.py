@@ -1274,7 +1274,8 @@ def main():
     # DRAM traffic of one integration launch, from the committed ncu summary of
     # this workload (dram__bytes_read.sum + dram__bytes_write.sum).
     traffic = None
-    layout = "thread" if eng.get_tuning()["lanes_per_sim"] == 1 else "atom"
+    lanes = eng.get_tuning()["lanes_per_sim"]
+    layout = "thread" if lanes == 1 else ("pair" if lanes == 2 and mol.n >= 3 else "atom")
     tp = ROOT / "profiles" / f"rk45_{layout}_{args.molecule}_1e6.md"
     if tp.exists() and S == S_DEFAULT and args.molecule == "ch4" and args.mode == 0:
         import re

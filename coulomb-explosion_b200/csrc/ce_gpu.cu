@@ -140,7 +140,9 @@ int ce_set_tuning(ce_engine* e, const ce_tuning* t) {
   if (v.refill_threshold < 0 || v.refill_threshold > 32)
     return ce::fail(e, CE_ERR_INVALID, "ce_set_tuning: refill_threshold must be in 0..32");
   if (v.lanes_per_sim < 0 || v.lanes_per_sim > CE_MAX_ATOMS)
-    return ce::fail(e, CE_ERR_INVALID, "ce_set_tuning: lanes_per_sim must be 0 (auto), 1 or 2..10 (lane per atom)");
+    return ce::fail(e, CE_ERR_INVALID,
+                    "ce_set_tuning: lanes_per_sim must be 0 (auto), 1 (thread per sim), 2 (two threads per sim) or "
+                    "3..10 (lane per atom)");
   e->tuning = v;
   return CE_OK;
 }
@@ -188,16 +190,19 @@ struct FixedShape {
 int fixed_shape(ce_engine* e, int mode, FixedShape* sh) {
   cudaError_t st;
   const ce_tuning t = effective_tuning(e, e->n, mode);
-  const bool atom = t.lanes_per_sim >= 2;
-  sh->fn = atom ? ce::select_atom_kernel(e->n, mode) : ce::select_fixed_kernel(e->n, mode);
+  const int layout = ce::layout_of(e->n, t.lanes_per_sim);
+  sh->fn = layout == ce::kLayoutAtom   ? ce::select_atom_kernel(e->n, mode)
+           : layout == ce::kLayoutPair ? ce::select_pair_kernel(e->n, mode)
+                                       : ce::select_fixed_kernel(e->n, mode);
   if (!sh->fn) return ce::fail(e, CE_ERR_INVALID, "ce_run: no kernel for this atom count");
-  // The thread-per-sim kernel's shared-memory offsets assume exactly thread_block(n) threads.
-  sh->block = atom ? std::min(t.block_threads, ce::kAtomMaxBlock) : ce::thread_block(e->n);
-  sh->sims_per_block = atom ? static_cast<uint64_t>(sh->block / 32) * static_cast<uint64_t>(32 / e->n)
-                            : static_cast<uint64_t>(sh->block);
+  // The thread-per-sim and two-thread kernels fix their block size at compile
+  // time (their shared-memory offsets are immediates) and keep their stage
+  // accelerations in dynamic shared memory.
+  const ce::FixedLaunchShape ls = ce::fixed_launch_shape(e->n, layout, mode, t.block_threads);
+  sh->block = ls.block;
+  sh->sims_per_block = ls.sims_per_block;
   sh->refill = t.refill_threshold;
-  // The thread-per-sim kernel keeps its stage accelerations in dynamic shared memory.
-  sh->smem = atom ? 0 : ce::thread_smem_bytes(e->n, sh->block, mode);
+  sh->smem = ls.smem;
   if (sh->smem > 0) {
     st = cudaFuncSetAttribute(reinterpret_cast<const void*>(sh->fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
                               static_cast<int>(sh->smem));

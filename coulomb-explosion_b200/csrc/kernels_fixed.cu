@@ -1,6 +1,7 @@
-// kernels_fixed.cu -- instantiates the fixed-molecule persistent kernel for
-// N = 1..10 atoms at one precision mode. Compiled once per mode
-// (-DCE_MODE=0..3) so the 40 instantiations build in parallel.
+// kernels_fixed.cu -- instantiates the fixed-molecule persistent kernels at one
+// precision mode: one thread per sim for N = 1..10 atoms, two threads per sim
+// for N = 3..10. Compiled once per mode (-DCE_MODE=0..3) so the instantiations
+// build in parallel.
 #include "rk45_sim.cuh"
 
 #ifndef CE_MODE
@@ -24,6 +25,20 @@ FixedKernelFn CE_CAT(fixed_kernel_m, CE_MODE)(int n) {
     case 8: return &rk45_fixed_kernel<8, CE_MODE>;
     case 9: return &rk45_fixed_kernel<9, CE_MODE>;
     case 10: return &rk45_fixed_kernel<10, CE_MODE>;
+    default: return nullptr;
+  }
+}
+
+FixedKernelFn CE_CAT(pair_kernel_m, CE_MODE)(int n) {
+  switch (n) {
+    case 3: return &rk45_pair_kernel<3, CE_MODE>;
+    case 4: return &rk45_pair_kernel<4, CE_MODE>;
+    case 5: return &rk45_pair_kernel<5, CE_MODE>;
+    case 6: return &rk45_pair_kernel<6, CE_MODE>;
+    case 7: return &rk45_pair_kernel<7, CE_MODE>;
+    case 8: return &rk45_pair_kernel<8, CE_MODE>;
+    case 9: return &rk45_pair_kernel<9, CE_MODE>;
+    case 10: return &rk45_pair_kernel<10, CE_MODE>;
     default: return nullptr;
   }
 }

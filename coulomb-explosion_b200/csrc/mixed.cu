@@ -593,17 +593,19 @@ int ce_autotune_fixed(ce_engine* e, uint64_t S, const float* pos_dev, const ce_r
   if (rc != CE_OK) return rc;
   const ce_tuning saved = e->tuning;
   e->tuned_fixed[e->n].valid = false;
+  // Layouts: one thread per sim, two threads per sim (3+ atoms), one lane per atom.
   std::vector<int> layouts = {1};
+  if (e->n >= 3) layouts.push_back(2);
   if (e->n >= 2) layouts.push_back(e->n);
-  // The thread-per-sim kernel always runs thread_block(n) threads per block.
-  const std::vector<int> blocks_sim = {ce::thread_block(e->n)};
   const std::vector<int> blocks_atom = {64, 96, ce::kAtomMaxBlock};
   const int refills[] = {0, 1, 2, 4, 8};  // 0: the per-size default
   double best = -1.0;
   ce_tuning best_t{};
   int count = 0;
   for (int L : layouts)
-    for (int B : (L == 1 ? blocks_sim : blocks_atom))
+    for (int B : (ce::layout_of(e->n, L) == ce::kLayoutAtom
+                      ? blocks_atom  // the other two kernels fix their block size
+                      : std::vector<int>{ce::fixed_launch_shape(e->n, ce::layout_of(e->n, L), cfg->precision_mode, 0).block}))
       for (int R : refills) {
         ce_tuning t{B, 0, R, L};
         e->tuning = t;

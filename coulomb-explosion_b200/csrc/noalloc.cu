@@ -74,14 +74,23 @@ int scratch_address(int dev, unsigned long long** addr, char* err, size_t err_le
 }
 
 // The kernel ce_run_device launches by default (ce::default_lanes): one thread
-// per simulation, or one lane per atom.
+// per simulation, two threads per simulation, or one lane per atom.
 ce::FixedKernelFn kernel_for(int n, int mode) {
-  if (ce::default_lanes(n, mode) >= 2) {
+  const int layout = ce::layout_of(n, ce::default_lanes(n, mode));
+  if (layout == ce::kLayoutAtom) {
     switch (mode & 3) {
       case 0: return ce::atom_kernel_m0(n);
       case 1: return ce::atom_kernel_m1(n);
       case 2: return ce::atom_kernel_m2(n);
       default: return ce::atom_kernel_m3(n);
+    }
+  }
+  if (layout == ce::kLayoutPair) {
+    switch (mode & 3) {
+      case 0: return ce::pair_kernel_m0(n);
+      case 1: return ce::pair_kernel_m1(n);
+      case 2: return ce::pair_kernel_m2(n);
+      default: return ce::pair_kernel_m3(n);
     }
   }
   switch (mode & 3) {
@@ -135,10 +144,12 @@ extern "C" int ce_run_device_noalloc(int n, const double* mass_me, const double*
 
   const ce::FixedKernelFn fn = kernel_for(n, cfg->precision_mode);
   const int lanes = ce::default_lanes(n, cfg->precision_mode);
-  const int block = lanes >= 2 ? 128 : ce::thread_block(n);
-  // The thread-per-sim kernel takes its stage slots as dynamic shared memory
-  // (on-chip, per block; not an allocation).
-  const size_t smem = lanes >= 2 ? 0 : ce::thread_smem_bytes(n, block, cfg->precision_mode);
+  // The thread-per-sim and two-thread kernels take their stage slots as dynamic
+  // shared memory (on-chip, per block; not an allocation).
+  const ce::FixedLaunchShape ls =
+      ce::fixed_launch_shape(n, ce::layout_of(n, lanes), cfg->precision_mode, ce::kAtomMaxBlock);
+  const int block = ls.block;
+  const size_t smem = ls.smem;
   if (smem > 0 &&
       (cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
                             static_cast<int>(smem)) != cudaSuccess ||
@@ -150,8 +161,7 @@ extern "C" int ce_run_device_noalloc(int n, const double* mass_me, const double*
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     return report(err, err_len, CE_ERR_CUDA, "ce_run_device_noalloc: device query failed");
   if (per_sm < 1) per_sm = 1;
-  const uint64_t sims_per_block =
-      lanes >= 2 ? static_cast<uint64_t>(block / 32) * static_cast<uint64_t>(32 / n) : static_cast<uint64_t>(block);
+  const uint64_t sims_per_block = ls.sims_per_block;
   const uint64_t need = (S + sims_per_block - 1) / sims_per_block;
   const uint64_t grid = need < static_cast<uint64_t>(sms) * per_sm ? need : static_cast<uint64_t>(sms) * per_sm;
 

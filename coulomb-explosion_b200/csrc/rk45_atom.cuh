@@ -50,24 +50,62 @@ constexpr int kAtomMaxBlock = 128;
 // least one (measured: CH4, G = 6: 1 beats 2 and 3 by 0.5 % and 1.5 %; stiff
 // H2O, G = 10: 3 beats 2 and 4 by 0.3 % and 3.7 %; N = 10, G = 3: 1).
 // Thread-per-sim refills once 4 of a warp's 32 sims are idle (CH4: 4 beats 1,
-// 2, 6 and 8 by 0.2 to 6 %); a single atom finishes at once, so 1. A refill
-// threshold of 0 in RunParams or ce_tuning means this per-size default.
+// 2, 6 and 8 by 0.2 to 6 %), two threads per sim once 2 of its 16 are; a
+// single atom finishes at once, so 1. A refill threshold of 0 in RunParams or
+// ce_tuning means this per-size default.
 __host__ __device__ constexpr int default_refill(int n, int lanes_per_sim) {
-  return n < 2 ? 1 : (lanes_per_sim < 2 ? 4 : ((32 / n - 1) / 3 > 1 ? (32 / n - 1) / 3 : 1));
+  return n < 2 ? 1
+               : (lanes_per_sim < 2 ? 4
+                                    : ((lanes_per_sim == 2 && n >= 3)
+                                           ? 2
+                                           : ((32 / n - 1) / 3 > 1 ? (32 / n - 1) / 3 : 1)));
 }
 
 // Default layout of a fixed-molecule run (ce_tuning::lanes_per_sim): one thread
-// per sim for up to kThreadMaxAtoms atoms, and with Kahan compensation (whose
-// terms take four more stage slots, so fewer blocks fit) from 4 atoms up;
-// otherwise one lane per atom. Measured at the tight point, 1e6 sims: CH4 plain
-// FP32 2.78e8 against 2.15e8 explosions/s, full precision form (Kahan + FP64
-// t/E) 2.13e8 against 2.02e8; stiff H2O plain 5.22e8 against 4.66e8, full
-// precision 4.24e8 against 4.32e8 (lane wins); at 10 atoms the seven stage
-// slots allow one 128-thread block per SM and the lane layout wins (6.3e7
-// against 4.4e7).
+// per sim for up to kThreadMaxAtoms atoms (with Kahan compensation, whose terms
+// take four more stage slots, from 4 atoms up), two threads per sim from 7
+// atoms (with Kahan compensation for even counts only), otherwise one lane per
+// atom. Measured at the tight point, 1e6 sims, explosions/s:
+//   CH4, plain FP32: thread 2.78e8, lane 2.15e8; full precision form (Kahan +
+//   FP64 t/E): thread 2.13e8, lane 2.02e8. Stiff H2O plain: thread 5.22e8,
+//   lane 4.66e8; full precision: thread 4.24e8, lane 4.32e8.
+//   Random 7 / 8 / 9 / 10-atom molecules (q in 1..3), plain: two-thread 1.14e8 /
+//   1.08e8 / 7.27e7 / 6.99e7, lane 1.13e8 / 9.60e7 / 6.85e7 / 5.90e7, thread
+//   (7 and 10) 1.13e8 / 4.21e7; full precision: two-thread 1.03e8 / 9.78e7 /
+//   5.87e7 / 5.61e7, lane 1.05e8 / 9.12e7 / 6.54e7 / 5.54e7. C2H6-like plain:
+//   two-thread 7.49e7, lane 6.34e7.
 constexpr int kThreadMaxAtoms = 6;
 __host__ __device__ constexpr int default_lanes(int n, int mode) {
-  return n < 2 ? 1 : ((n <= kThreadMaxAtoms && ((mode & CE_PREC_KAHAN) == 0 || n >= 4)) ? 1 : n);
+  return n < 2 ? 1
+               : (n <= kThreadMaxAtoms ? (((mode & CE_PREC_KAHAN) == 0 || n >= 4) ? 1 : n)
+                                       : (((mode & CE_PREC_KAHAN) == 0 || n % 2 == 0) ? 2 : n));
+}
+
+// Layout of a fixed-molecule run from ce_tuning::lanes_per_sim: 1 = one thread
+// per sim, 2 = two threads per sim (3 or more atoms; with 2 atoms that is one
+// lane per atom), anything larger = one lane per atom.
+enum : int { kLayoutThread = 0, kLayoutPair = 1, kLayoutAtom = 2 };
+__host__ __device__ constexpr int layout_of(int n, int lanes_per_sim) {
+  return (lanes_per_sim <= 1 || n < 2) ? kLayoutThread
+                                       : ((lanes_per_sim == 2 && n >= 3) ? kLayoutPair : kLayoutAtom);
+}
+
+// Threads per block, dynamic shared memory and sims per block of a
+// fixed-molecule launch in layout `layout` (atom_block: the lane-per-atom
+// kernel's block size; the other two kernels fix theirs at compile time).
+struct FixedLaunchShape {
+  int block;
+  size_t smem;
+  unsigned long long sims_per_block;
+};
+inline FixedLaunchShape fixed_launch_shape(int n, int layout, int mode, int atom_block) {
+  if (layout == kLayoutThread) {
+    const int b = thread_block(n);
+    return {b, thread_smem_bytes(n, b, mode), static_cast<unsigned long long>(b)};
+  }
+  if (layout == kLayoutPair) return {kPairBlock, pair_smem_bytes(n, mode), static_cast<unsigned long long>(kPairBlock / 2)};
+  const int b = atom_block < kAtomMaxBlock ? atom_block : kAtomMaxBlock;
+  return {b, 0, static_cast<unsigned long long>(b / 32) * static_cast<unsigned long long>(32 / n)};
 }
 
 template <int N>

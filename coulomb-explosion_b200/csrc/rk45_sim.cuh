@@ -34,6 +34,20 @@
 // pair force and every stage combination then runs on packed FP32x2
 // instructions (FFMA2 / FMUL2 / FADD2, per-element IEEE rounding, so results
 // equal the scalar formulation).
+//
+// Two-thread layout (T = 2, rk45_pair_kernel): for 7..10 atoms a whole sim per
+// thread needs more registers and stage slots than leave room for enough warps,
+// and one lane per atom spends a third of its issue slots on exchange shuffles
+// (the SM's shuffle rate bounds it). Two adjacent lanes then share one sim:
+// lane h of the pair owns atoms h A .. h A + A - 1 (A = ceil(N / 2)) with the
+// same register / stage-slot code as a thread-per-sim run of A atoms, and per
+// force evaluation the two lanes swap positions and cross-pair reactions with
+// 6A shuffles (pair_forces). Sums over the sim (error norm, potential, kinetic
+// energy, initial-step norms) add the partner's part once; IEEE addition is
+// commutative, so both lanes hold the identical value and take identical
+// decisions. With N odd the second lane's last slot is a phantom atom (charge
+// 0, parked 1e15 bohr away): its pair terms are exactly 0, it never moves, and
+// it is left out of every norm, sum and output.
 #pragma once
 
 #include <cstdint>
@@ -133,6 +147,18 @@ struct ThreadShape {
   static constexpr int kMinBlocks = N <= 5 ? 4 : (N <= 7 ? 3 : 2);
 };
 
+// One thread's share of a simulation: T threads per sim (1, or 2 for the
+// two-thread layout), A atoms a thread; ThreadShape<A> sizes its registers and
+// stage slots. With T = 2 and N odd the second thread's last slot is a phantom.
+template <int N, int T>
+struct SimShape {
+  static constexpr int A = (N + T - 1) / T;
+  static constexpr int NF = 3 * A;
+  static constexpr int NC = (NF + 3) / 4;
+  static constexpr int NP = 2 * NC;
+  static constexpr bool kPhantom = T * A != N;
+};
+
 // Stage slots per thread: k2..k6 and k1 / k7 (7); with Kahan compensation also
 // cx and cv, each alternating between two slots like k1 / k7 (11).
 __host__ __device__ constexpr int thread_slots(int mode) { return (mode & CE_PREC_KAHAN) ? 11 : 7; }
@@ -149,10 +175,31 @@ constexpr int kThreadMaxBlock = 128;
 __host__ __device__ constexpr int thread_block(int n) { return n >= 8 ? 64 : kThreadMaxBlock; }
 
 // Dynamic shared memory of one thread-per-sim block: thread_slots(mode) stage
-// slots of NC 16-byte chunks for each of its threads.
+// slots of NC 16-byte chunks for each of its threads (n = atoms a thread).
 __host__ __device__ constexpr size_t thread_smem_bytes(int n, int block, int mode) {
   return static_cast<size_t>(thread_slots(mode)) * static_cast<size_t>((3 * n + 3) / 4) * 16u *
          static_cast<size_t>(block);
+}
+
+// Two-thread layout: 128-thread blocks (64 sims), at most 5 atoms a thread.
+constexpr int kPairBlock = 128;
+__host__ __device__ constexpr int pair_atoms(int n) { return (n + 1) / 2; }
+__host__ __device__ constexpr size_t pair_smem_bytes(int n, int mode) {
+  return thread_smem_bytes(pair_atoms(n), kPairBlock, mode);
+}
+// Blocks per SM the two-thread kernel's register allocator aims for: five
+// atoms a thread (9 and 10 atoms) take 168 registers at 3 blocks (C2H6-like,
+// 1e6 sims at the tight point: 7.49e7 explosions/s against 6.76e7 at 128
+// registers with spills); with the Kahan slots shared memory allows 2 blocks.
+template <int N, int MODE>
+__host__ __device__ constexpr int pair_min_blocks() {
+  return (SimShape<N, 2>::A >= 5 && (MODE & CE_PREC_KAHAN) == 0) ? 3 : thread_min_blocks<SimShape<N, 2>::A, MODE>();
+}
+// Threads per block of the T-threads-per-sim kernels (fixed at compile time:
+// the stage-slot offsets are immediates).
+template <int N, int T>
+__host__ __device__ constexpr int sim_block() {
+  return T == 2 ? kPairBlock : thread_block(N);
 }
 
 // Flat float f of a register 3N-vector (x_i at 2i, y_i at 2i + 1, z_i at 2N + i);
@@ -215,11 +262,184 @@ __device__ __forceinline__ void thread_forces(const float2 (&x)[ThreadShape<N>::
   for (int f = 3 * N; f < 2 * NP; ++f) fl_set<NP>(a, f, 0.0f);
 }
 
-template <int N, int MODE>
+// Cross pairs of the two-thread layout. Thread h owns atoms h A + a (slots
+// a = 0..A-1) and sees its partner's atoms in the same slots b. It evaluates
+// the cross pair (own a, partner b) for b - a = d (mod A) with d = 0 (both
+// threads evaluate these; each keeps its own side and half the potential),
+// 0 < 2d < A, and 2d = A when a < A/2. The partner evaluates the mirror
+// offsets -d, so every other cross pair is evaluated by exactly one thread,
+// which hands the reaction -f to the other (Newton's third law).
+__host__ __device__ constexpr bool pair_cross(int A, int b, int d) {
+  return d == 0 || 2 * d < A || (2 * d == A && (b - d + A) % A < A / 2);
+}
+template <int A>
+__host__ __device__ constexpr int pair_cross_count() {
+  int c = 0;
+  for (int b = 0; b < A; ++b)
+    for (int d = 0; d < A; ++d)
+      if (pair_cross(A, b, d)) ++c;
+  return c;
+}
+
+// One thread's constants in the two-thread layout, in registers (the two
+// threads of a pair own different atoms, so a constant-bank operand at a
+// compile-time index cannot serve both): k q_i q_j of its own pairs (i < j
+// order) and of the cross pairs it evaluates (pair_forces' loop order), 1/m of
+// its atoms. Phantom entries are 0 (1 for 1/m).
+struct NoConsts {};
+template <int N>
+struct PairConsts {
+  static constexpr int A = SimShape<N, 2>::A;
+  static constexpr int NI = A * (A - 1) / 2;
+  static constexpr int NX = pair_cross_count<A>();
+  float pcI[NI > 0 ? NI : 1];
+  float pcX[NX];
+  float inv_m[A];
+  int half;        // 0 or 1: which half of the sim's atoms this thread owns
+  unsigned pmask;  // this thread's lane and its partner's
+};
+template <int N, int T>
+using SimConsts = typename std::conditional<T == 2, PairConsts<N>, NoConsts>::type;
+
+template <int N>
+__device__ __forceinline__ void load_pair_consts(PairConsts<N>& C, const FixedMol& M, unsigned lane) {
+  constexpr int A = PairConsts<N>::A;
+  C.half = static_cast<int>(lane & 1u);
+  C.pmask = 3u << (lane & 30u);
+  const int o = C.half * A, po = (1 - C.half) * A;
+  int k = 0;
+#pragma unroll
+  for (int i = 0; i < A; ++i)
+#pragma unroll
+    for (int j = 0; j < A; ++j) {
+      if (j <= i) continue;
+      C.pcI[k++] = (o + j < N) ? M.pc[(o + i) * N + o + j] : 0.0f;
+    }
+  k = 0;
+#pragma unroll
+  for (int b = 0; b < A; ++b)
+#pragma unroll
+    for (int d = 0; d < A; ++d) {
+      if (!pair_cross(A, b, d)) continue;
+      const int i = (b - d + A) % A;
+      C.pcX[k++] = (o + i < N && po + b < N) ? M.pc[(o + i) * N + po + b] : 0.0f;
+    }
+#pragma unroll
+  for (int a = 0; a < A; ++a) C.inv_m[a] = (o + a < N) ? M.inv_m[o + a] : 1.0f;
+}
+
+// a for this thread's A atoms in the two-thread layout: its own pairs as in
+// thread_forces, then the cross pairs partner slot by partner slot: the
+// partner's position of slot b arrives by three shuffles, the pairs
+// (b - d, b) of pair_cross are evaluated, and the reactions this thread
+// collected for the partner's atom b are swapped for the ones the partner
+// collected for this thread's atom b (three more shuffles). pe gets this
+// thread's share of the potential (its own pairs, its cross pairs, half of
+// each d = 0 pair); the two shares add up to PE.
+template <int N, typename TPE>
+__device__ __forceinline__ void pair_forces(const float2 (&x)[SimShape<N, 2>::NP], float2 (&a)[SimShape<N, 2>::NP],
+                                            const PairConsts<N>& C, bool want_pe, TPE& pe) {
+  constexpr int A = SimShape<N, 2>::A;
+  constexpr int NP = SimShape<N, 2>::NP;
+  float2 axy[A];
+  float az[A];
+#pragma unroll
+  for (int i = 0; i < A; ++i) {
+    axy[i] = make_float2(0.0f, 0.0f);
+    az[i] = 0.0f;
+  }
+  int k = 0;
+#pragma unroll
+  for (int i = 0; i < A; ++i) {
+#pragma unroll
+    for (int j = 0; j < A; ++j) {
+      if (j <= i) continue;
+      const float2 rxy = __ffma2_rn(bcast(-1.0f), x[j], x[i]);
+      const float rz = flc<NP>(x, 2 * A + i) - flc<NP>(x, 2 * A + j);
+      const float d2 = fmaf(rxy.x, rxy.x, fmaf(rxy.y, rxy.y, rz * rz));
+      const float rinv = rsqrtf(d2);
+      const float u = C.pcI[k++] * rinv;
+      if (want_pe) pe += static_cast<TPE>(u);
+      const float sc = u * (rinv * rinv);
+      axy[i] = __ffma2_rn(rxy, bcast(sc), axy[i]);
+      az[i] = fmaf(rz, sc, az[i]);
+      axy[j] = __ffma2_rn(rxy, bcast(-sc), axy[j]);
+      az[j] = fmaf(-rz, sc, az[j]);
+    }
+  }
+  k = 0;
+#pragma unroll
+  for (int b = 0; b < A; ++b) {
+    const float2 pxy = make_float2(__shfl_xor_sync(C.pmask, x[b].x, 1), __shfl_xor_sync(C.pmask, x[b].y, 1));
+    const float pz = __shfl_xor_sync(C.pmask, flc<NP>(x, 2 * A + b), 1);
+    float2 rbxy = make_float2(0.0f, 0.0f);  // reaction on the partner's atom b
+    float rbz = 0.0f;
+#pragma unroll
+    for (int d = 0; d < A; ++d) {
+      if (!pair_cross(A, b, d)) continue;
+      const int i = (b - d + A) % A;
+      const float2 rxy = __ffma2_rn(bcast(-1.0f), pxy, x[i]);
+      const float rz = flc<NP>(x, 2 * A + i) - pz;
+      const float d2 = fmaf(rxy.x, rxy.x, fmaf(rxy.y, rxy.y, rz * rz));
+      const float rinv = rsqrtf(d2);
+      const float u = C.pcX[k++] * rinv;
+      if (want_pe) pe += static_cast<TPE>(d == 0 ? 0.5f * u : u);
+      const float sc = u * (rinv * rinv);
+      axy[i] = __ffma2_rn(rxy, bcast(sc), axy[i]);
+      az[i] = fmaf(rz, sc, az[i]);
+      if (d != 0) {
+        rbxy = __ffma2_rn(rxy, bcast(-sc), rbxy);
+        rbz = fmaf(-rz, sc, rbz);
+      }
+    }
+    const float2 gxy = make_float2(__shfl_xor_sync(C.pmask, rbxy.x, 1), __shfl_xor_sync(C.pmask, rbxy.y, 1));
+    axy[b] = __fadd2_rn(axy[b], gxy);
+    az[b] += __shfl_xor_sync(C.pmask, rbz, 1);
+  }
+#pragma unroll
+  for (int i = 0; i < A; ++i) {
+    a[i] = make_float2(axy[i].x * C.inv_m[i], axy[i].y * C.inv_m[i]);
+    fl_set<NP>(a, 2 * A + i, az[i] * C.inv_m[i]);
+  }
+#pragma unroll
+  for (int f = 3 * A; f < 2 * NP; ++f) fl_set<NP>(a, f, 0.0f);
+}
+
+// The force evaluation of a T-threads-per-sim run.
+template <int N, int T, typename TPE>
+__device__ __forceinline__ void sim_forces(const float2 (&x)[SimShape<N, T>::NP], float2 (&a)[SimShape<N, T>::NP],
+                                           const FixedMol& M, const SimConsts<N, T>& C, bool want_pe, TPE& pe) {
+  if constexpr (T == 2)
+    pair_forces<N, TPE>(x, a, C, want_pe, pe);
+  else
+    thread_forces<N, TPE>(x, a, M, want_pe, pe);
+}
+
+// Sum of a per-thread part over the T threads of a sim (v + partner's v: the
+// same bits in both threads).
+template <int N, int T, typename V>
+__device__ __forceinline__ V sim_sum(V v, const SimConsts<N, T>& C) {
+  if constexpr (T == 2)
+    return v + __shfl_xor_sync(C.pmask, v, 1);
+  else
+    return v;
+}
+
+// Whether flat float f of thread `half`'s register vector belongs to a real
+// atom (false only for the phantom slot).
+template <int N, int T>
+__device__ __forceinline__ bool sim_real(int f, int half) {
+  constexpr int A = SimShape<N, T>::A;
+  if constexpr (!SimShape<N, T>::kPhantom) return true;
+  const int atom = f < 2 * A ? (f >> 1) : f - 2 * A;
+  return half == 0 || atom != A - 1;
+}
+
+template <int N, int MODE, int T = 1>
 struct ThreadSim {
   static constexpr bool kKahan = (MODE & CE_PREC_KAHAN) != 0;
   static constexpr bool kF64 = (MODE & CE_PREC_FP64) != 0;
-  static constexpr int NP = ThreadShape<N>::NP;
+  static constexpr int NP = SimShape<N, T>::NP;
 
   using Acc = typename std::conditional<kF64, double, float>::type;
 
@@ -236,11 +456,12 @@ struct ThreadSim {
   unsigned long long sim;
 };
 
-// Stores K contiguous floats (K compile-time) with float2 stores: an 8-byte
+// Stores the first K floats of v (K compile-time) with float2 stores: an 8-byte
 // aligned start writes pairs (and a trailing single when K is odd), a start 4
 // bytes past alignment writes one single first.
-template <int K>
-__device__ __forceinline__ void store_record(float* dst, const float (&v)[K]) {
+template <int K, int L>
+__device__ __forceinline__ void store_record(float* dst, const float (&v)[L]) {
+  static_assert(K <= L, "store_record: record longer than its source");
   if ((reinterpret_cast<uintptr_t>(dst) & 7u) == 0u) {
 #pragma unroll
     for (int f = 0; f + 1 < K; f += 2) *reinterpret_cast<float2*>(dst + f) = make_float2(v[f], v[f + 1]);
@@ -255,49 +476,66 @@ __device__ __forceinline__ void store_record(float* dst, const float (&v)[K]) {
 
 // FP64 finalize: KE, s = sqrt(E0/KE), p_i = (m_i s) v_i, KER = s^2 KE; then the
 // per-sim output record. A converged sim with non-finite momenta is
-// CE_SIM_NONFINITE.
-template <int N, int MODE>
-__device__ __forceinline__ void thread_finalize(const ThreadSim<N, MODE>& s, int status, double pe_final,
-                                                const RunParams& P, const FixedMol& M) {
-  constexpr int NP = ThreadShape<N>::NP;
+// CE_SIM_NONFINITE. In the two-thread layout each thread writes its own atoms'
+// momenta (the record from atom h A on) and thread 0 the per-sim scalars.
+template <int N, int MODE, int T>
+__device__ __forceinline__ void thread_finalize(const ThreadSim<N, MODE, T>& s, int status, double pe_final,
+                                                const RunParams& P, const FixedMol& M, const SimConsts<N, T>& C) {
+  constexpr int A = SimShape<N, T>::A;
+  constexpr int NP = SimShape<N, T>::NP;
+  int half = 0;
+  if constexpr (T == 2) half = C.half;
+  const int o = half * A;  // first atom of this thread
   double ke = 0.0;
   bool finite = true;
 #pragma unroll
-  for (int i = 0; i < N; ++i) {
-    const double vx = s.v[i].x, vy = s.v[i].y, vz = flc<NP>(s.v, 2 * N + i);
-    ke += 0.5 * M.mass[i] * (vx * vx + vy * vy + vz * vz);
+  for (int i = 0; i < A; ++i) {
+    if (!sim_real<N, T>(2 * i, half)) continue;
+    const double vx = s.v[i].x, vy = s.v[i].y, vz = flc<NP>(s.v, 2 * A + i);
+    ke += 0.5 * M.mass[o + i] * (vx * vx + vy * vy + vz * vz);
     finite = finite && isfinite(vx) && isfinite(vy) && isfinite(vz);
+  }
+  if constexpr (T == 2) {
+    ke = sim_sum<N, T>(ke, C);
+    finite = (__shfl_xor_sync(C.pmask, finite ? 1 : 0, 1) != 0) && finite;
   }
   if (status == CE_SIM_OK && !finite) status = CE_SIM_NONFINITE;
   const double e0d = static_cast<double>(s.e0);
   const double sc =
       (P.redistribute && ke > 0.0) ? (e0d > 0.0 ? e0d * rsqrt(e0d * ke) : sqrt(e0d / ke)) : 1.0;
-  // The sim's 3N momenta, written as one contiguous record with 8-byte stores
-  // (a record starts 8-byte aligned or 4 bytes past it, depending on the sim).
-  float pm[3 * N];
+  // The momenta, written as one contiguous record with 8-byte stores (a record
+  // starts 8-byte aligned or 4 bytes past it, depending on the sim).
+  float pm[3 * A];
 #pragma unroll
-  for (int i = 0; i < N; ++i) {
-    const double mm = M.mass[i] * sc;
+  for (int i = 0; i < A; ++i) {
+    const double mm = M.mass[o + i] * sc;
     pm[i * 3 + 0] = static_cast<float>(mm * static_cast<double>(s.v[i].x));
     pm[i * 3 + 1] = static_cast<float>(mm * static_cast<double>(s.v[i].y));
-    pm[i * 3 + 2] = static_cast<float>(mm * static_cast<double>(flc<NP>(s.v, 2 * N + i)));
+    pm[i * 3 + 2] = static_cast<float>(mm * static_cast<double>(flc<NP>(s.v, 2 * A + i)));
   }
-  store_record<3 * N>(P.momenta + s.sim * (3ull * N), pm);
-  if (P.ker) P.ker[s.sim] = (sc * sc) * ke;
-  if (P.steps) P.steps[s.sim] = s.steps;
-  if (P.status) P.status[s.sim] = static_cast<uint8_t>(status);
-  if (P.rejects) P.rejects[s.sim] = s.rejects;
-  if (P.t_final) P.t_final[s.sim] = static_cast<double>(s.t);
-  if (P.pe_final) P.pe_final[s.sim] = pe_final;
-  if (P.ke_before) P.ke_before[s.sim] = ke;
-  if (P.e0) P.e0[s.sim] = e0d;
+  float* dst = P.momenta + s.sim * (3ull * N) + 3 * o;
+  if (SimShape<N, T>::kPhantom && half == 1)
+    store_record<3 * (A - 1)>(dst, pm);
+  else
+    store_record<3 * A>(dst, pm);
+  if (half == 0) {
+    if (P.ker) P.ker[s.sim] = (sc * sc) * ke;
+    if (P.steps) P.steps[s.sim] = s.steps;
+    if (P.status) P.status[s.sim] = static_cast<uint8_t>(status);
+    if (P.rejects) P.rejects[s.sim] = s.rejects;
+    if (P.t_final) P.t_final[s.sim] = static_cast<double>(s.t);
+    if (P.pe_final) P.pe_final[s.sim] = pe_final;
+    if (P.ke_before) P.ke_before[s.sim] = ke;
+    if (P.e0) P.e0[s.sim] = e0d;
+  }
   if (P.positions) {
-    float* xp = P.positions + s.sim * (3ull * N);
+    float* xp = P.positions + s.sim * (3ull * N) + 3 * o;
 #pragma unroll
-    for (int i = 0; i < N; ++i) {
+    for (int i = 0; i < A; ++i) {
+      if (!sim_real<N, T>(2 * i, half)) continue;
       xp[i * 3 + 0] = s.x[i].x;
       xp[i * 3 + 1] = s.x[i].y;
-      xp[i * 3 + 2] = flc<NP>(s.x, 2 * N + i);
+      xp[i * 3 + 2] = flc<NP>(s.x, 2 * A + i);
     }
   }
 }
@@ -306,39 +544,49 @@ __device__ __forceinline__ void thread_finalize(const ThreadSim<N, MODE>& s, int
 // heuristic from rest, src/integrators.cpp:197-250 with v0 = 0: every velocity
 // term is 0, sv = atol, and the probe accelerations equal k1; its quotients use
 // the fast forms, as the initial step is a heuristic). Returns false when the
-// sim is already finished (written out).
-template <int N, int MODE>
-__device__ __forceinline__ bool thread_init(ThreadSim<N, MODE>& s, unsigned long long sim, const RunParams& P,
-                                            const FixedMol& M, float4* ks, int B) {
-  using S = ThreadSim<N, MODE>;
+// sim is already finished (written out). In the two-thread layout both
+// threads of the pair run it for their own atoms.
+template <int N, int MODE, int T>
+__device__ __forceinline__ bool thread_init(ThreadSim<N, MODE, T>& s, unsigned long long sim, const RunParams& P,
+                                            const FixedMol& M, const SimConsts<N, T>& C, float4* ks, int B) {
+  using S = ThreadSim<N, MODE, T>;
   using Acc = typename S::Acc;
-  constexpr int NP = ThreadShape<N>::NP;
+  constexpr int A = SimShape<N, T>::A;
+  constexpr int NP = SimShape<N, T>::NP;
+  constexpr int NC = SimShape<N, T>::NC;
+  int half = 0;
+  if constexpr (T == 2) half = C.half;
   s.sim = sim;
-  const float* src = P.pos + sim * (3ull * N);
+  const float* src = P.pos + sim * (3ull * N) + 3 * (half * A);
 #pragma unroll
   for (int p = 0; p < NP; ++p) s.x[p] = s.v[p] = make_float2(0.0f, 0.0f);
 #pragma unroll
-  for (int i = 0; i < N; ++i) {
-    s.x[i] = make_float2(__ldg(src + 3 * i), __ldg(src + 3 * i + 1));
-    fl_set<NP>(s.x, 2 * N + i, __ldg(src + 3 * i + 2));
+  for (int i = 0; i < A; ++i) {
+    if (!sim_real<N, T>(2 * i, half)) {  // the phantom: zero charge, parked far from every atom
+      s.x[i] = make_float2(1e15f, 1e15f);
+      fl_set<NP>(s.x, 2 * A + i, 1e15f);
+    } else {
+      s.x[i] = make_float2(__ldg(src + 3 * i), __ldg(src + 3 * i + 1));
+      fl_set<NP>(s.x, 2 * A + i, __ldg(src + 3 * i + 2));
+    }
   }
-#pragma unroll
   if (S::kKahan) {  // compensation terms start at zero
     s.cxs = 7;
     s.cvs = 9;
 #pragma unroll
-    for (int c = 0; c < ThreadShape<N>::NC; ++c) {
-      ks[(7 * ThreadShape<N>::NC + c) * B] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-      ks[(9 * ThreadShape<N>::NC + c) * B] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    for (int c = 0; c < NC; ++c) {
+      ks[(7 * NC + c) * B] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      ks[(9 * NC + c) * B] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
   }
   Acc pe0 = Acc(0);
   float2 k0[NP];
-  thread_forces<N, Acc>(s.x, k0, M, true, pe0);
+  sim_forces<N, T, Acc>(s.x, k0, M, C, true, pe0);
+  pe0 = sim_sum<N, T>(pe0, C);
   s.k1s = 5;
 #pragma unroll
-  for (int c = 0; c < ThreadShape<N>::NC; ++c)
-    ks[(5 * ThreadShape<N>::NC + c) * B] = make_float4(k0[2 * c].x, k0[2 * c].y, k0[2 * c + 1].x, k0[2 * c + 1].y);
+  for (int c = 0; c < NC; ++c)
+    ks[(5 * NC + c) * B] = make_float4(k0[2 * c].x, k0[2 * c].y, k0[2 * c + 1].x, k0[2 * c + 1].y);
   s.t = Acc(0);
   s.steps = s.rejects = s.rej_in_step = 0u;
   s.rej_once = false;
@@ -352,19 +600,21 @@ __device__ __forceinline__ bool thread_init(ThreadSim<N, MODE>& s, unsigned long
   else if (!(pe0 > s.pe_stop)) fin = CE_SIM_OK;  // already at or below the stop (driver.cpp:19)
   else if (P.max_steps == 0u) fin = CE_SIM_MAX_STEPS;
   if (fin >= 0) {
-    thread_finalize(s, fin, static_cast<double>(pe0), P, M);
+    thread_finalize<N, MODE, T>(s, fin, static_cast<double>(pe0), P, M, C);
     return false;
   }
   float d0_sq = 0.0f, d1_sq = 0.0f;
   const float inv_atol = __frcp_rn(P.atol);
 #pragma unroll
-  for (int f = 0; f < 3 * N; ++f) {
+  for (int f = 0; f < 3 * A; ++f) {
     const float xf = flc<NP>(s.x, f);
     const float r0 = __fdividef(xf, P.atol + P.rtol * fabsf(xf));
     const float r1 = flc<NP>(k0, f) * inv_atol;
-    d0_sq += r0 * r0;
+    if (sim_real<N, T>(f, half)) d0_sq += r0 * r0;
     d1_sq += r1 * r1;
   }
+  d0_sq = sim_sum<N, T>(d0_sq, C);
+  d1_sq = sim_sum<N, T>(d1_sq, C);
   constexpr float inv_denom = 1.0f / static_cast<float>(6 * N);
   const float d0 = sqrt_approx(d0_sq * inv_denom);
   const float d1 = sqrt_approx(d1_sq * inv_denom);
@@ -372,11 +622,12 @@ __device__ __forceinline__ bool thread_init(ThreadSim<N, MODE>& s, unsigned long
                                                                                          : __fdividef(0.01f * d0, d1);
   float d2_sq = 0.0f;
 #pragma unroll
-  for (int f = 0; f < 3 * N; ++f) {
+  for (int f = 0; f < 3 * A; ++f) {
     const float xf = flc<NP>(s.x, f);
     const float r = __fdividef(flc<NP>(k0, f) * h0, P.atol + P.rtol * fabsf(xf));
     d2_sq += r * r;
   }
+  d2_sq = sim_sum<N, T>(d2_sq, C);
   const float d2 = __fdividef(sqrt_approx(d2_sq * inv_denom), h0);
   const float h1 = (static_cast<double>(d1) <= 1e-15 && static_cast<double>(d2) <= 1e-15)
                        ? fmaxf(1e-6f, h0 * 1e-3f)
@@ -391,17 +642,17 @@ __device__ __forceinline__ bool thread_init(ThreadSim<N, MODE>& s, unsigned long
 // One DP5(4) attempt (src/integrators.cpp:83-146) plus, on acceptance, the
 // driver's stop test (src/driver.cpp:19-30). `ks` is this thread's first stage
 // chunk in shared memory; chunk c of stage slot l is ks[(l * NC + c) * B], B =
-// kThreadMaxBlock, so every slot offset is an immediate.
+// sim_block<N, T>(), so every slot offset is an immediate.
 // Returns false once the sim is finished and written out.
-template <int N, int MODE>
-__device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE>& s, const RunParams& P, const FixedMol& M,
-                                               float4* ks) {
-  using S = ThreadSim<N, MODE>;
+template <int N, int MODE, int T>
+__device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE, T>& s, const RunParams& P, const FixedMol& M,
+                                               const SimConsts<N, T>& C, float4* ks) {
+  using S = ThreadSim<N, MODE, T>;
   using Acc = typename S::Acc;
-  constexpr int NC = ThreadShape<N>::NC;
-  constexpr int NP = ThreadShape<N>::NP;
-  constexpr int NF = ThreadShape<N>::NF;
-  constexpr int B = thread_block(N);
+  constexpr int NC = SimShape<N, T>::NC;
+  constexpr int NP = SimShape<N, T>::NP;
+  constexpr int NF = SimShape<N, T>::NF;
+  constexpr int B = sim_block<N, T>();
   const float hh = (P.max_dt < s.h) ? P.max_dt : s.h;  // std::min(h_, max_dt)
 
   // Stages 2..6: x_s = x + (c_s h) v + h^2 sum_l abar_sl k_l; k_s = a(x_s)
@@ -438,7 +689,7 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE>& s, const RunP
           xs[2 * c + 1] = __ffma2_rn(bcast(al), make_float2(q.z, q.w), xs[2 * c + 1]);
         }
       }
-      thread_forces<N, Acc>(xs, a, M, false, no_pe);
+      sim_forces<N, T, Acc>(xs, a, M, C, false, no_pe);
       float4* out = ks + (si - 1) * NC * B;
 #pragma unroll
       for (int c = 0; c < NC; ++c)
@@ -471,7 +722,8 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE>& s, const RunP
         xs[p] = __ffma2_rn(bcast(hh2), sum, __ffma2_rn(bcast(hh), s.v[p], s.x[p]));  // c_7 = 1
       }
     }
-    thread_forces<N, Acc>(xs, a, M, true, pe_new);
+    sim_forces<N, T, Acc>(xs, a, M, C, true, pe_new);
+    pe_new = sim_sum<N, T>(pe_new, C);
 #pragma unroll
     for (int c = 0; c < NC; ++c)
       ks[((11 - s.k1s) * NC + c) * B] = make_float4(a[2 * c].x, a[2 * c].y, a[2 * c + 1].x, a[2 * c + 1].y);
@@ -539,7 +791,7 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE>& s, const RunP
   }
   // RMS norm squared: en <= 1 exactly when en^2 <= 1, and the controller's
   // en^-1/5 is (en^2)^-1/10, so no square root is taken.
-  const float en2 = (err2.x + err2.y) * (1.0f / static_cast<float>(6 * N));
+  const float en2 = sim_sum<N, T>(err2.x + err2.y, C) * (1.0f / static_cast<float>(6 * N));
   if (en2 <= 1.0f) {
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
@@ -563,7 +815,7 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE>& s, const RunP
     if (!(pe_new > s.pe_stop)) fin = CE_SIM_OK;
     else if (s.steps >= P.max_steps) fin = CE_SIM_MAX_STEPS;
     if (fin >= 0) {
-      thread_finalize(s, fin, static_cast<double>(pe_new), P, M);
+      thread_finalize<N, MODE, T>(s, fin, static_cast<double>(pe_new), P, M, C);
       return false;
     }
     return true;
@@ -573,48 +825,68 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE>& s, const RunP
   s.rejects += 1u;
   s.rej_in_step += 1u;
   if (s.rej_in_step > static_cast<uint32_t>(kMaxRejections)) {
-    thread_finalize(s, CE_SIM_REJECT_LIMIT, static_cast<double>(pe_new), P, M);
+    thread_finalize<N, MODE, T>(s, CE_SIM_REJECT_LIMIT, static_cast<double>(pe_new), P, M, C);
     return false;
   }
   return true;
 }
 
-// Persistent kernel: each warp keeps its 32 lanes busy by pulling sim indices
-// from a global cursor (one warp-aggregated atomicAdd per refill) whenever at
-// least `refill_threshold` lanes are idle (or all of them). Launched with
-// thread_block(N) threads per block and thread_smem_bytes(N, thread_block(N), MODE)
-// bytes of dynamic shared memory.
-template <int N, int MODE>
-__global__ void __launch_bounds__(thread_block(N), (thread_min_blocks<N, MODE>()))
-    rk45_fixed_kernel(const RunParams P, const FixedMol M) {
+// Persistent loop: each warp keeps its sims busy by pulling sim indices from a
+// global cursor (one warp-aggregated atomicAdd per refill) whenever at least
+// `refill_threshold` of its sims are idle (or all of them). A sim is one lane
+// (T = 1, 32 sims a warp) or one even/odd lane pair (T = 2, 16 sims a warp; the
+// pair's lanes are always active or idle together).
+template <int N, int MODE, int T>
+__device__ __forceinline__ void fixed_loop(const RunParams& P, const FixedMol& M) {
   extern __shared__ float4 ce_stage_slots[];
-  ThreadSim<N, MODE> s;
+  ThreadSim<N, MODE, T> s;
+  SimConsts<N, T> C;
   bool active = false;
   bool queue_empty = false;
   const unsigned lane = threadIdx.x & 31u;
-  const unsigned lt_mask = (1u << lane) - 1u;
+  if constexpr (T == 2) load_pair_consts<N>(C, M, lane);
+  constexpr unsigned kSimLanes = T == 2 ? 0x55555555u : 0xffffffffu;  // one lane per sim
+  const unsigned first = T == 2 ? (lane & ~1u) : lane;                // this sim's first lane
+  const unsigned lt_mask = (1u << first) - 1u;
   float4* ks = ce_stage_slots + threadIdx.x;
   const int B = static_cast<int>(blockDim.x);
   for (;;) {
     const unsigned idle = __ballot_sync(0xffffffffu, !active);
-    if (!queue_empty && idle != 0u && (idle == 0xffffffffu || __popc(idle) >= P.refill_threshold)) {
-      const int cnt = __popc(idle);
-      const int leader = __ffs(idle) - 1;
+    const unsigned idle_s = idle & kSimLanes;
+    if (!queue_empty && idle != 0u && (idle == 0xffffffffu || __popc(idle_s) >= P.refill_threshold)) {
+      const int cnt = __popc(idle_s);
+      const int leader = __ffs(idle_s) - 1;
       unsigned long long base = 0ull;
       if (static_cast<int>(lane) == leader) base = atomicAdd(P.cursor, static_cast<unsigned long long>(cnt));
       base = __shfl_sync(0xffffffffu, base, leader);
       queue_empty = (base + static_cast<unsigned long long>(cnt) >= P.S);
       if (!active) {
-        const unsigned long long sim = base + static_cast<unsigned long long>(__popc(idle & lt_mask));
-        if (sim < P.S) active = thread_init(s, sim, P, M, ks, B);
+        const unsigned long long sim = base + static_cast<unsigned long long>(__popc(idle_s & lt_mask));
+        if (sim < P.S) active = thread_init<N, MODE, T>(s, sim, P, M, C, ks, B);
       }
     }
     if (!__any_sync(0xffffffffu, active)) {
       if (queue_empty) break;
       continue;
     }
-    if (active) active = thread_attempt(s, P, M, ks);
+    if (active) active = thread_attempt<N, MODE, T>(s, P, M, C, ks);
   }
+}
+
+// One thread per sim: thread_block(N) threads per block and
+// thread_smem_bytes(N, thread_block(N), MODE) bytes of dynamic shared memory.
+template <int N, int MODE>
+__global__ void __launch_bounds__(thread_block(N), (thread_min_blocks<N, MODE>()))
+    rk45_fixed_kernel(const RunParams P, const FixedMol M) {
+  fixed_loop<N, MODE, 1>(P, M);
+}
+
+// Two threads per sim (N >= 3): kPairBlock threads per block and
+// pair_smem_bytes(N, MODE) bytes of dynamic shared memory.
+template <int N, int MODE>
+__global__ void __launch_bounds__(kPairBlock, (pair_min_blocks<N, MODE>()))
+    rk45_pair_kernel(const RunParams P, const FixedMol M) {
+  fixed_loop<N, MODE, 2>(P, M);
 }
 
 using FixedKernelFn = void (*)(RunParams, FixedMol);
@@ -623,5 +895,10 @@ FixedKernelFn fixed_kernel_m0(int n);
 FixedKernelFn fixed_kernel_m1(int n);
 FixedKernelFn fixed_kernel_m2(int n);
 FixedKernelFn fixed_kernel_m3(int n);
+// Two-thread layout, N = 3..10 (nullptr otherwise).
+FixedKernelFn pair_kernel_m0(int n);
+FixedKernelFn pair_kernel_m1(int n);
+FixedKernelFn pair_kernel_m2(int n);
+FixedKernelFn pair_kernel_m3(int n);
 
 }  // namespace ce

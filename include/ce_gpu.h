@@ -111,11 +111,14 @@ typedef struct ce_outputs {
 typedef struct ce_tuning {
   int32_t block_threads;    /* threads per block, multiple of 32 up to 256; the     *
                              * lane-per-atom and mixed kernels run at most 128 and  *
-                             * clamp a larger request; thread-per-sim runs 128      */
+                             * clamp a larger request; thread-per-sim runs 128 (64  *
+                             * from 8 atoms), two threads per sim 128               */
   int32_t blocks_per_sm;    /* persistent grid = SMs * this (0: occupancy limit)    */
   int32_t refill_threshold; /* refill a warp once this many sims are idle (1..32;   *
                              * 0: a default per molecule size)                       */
-  int32_t lanes_per_sim;    /* 1 = one thread per sim; 2..10 = one lane per atom    */
+  int32_t lanes_per_sim;    /* 1 = one thread per sim; 2 = two threads per sim     *
+                             * (3+ atoms; at 2 atoms, one lane per atom); 3..10 =   *
+                             * one lane per atom                                     */
 } ce_tuning;
 
 /* Engine lifetime. ce_create selects `device` and allocates the engine's small
@@ -133,7 +136,8 @@ int ce_set_molecule(ce_engine* e, int n, const double* mass_me, const double* ch
 int ce_set_tuning(ce_engine* e, const ce_tuning* t);
 /* The launch shape a plain-FP32 run of the current molecule uses (explicit
  * fields, else the autotuned entry, else the defaults: one thread per sim up to
- * 6 atoms (4 to 6 with Kahan compensation), else one lane per atom). */
+ * 6 atoms (4 to 6 with Kahan compensation), two threads per sim from 7 atoms
+ * (8 and 10 with Kahan compensation), else one lane per atom). */
 int ce_get_tuning(const ce_engine* e, ce_tuning* t);
 
 /* Integrate S explosions of the fixed molecule from rest.
@@ -241,7 +245,8 @@ void ce_graph_destroy(ce_graph* g);
 /* ---- autotuner -----------------------------------------------------------
  * Time candidate launch shapes on the device -- threads per block (sims per
  * block), refill granularity, and for the fixed path the layout (one thread per
- * sim or one lane per atom) -- over the caller's device inputs, and keep the
+ * sim, two threads per sim or one lane per atom) -- over the caller's device
+ * inputs, and keep the
  * fastest in the engine; it then applies wherever the matching ce_tuning field
  * is 0 (fixed path: per atom count; mixed path: one entry, plus the faster
  * schedule in *best_schedule). `report` (may be NULL) receives up to `cap`

@@ -1,7 +1,10 @@
 // Prints the chunk schedule of the pipelined host-buffer paths (ce::chunk_bounds)
 // for the sizes given on the command line: "S nchunks cmax b0 b1 ... bn" per line;
-// with the single argument "refill", the default refill granularity
-// (ce::default_refill) for n = 1..10 atoms: "n lane-per-atom thread-per-sim".
+// with the single argument "refill", per atom count n = 1..10 the default refill
+// granularity (ce::default_refill) of the lane-per-atom, thread-per-sim and
+// two-thread layouts, the default layout (ce::default_lanes) in plain FP32 and in
+// the full precision form, and the layout lanes_per_sim = 2 selects
+// (ce::layout_of): "n lane thread pair lanes_fp32 lanes_full layout_of_2".
 // Host code only; compiled by tests/test_chunking.py.
 #include <cstdio>
 #include <cstdlib>
@@ -10,7 +13,9 @@
 
 int main(int argc, char** argv) {
   if (argc == 2 && argv[1][0] == 'r') {
-    for (int n = 1; n <= 10; ++n) std::printf("%d %d %d\n", n, ce::default_refill(n, n), ce::default_refill(n, 1));
+    for (int n = 1; n <= 10; ++n)
+      std::printf("%d %d %d %d %d %d %d\n", n, ce::default_refill(n, n), ce::default_refill(n, 1),
+                  ce::default_refill(n, 2), ce::default_lanes(n, 0), ce::default_lanes(n, 3), ce::layout_of(n, 2));
     return 0;
   }
   for (int a = 3; a < argc; ++a) {

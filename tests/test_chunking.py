@@ -3,7 +3,7 @@
 chunks cover [0, S) in order with none empty, below 2 minimum chunks there is one,
 from 6 chunks on the two at each end weigh 1/4 and 1/2 of a full one, and the
 reported largest chunk is the one the device slots are sized for. Also the
-default refill granularity of the lane-per-atom kernels per molecule size."""
+default refill granularity and layout per molecule size."""
 from __future__ import annotations
 
 import shutil
@@ -57,3 +57,17 @@ def test_default_refill(schedule):
     assert [r[0] for r in rows] == list(range(1, 11))
     assert {r[0]: r[1] for r in rows} == {1: 1, 2: 5, 3: 3, 4: 2, 5: 1, 6: 1, 7: 1, 8: 1, 9: 1, 10: 1}
     assert {r[0]: r[2] for r in rows} == {1: 1, **{n: 4 for n in range(2, 11)}}
+    # two threads per sim refill once 2 of a warp's 16 sims are idle (at 2 atoms
+    # lanes_per_sim = 2 is the lane-per-atom layout)
+    assert {r[0]: r[3] for r in rows} == {1: 1, 2: 5, **{n: 2 for n in range(3, 11)}}
+
+
+def test_default_layout(schedule):
+    # lanes_per_sim: 1 = thread per sim, 2 = two threads per sim, n = lane per atom
+    rows = {r[0]: r[4:] for r in schedule("refill")}
+    fp32 = {n: rows[n][0] for n in rows}
+    full = {n: rows[n][1] for n in rows}
+    assert fp32 == {1: 1, 2: 1, 3: 1, 4: 1, 5: 1, 6: 1, 7: 2, 8: 2, 9: 2, 10: 2}
+    assert full == {1: 1, 2: 2, 3: 3, 4: 1, 5: 1, 6: 1, 7: 7, 8: 2, 9: 9, 10: 2}
+    # layout_of(n, 2): 0 thread, 1 two threads, 2 lane per atom
+    assert {n: rows[n][2] for n in rows} == {1: 0, 2: 2, **{n: 1 for n in range(3, 11)}}

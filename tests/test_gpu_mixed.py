@@ -233,13 +233,15 @@ def test_autotuner_picks_a_measured_candidate_and_keeps_results(ce, wl):
     engine.set_molecule(mol.masses_me, mol.charge_array)
     x = torch.from_numpy(wl.sample_molecule(mol, S, seed=36).astype(np.float32)).cuda()
     rep = engine.autotune_fixed(S, x.data_ptr(), cfg)
-    # thread-per-sim (128 threads) and lane-per-atom (3 block sizes) x 5 refill thresholds
-    assert len(rep) == 20 and {r["lanes_per_sim"] for r in rep} == {1, 5}
+    # thread per sim and two threads per sim (128 threads each) and lane per atom
+    # (3 block sizes), x 5 refill thresholds
+    assert len(rep) == 25 and {r["lanes_per_sim"] for r in rep} == {1, 2, 5}
     t = engine.get_tuning()
     best_f = max(rep, key=lambda r: r["sims_per_s"])
-    # get_tuning reports the resolved shape: refill 0 is CH4's default of 1 in both layouts
+    # get_tuning reports the resolved shape: refill 0 is CH4's per-layout default
+    default_refill = {1: 4, 2: 2, 5: 1}[best_f["lanes_per_sim"]]
     assert (t["block_threads"], t["refill_threshold"], t["lanes_per_sim"]) == (
-        best_f["block_threads"], best_f["refill_threshold"] or 1, best_f["lanes_per_sim"])
+        best_f["block_threads"], best_f["refill_threshold"] or default_refill, best_f["lanes_per_sim"])
 
 
 def _state(torch, ce, S):

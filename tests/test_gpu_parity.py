@@ -76,6 +76,60 @@ def test_ch4_thread_per_sim_layout_matches_reference_engine(engine, ce, wl, gold
     assert abs(r.steps.mean() - steps_ref.mean()) <= 0.03 * steps_ref.mean()
 
 
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
+@pytest.mark.parametrize("point", ["prod", "tight"])
+def test_ch4_two_thread_layout_matches_reference_engine(engine, ce, wl, golden_ch4, mode, point):
+    """The two-thread layout on the CH4 golden set (5 atoms: 3 + 2, the second
+    thread's last slot a phantom), every precision mode, both tolerance points."""
+    g = golden_ch4
+    engine.set_tuning(lanes_per_sim=2)
+    try:
+        r = run(engine, ce, g["masses"], g["charges"], g["pos"], wl.TIGHT if point == "tight" else wl.PRODUCTION,
+                mode, diagnostics=True)
+    finally:
+        engine.set_tuning()
+    assert (r.status == 0).all()
+    if point == "tight":
+        for bits in (32, 64):
+            err = ol.config_norm_error(r.momenta, g[f"p_tight_f{bits}"])
+            assert err.max() <= TIGHT_MAX, (bits, err.max())
+        steps_ref = g["steps_tight_f32"].astype(float)
+    else:
+        err = ol.config_norm_error(r.momenta, g["p_prod_f32"])
+        assert np.median(err) <= PROD_MEDIAN and np.percentile(err, 99) <= PROD_P99 and err.max() <= PROD_MAX, (
+            np.median(err), np.percentile(err, 99), err.max())
+        steps_ref = g["steps_prod_f32"].astype(float)
+    assert abs(r.steps.mean() - steps_ref.mean()) <= 0.03 * steps_ref.mean()
+    # KER = E_0, and the FP64 sums over both threads' atoms
+    np.testing.assert_allclose(r.ker, r.e0, rtol=1e-9)
+    assert np.isfinite(r.positions).all() and (np.abs(r.positions) < 1e12).all()  # no phantom written out
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
+@pytest.mark.parametrize("n", [7, 8, 9, 10])
+def test_two_thread_layout_every_mode_matches_oracle(engine, ce, wl, n, mode):
+    """Seven to ten atoms, where the two-thread layout is meant to run (odd
+    counts carry a phantom), every precision mode, against the FP64 oracle at
+    the tight point, plus the potential / energy bookkeeping."""
+    rng = np.random.default_rng(700 + n)
+    pos = wl.sample_ball(rng, 160, n, 2.0 * n ** (1 / 3), 0.5).astype(np.float32)
+    mass = rng.choice([1.008, 12.011, 14.007, 15.999, 32.06], n) * wl.AMU_TO_ME
+    q = rng.integers(1, 4, n).astype(float)
+    engine.set_tuning(lanes_per_sim=2)
+    try:
+        r = run(engine, ce, mass, q, pos, wl.TIGHT, mode, diagnostics=True)
+    finally:
+        engine.set_tuning()
+    ref = ol.run_batch(pos.astype(np.float64), mass, q, bits=64, rtol=wl.TIGHT[0], atol=wl.TIGHT[1],
+                       pe_stop=wl.TIGHT[2])
+    assert (r.status == ce.CE_SIM_OK).all()
+    err = ol.config_norm_error(r.momenta, ref["momenta"])
+    assert err.max() <= TIGHT_MAX, err.max()
+    np.testing.assert_allclose(r.e0, ref["ker"], rtol=1e-6)  # the oracle's KER is its E_0 = PE_0
+    np.testing.assert_allclose(r.ker, r.e0, rtol=1e-9)
+    assert (r.pe_final <= wl.TIGHT[2] * r.e0 * (1 + 1e-6)).all()
+
+
 def test_ch4_tight_matches_scipy_oracle(engine, ce, wl, golden_ch4):
     g = golden_ch4
     n = len(g["p_scipy"])
@@ -120,16 +174,21 @@ def test_reference_golden_cases(engine, ce, wl):
         assert r.ker[0] == pytest.approx(c["potential_energy_init"], rel=1e-6)
 
 
-@pytest.mark.parametrize("layout", ["sim", "atom"])
+LAYOUT_LANES = {"sim": lambda n: 1, "pair": lambda n: 2, "atom": lambda n: n}
+
+
+@pytest.mark.parametrize("layout", ["sim", "pair", "atom"])
 @pytest.mark.parametrize("n", list(range(1, 11)))
 def test_every_atom_count_matches_oracle(engine, ce, wl, n, layout):
     if layout == "atom" and n == 1:
         pytest.skip("the lane-per-atom layout needs at least two atoms")
+    if layout == "pair" and n < 3:
+        pytest.skip("the two-thread layout starts at three atoms")
     rng = np.random.default_rng(50 + n)
     pos = wl.sample_ball(rng, 200, n, 2.0 * n ** (1 / 3), 0.5).astype(np.float32)
     mass = rng.choice([1.008, 12.011, 14.007, 15.999, 32.06], n) * wl.AMU_TO_ME
     q = rng.integers(1, 4, n).astype(float)
-    engine.set_tuning(lanes_per_sim=1 if layout == "sim" else n)
+    engine.set_tuning(lanes_per_sim=LAYOUT_LANES[layout](n))
     try:
         r = run(engine, ce, mass, q, pos, wl.TIGHT, 3)
     finally:
@@ -248,7 +307,7 @@ def test_full_size_invariants(engine, ce, wl):
         np.testing.assert_array_equal(a, b)
 
 
-@pytest.mark.parametrize("lanes", [1, 5])
+@pytest.mark.parametrize("lanes", [1, 2, 5])
 def test_results_independent_of_launch_shape(engine, ce, wl, lanes):
     # Each sim's arithmetic is private to its thread (or its lane group), so
     # block size, grid size and refill granularity cannot change a single bit.
