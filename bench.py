@@ -768,9 +768,12 @@ def run_stream(args):
     device, then the integration replayed from a CUDA graph captured once per
     buffer slot; on a side stream: the chunk's momenta / KER / steps / status
     copied into a pinned host ring (two slots) that the host consumes while the
-    next chunk computes. Plain RK45 and the learned closure (a network trained
-    on this molecule, held-out sims) run the same pipeline back to back; the
-    timed region is the whole stream, first geometry to last host byte."""
+    next chunk computes. Plain RK45 (the fixed-molecule entry point
+    ce_run_device, autotuned layout) and the learned closure (a network trained
+    on this molecule, held-out sims; its loose run and continuation go through
+    the mixed-batch entry points, which save and resume integrator state) run
+    the same pipeline back to back; the timed region is the whole stream, first
+    geometry to last host byte."""
     import ctypes
     import importlib
 
@@ -845,6 +848,11 @@ def run_stream(args):
         slots.append(d)
     _, sched = eng.autotune_mixed(C_, slots[0]["cb"], cfg)
     eng.reserve_mixed(C_)
+    # the plain leg: this molecule through the fixed-molecule entry point (rows of
+    # 10 atoms are the same [S][10][3] layout in both), its layout autotuned
+    eng.set_molecule(mol.masses_me, mol.charge_array)
+    eng.autotune_fixed(C_, slots[0]["batch"].pos.data_ptr(), cfg)
+    fixed_tuning = eng.get_tuning()
     clo = cl.Closure(eng, net, C_)
     compute = torch.cuda.Stream(device=dev)
     side = torch.cuda.Stream(device=dev)
@@ -860,13 +868,13 @@ def run_stream(args):
             if mode == "closure":
                 clo.serve(d["batch"], cfg, gate, d["out"], loose_pe_stop=args.loose_pe_stop, stream=cs, cbatch=d["cb"])
             else:
-                eng.run_mixed_device(C_, d["cb"], cfg, d["out"], sched, cs)
+                eng.run_device(C_, d["batch"].pos.data_ptr(), cfg, d["out"], cs)
             torch.cuda.synchronize()
             eng.graph_begin(cs)
             if mode == "closure":
                 clo.serve(d["batch"], cfg, gate, d["out"], loose_pe_stop=args.loose_pe_stop, stream=cs, cbatch=d["cb"])
             else:
-                eng.run_mixed_device(C_, d["cb"], cfg, d["out"], sched, cs)
+                eng.run_device(C_, d["batch"].pos.data_ptr(), cfg, d["out"], cs)
             graphs.append(eng.graph_end(cs))
         return graphs
 
@@ -932,7 +940,7 @@ def run_stream(args):
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(4)]
     for a_, b_ in evs:
         a_.record(compute)
-        eng.run_mixed_device(C_, d0["cb"], cfg, d0["out"], sched, cs)
+        eng.run_device(C_, d0["batch"].pos.data_ptr(), cfg, d0["out"], cs)
         b_.record(compute)
     torch.cuda.synchronize()
     int_ms = float(np.median([a_.elapsed_time(b_) for a_, b_ in evs[1:]]))
@@ -1003,6 +1011,10 @@ def run_stream(args):
                    "rtol": rtol, "atol": atol, "pe_stop": pes, "loose_pe_stop": args.loose_pe_stop,
                    "pipeline": "compute stream: sampler + CUDA-graph replay per chunk; side stream: D2H into a "
                                "2-slot pinned host ring consumed by the host",
+                   "plain_path": "ce_run_device (fixed molecule), autotuned lanes_per_sim "
+                                 f"{fixed_tuning['lanes_per_sim']}, refill {fixed_tuning['refill_threshold']}",
+                   "closure_path": "ce_closure_serve: loose run and continuation through the mixed-batch kernels "
+                                   "(lane per atom)",
                    "d2h_bytes_per_chunk": d2h_bytes},
         "plain": res["plain"], "closure": res["closure"],
         "speedup_vs_plain": res["closure"]["explosions_per_s"] / res["plain"]["explosions_per_s"],
@@ -1013,7 +1025,7 @@ def run_stream(args):
                 "d2h_bytes_per_step": d2h_bytes * (total // C_),
                 "path": "whole stream, first geometry to last host byte: geometries drawn on the device (no input "
                         "copy), every chunk's results copied into pinned host memory"},
-        "roofline": {"bound": "fp32", "kernel": "plain integration of one 1e6-sim chunk (mixed-batch kernels, "
+        "roofline": {"bound": "fp32", "kernel": "plain integration of one 1e6-sim chunk (ce_run_device, "
                                                 "N = 10), event-timed outside the stream",
                      "achieved": int_tf, "peak": fp32["tflops"], "unit": "TFLOP/s", "frac": int_tf / fp32["tflops"],
                      "peak_source": fp32["source"], "flops_per_chunk": int_flops, "chunk_ms": int_ms},

@@ -2,13 +2,13 @@
 1e8 C2H6-like explosions), checked chunk by chunk.
 
 Per chunk, on a compute stream: Philox geometries on the device, then the
-integration replayed from a CUDA graph captured once per buffer slot; on a side
-stream: the chunk's momenta / KER / steps / status copied into a two-slot pinned
-host ring that the host reads while the next chunk computes. This replaces the
-reference's production loop (examples/generate_dataset.cpp:159-240). Every chunk
-read from the ring must equal, bit for bit, an eager ce_run_device of the same
-geometries (the fixed-molecule entry point), and the first chunk must match the
-FP64 oracle on a subset within the tight-point tolerance.
+integration (ce_run_device, the fixed-molecule entry point) replayed from a CUDA
+graph captured once per buffer slot; on a side stream: the chunk's momenta / KER
+/ steps / status copied into a two-slot pinned host ring that the host reads
+while the next chunk computes. This replaces the reference's production loop
+(examples/generate_dataset.cpp:159-240). Every chunk read from the ring must
+equal, bit for bit, an eager ce_run_device of the same geometries, and the first
+chunk must match the FP64 oracle on a subset within the tight-point tolerance.
 """
 from __future__ import annotations
 
@@ -36,7 +36,7 @@ def test_graph_replayed_chunks_in_the_pinned_ring_equal_ce_run_device(ce, wl):
     cfg = ce.RunConfig(rtol=wl.TIGHT[0], atol=wl.TIGHT[1], pe_stop_fraction=wl.TIGHT[2], precision_mode=0)
     eng = ce.Engine(0)
     try:
-        eng.reserve_mixed(Cn)
+        eng.set_molecule(mol.masses_me, mol.charge_array)
         slots = []
         for _ in range(2):
             b = cl.sample_molecule_device(mol, Cn, seed, first_sim=0)
@@ -53,11 +53,11 @@ def test_graph_replayed_chunks_in_the_pinned_ring_equal_ce_run_device(ce, wl):
         compute, side = torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)
         cs = compute.cuda_stream
         graphs = []
-        for d in slots:  # eager call first (sizes scratch), then the capture
-            eng.run_mixed_device(Cn, d["cb"], cfg, d["out"], ce.CE_SCHEDULE_PER_SIZE, cs)
+        for d in slots:  # eager call first (sets the kernel attributes), then the capture
+            eng.run_device(Cn, d["batch"].pos.data_ptr(), cfg, d["out"], cs)
             torch.cuda.synchronize()
             eng.graph_begin(cs)
-            eng.run_mixed_device(Cn, d["cb"], cfg, d["out"], ce.CE_SCHEDULE_PER_SIZE, cs)
+            eng.run_device(Cn, d["batch"].pos.data_ptr(), cfg, d["out"], cs)
             graphs.append(eng.graph_end(cs))
         bcfg = sp.ball_config(mol, seed)
         done = [torch.cuda.Event() for _ in range(2)]
@@ -89,8 +89,7 @@ def test_graph_replayed_chunks_in_the_pinned_ring_equal_ce_run_device(ce, wl):
         for g in graphs:
             g.close()
 
-        # The same geometries through the fixed-molecule entry point, eagerly.
-        eng.set_molecule(mol.masses_me, mol.charge_array)
+        # The same geometries through the same entry point, eagerly.
         pos = torch.empty((Cn, 10, 3), dtype=torch.float32, device=dev)
         ref = {"momenta": torch.empty((Cn, 10, 3), dtype=torch.float32, device=dev),
                "ker": torch.empty(Cn, dtype=torch.float64, device=dev),
