@@ -7,10 +7,12 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 
 #include "ce_gpu.h"
 #include "engine.hpp"
@@ -93,6 +95,7 @@ void ce_destroy(ce_engine* e) {
   for (cudaEvent_t ev : {e->ev_mix_fork, e->ev_mix_join})
     if (ev) cudaEventDestroy(ev);
   if (e->d_arena) cudaFree(e->d_arena);
+  if (e->h_io) cudaFreeHost(e->h_io);
   if (e->d_mixed) cudaFree(e->d_mixed);
   if (e->d_cursor) cudaFree(e->d_cursor);
   if (e->stream) cudaStreamDestroy(e->stream);
@@ -185,11 +188,26 @@ struct FixedShape {
   int per_sm = 0;
   uint64_t sims_per_block = 0;
   int refill = 0;
+  int layout = 0;
 };
 
 int fixed_shape(ce_engine* e, int mode, FixedShape* sh) {
   cudaError_t st;
   const ce_tuning t = effective_tuning(e, e->n, mode);
+  ce_engine::FixedShapeCache& c = e->shape_cache;
+  if (c.valid && c.n == e->n && c.mode == mode && c.t.block_threads == t.block_threads &&
+      c.t.blocks_per_sm == t.blocks_per_sm && c.t.refill_threshold == t.refill_threshold &&
+      c.t.lanes_per_sim == t.lanes_per_sim) {
+    sh->fn = c.fn;
+    sh->block = c.block;
+    sh->smem = c.smem;
+    sh->per_sm = c.per_sm;
+    sh->sims_per_block = c.sims_per_block;
+    sh->refill = t.refill_threshold;
+    sh->layout = c.layout;
+    return CE_OK;
+  }
+  c.valid = false;
   const int layout = ce::layout_of(e->n, t.lanes_per_sim);
   sh->fn = layout == ce::kLayoutAtom   ? ce::select_atom_kernel(e->n, mode)
            : layout == ce::kLayoutPair ? ce::select_pair_kernel(e->n, mode)
@@ -203,6 +221,7 @@ int fixed_shape(ce_engine* e, int mode, FixedShape* sh) {
   sh->sims_per_block = ls.sims_per_block;
   sh->refill = t.refill_threshold;
   sh->smem = ls.smem;
+  sh->layout = layout;
   if (sh->smem > 0) {
     st = cudaFuncSetAttribute(reinterpret_cast<const void*>(sh->fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
                               static_cast<int>(sh->smem));
@@ -220,6 +239,16 @@ int fixed_shape(ce_engine* e, int mode, FixedShape* sh) {
     if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     if (sh->per_sm < 1) sh->per_sm = 1;
   }
+  c.n = e->n;
+  c.mode = mode;
+  c.t = t;
+  c.fn = sh->fn;
+  c.block = sh->block;
+  c.smem = sh->smem;
+  c.per_sm = sh->per_sm;
+  c.sims_per_block = sh->sims_per_block;
+  c.layout = sh->layout;
+  c.valid = true;
   return CE_OK;
 }
 
@@ -250,6 +279,192 @@ int launch_fixed(ce_engine* e, uint64_t S, const float* pos, const ce_run_config
   st = cudaGetLastError();
   if (st != cudaSuccess) return ce::cuda_fail(e, st, "rk45 kernel launch");
   e->last_launches = 1;
+  return CE_OK;
+}
+
+// Streamed host-buffer run (the thread-per-sim and two-thread layouts): ONE
+// persistent launch over all S sims in device buffers, with the copies around
+// it. Positions go up in kIoMaxChunks-bounded chunks on the copy-in stream,
+// each followed by a 4-byte copy that marks the chunk present (io_ready); the
+// kernel's warps wait (bounded) for the chunk of the sims they claim. Every
+// finished sim is counted toward its chunk, and the count that completes a
+// chunk raises a flag in mapped host memory; the host, polling those flags in
+// order, sends each chunk's results down on the copy-out stream while the
+// kernel goes on. Nothing between the first chunk's upload and the last
+// chunk's download waits on a chunk boundary: no per-chunk kernel tails, no
+// slot reuse. Every wait the host makes is bounded and a failure raises the
+// abort word, which ends the kernel's input waits.
+constexpr uint64_t kIoMinChunk = 16384;
+constexpr size_t kIoHeader = 4096;  // cursor, error, ready flags, done counters
+constexpr size_t kIoMaxArena = 8ull << 30;
+
+size_t al256(size_t b) { return (b + 255) & ~static_cast<size_t>(255); }
+
+// Device bytes of a streamed run of S sims with the outputs `out` asks for.
+size_t streamed_bytes(const ce_engine* e, uint64_t S, const ce_outputs* out) {
+  const size_t n3 = static_cast<size_t>(e->n) * 3;
+  size_t b = kIoHeader + 2 * al256(S * n3 * sizeof(float));  // positions in, momenta out
+  if (out->positions) b += al256(S * n3 * sizeof(float));
+  for (const void* p : {static_cast<const void*>(out->ker), static_cast<const void*>(out->t_final),
+                        static_cast<const void*>(out->pe_final), static_cast<const void*>(out->ke_before),
+                        static_cast<const void*>(out->e0)})
+    if (p) b += al256(S * sizeof(double));
+  if (out->steps) b += al256(S * sizeof(uint32_t));
+  if (out->rejects) b += al256(S * sizeof(uint32_t));
+  if (out->status) b += al256(S);
+  return b;
+}
+
+int run_streamed(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg, const ce_outputs* out,
+                 const FixedShape& sh) {
+  cudaError_t st;
+  const size_t n3 = static_cast<size_t>(e->n) * 3;
+  const size_t total = streamed_bytes(e, S, out);
+  if (total > e->arena_bytes) {
+    cudaDeviceSynchronize();
+    if (e->d_arena) cudaFree(e->d_arena);
+    e->d_arena = nullptr;
+    e->arena_bytes = 0;
+    st = cudaMalloc(&e->d_arena, total);
+    if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMalloc(arena)");
+    e->arena_bytes = total;
+  }
+  if (!e->h_io) {
+    st = cudaHostAlloc(reinterpret_cast<void**>(&e->h_io), ce::kIoWords * sizeof(unsigned), cudaHostAllocMapped);
+    if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaHostAlloc(io flags)");
+    st = cudaHostGetDevicePointer(reinterpret_cast<void**>(&e->h_io_dev), e->h_io, 0);
+    if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaHostGetDevicePointer(io flags)");
+  }
+  // chunks: a power of two of sims (the kernel shifts instead of dividing), at
+  // least kIoMinChunk, at most kIoMaxChunks / 2 of them
+  unsigned io_shift = 0;
+  while ((1ull << io_shift) < kIoMinChunk || (S >> io_shift) >= static_cast<uint64_t>(ce::kIoMaxChunks / 2)) ++io_shift;
+  const uint64_t io_chunk = 1ull << io_shift;
+  const uint64_t J = (S + io_chunk - 1) / io_chunk;
+
+  char* base = static_cast<char*>(e->d_arena);
+  auto* cursor = reinterpret_cast<unsigned long long*>(base);
+  auto* ready = reinterpret_cast<unsigned*>(base + 256);
+  auto* done = reinterpret_cast<unsigned long long*>(base + 1024);
+  char* b = base + kIoHeader;
+  auto take = [&](size_t bytes) {
+    char* r = b;
+    b += al256(bytes);
+    return r;
+  };
+  auto* d_pos = reinterpret_cast<float*>(take(S * n3 * sizeof(float)));
+  ce_outputs d{};
+  d.momenta = reinterpret_cast<float*>(take(S * n3 * sizeof(float)));
+  if (out->positions) d.positions = reinterpret_cast<float*>(take(S * n3 * sizeof(float)));
+  if (out->ker) d.ker = reinterpret_cast<double*>(take(S * sizeof(double)));
+  if (out->t_final) d.t_final = reinterpret_cast<double*>(take(S * sizeof(double)));
+  if (out->pe_final) d.pe_final = reinterpret_cast<double*>(take(S * sizeof(double)));
+  if (out->ke_before) d.ke_before = reinterpret_cast<double*>(take(S * sizeof(double)));
+  if (out->e0) d.e0 = reinterpret_cast<double*>(take(S * sizeof(double)));
+  if (out->steps) d.steps = reinterpret_cast<uint32_t*>(take(S * sizeof(uint32_t)));
+  if (out->rejects) d.rejects = reinterpret_cast<uint32_t*>(take(S * sizeof(uint32_t)));
+  if (out->status) d.status = reinterpret_cast<uint8_t*>(take(S));
+
+  volatile unsigned* hio = e->h_io;
+  for (int k = 0; k < ce::kIoWords; ++k) hio[k] = 0u;
+  hio[ce::kIoOne] = 1u;
+
+  const ce::FixedKernelFn fn = ce::select_io_kernel(e->n, cfg->precision_mode, sh.layout == ce::kLayoutPair);
+  if (!fn) return ce::fail(e, CE_ERR_INVALID, "ce_run: no streamed kernel for this atom count");
+  if (sh.smem > 0) {  // the same attributes as the plain kernel of this layout
+    st = cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              static_cast<int>(sh.smem));
+    if (st == cudaSuccess)
+      st = cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributePreferredSharedMemoryCarveout,
+                                cudaSharedmemCarveoutMaxShared);
+    if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaFuncSetAttribute(streamed kernel)");
+  }
+  ce::RunParams P{};
+  ce::fill_run_params(P, cfg, &d, sh.refill);
+  P.pos = d_pos;
+  P.cursor = cursor;
+  P.S = S;
+  P.io_ready = ready;
+  P.io_done = done;
+  P.io_host_done = e->h_io_dev;
+  P.io_abort = e->h_io_dev + ce::kIoAbort;
+  P.io_error = e->h_io_dev + ce::kIoError;
+  P.io_shift = io_shift;
+  const uint64_t need_blocks = (S + sh.sims_per_block - 1) / sh.sims_per_block;
+  const uint64_t grid = std::min<uint64_t>(static_cast<uint64_t>(e->sms) * sh.per_sm, need_blocks);
+
+  // header zeroed, then the kernel; the uploads start once the header is zero
+  st = cudaMemsetAsync(base, 0, kIoHeader, e->stream);
+  if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaMemsetAsync(io header)");
+  int rc = ce::record(e, e->ev_loaded[0], e->stream);
+  if (rc != CE_OK) return rc;
+  fn<<<static_cast<unsigned>(grid), sh.block, sh.smem, e->stream>>>(P, e->mol);
+  st = cudaGetLastError();
+  if (st != cudaSuccess) return ce::cuda_fail(e, st, "rk45 streamed kernel launch");
+  e->last_launches = 1;
+
+  // From here on the kernel may be waiting for input: any failure raises the
+  // abort word before returning.
+  auto abort_run = [&](int code) {
+    hio[ce::kIoAbort] = 1u;
+    cudaStreamSynchronize(e->stream);
+    cudaStreamSynchronize(e->s_in);
+    cudaStreamSynchronize(e->s_out);
+    return code;
+  };
+  if ((rc = ce::wait_on(e, e->s_in, e->ev_loaded[0])) != CE_OK) return abort_run(rc);
+  for (uint64_t j = 0; j < J; ++j) {
+    const uint64_t s0 = j * io_chunk, Sj = std::min<uint64_t>(S, s0 + io_chunk) - s0;
+    st = cudaMemcpyAsync(d_pos + s0 * n3, pos + s0 * n3, Sj * n3 * sizeof(float), cudaMemcpyHostToDevice, e->s_in);
+    if (st == cudaSuccess)
+      st = cudaMemcpyAsync(ready + j, e->h_io + ce::kIoOne, sizeof(unsigned), cudaMemcpyHostToDevice, e->s_in);
+    if (st != cudaSuccess) return abort_run(ce::cuda_fail(e, st, "cudaMemcpyAsync(streamed H2D)"));
+  }
+  // Results down, chunk by chunk as the kernel completes them. The host waits
+  // at most kIoHostWaitSeconds for one chunk, and stops waiting once the kernel
+  // has ended without completing it.
+  constexpr double kIoHostWaitSeconds = 120.0;
+  for (uint64_t j = 0; j < J; ++j) {
+    const auto t0 = std::chrono::steady_clock::now();
+    for (uint64_t spin = 1; hio[j] == 0u; ++spin) {
+      if ((spin & 1023u) == 0u) {
+        const cudaError_t q = cudaStreamQuery(e->stream);
+        if (q != cudaErrorNotReady && hio[j] == 0u) {
+          if (q != cudaSuccess) return abort_run(ce::cuda_fail(e, q, "streamed kernel"));
+          return abort_run(ce::fail(e, CE_ERR_CUDA, "ce_run: the streamed kernel ended before finishing a chunk"));
+        }
+        if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > kIoHostWaitSeconds)
+          return abort_run(ce::fail(e, CE_ERR_CUDA, "ce_run: timed out waiting for a streamed chunk"));
+        std::this_thread::yield();
+      }
+    }
+    const uint64_t s0 = j * io_chunk, Sj = std::min<uint64_t>(S, s0 + io_chunk) - s0;
+    struct Copy {
+      void* dst;
+      const void* src;
+      size_t bytes;
+    } copies[] = {
+        {out->momenta + s0 * n3, d.momenta + s0 * n3, Sj * n3 * sizeof(float)},
+        {out->ker ? out->ker + s0 : nullptr, d.ker + s0, Sj * sizeof(double)},
+        {out->t_final ? out->t_final + s0 : nullptr, d.t_final + s0, Sj * sizeof(double)},
+        {out->pe_final ? out->pe_final + s0 : nullptr, d.pe_final + s0, Sj * sizeof(double)},
+        {out->ke_before ? out->ke_before + s0 : nullptr, d.ke_before + s0, Sj * sizeof(double)},
+        {out->e0 ? out->e0 + s0 : nullptr, d.e0 + s0, Sj * sizeof(double)},
+        {out->steps ? out->steps + s0 : nullptr, d.steps + s0, Sj * sizeof(uint32_t)},
+        {out->rejects ? out->rejects + s0 : nullptr, d.rejects + s0, Sj * sizeof(uint32_t)},
+        {out->status ? out->status + s0 : nullptr, d.status + s0, Sj},
+        {out->positions ? out->positions + s0 * n3 : nullptr, d.positions + s0 * n3, Sj * n3 * sizeof(float)}};
+    for (const Copy& c : copies) {
+      if (!c.dst) continue;
+      st = cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, e->s_out);
+      if (st != cudaSuccess) return abort_run(ce::cuda_fail(e, st, "cudaMemcpyAsync(streamed D2H)"));
+    }
+  }
+  st = cudaStreamSynchronize(e->s_out);
+  if (st == cudaSuccess) st = cudaStreamSynchronize(e->stream);
+  if (st == cudaSuccess) st = cudaStreamSynchronize(e->s_in);
+  if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaStreamSynchronize");
+  if (hio[ce::kIoError] != 0u) return ce::fail(e, CE_ERR_CUDA, "ce_run: a streamed input wait ran out");
   return CE_OK;
 }
 
@@ -307,6 +522,11 @@ int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
   FixedShape sh;
   rc = fixed_shape(e, cfg->precision_mode, &sh);
   if (rc != CE_OK) return rc;
+  // The thread-per-sim and two-thread layouts stream their I/O around one
+  // launch (run_streamed) when the whole batch fits the device arena bound.
+  if (sh.layout != ce::kLayoutAtom && S >= 2 * kIoMinChunk && S < (1ull << 31) &&
+      streamed_bytes(e, S, out) <= kIoMaxArena)
+    return run_streamed(e, S, pos, cfg, out, sh);
   const uint64_t resident = static_cast<uint64_t>(e->sms) * static_cast<uint64_t>(sh.per_sm) * sh.sims_per_block;
   const uint64_t min_chunk = std::max<uint64_t>(1ull << 16, kResidentQuartersPerChunk * resident / 4);
   uint64_t bnd[17], C = 0;

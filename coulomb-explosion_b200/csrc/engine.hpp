@@ -46,8 +46,34 @@ struct ce_engine {
   cudaStream_t s_mix2 = nullptr;
   cudaEvent_t ev_mix_fork = nullptr, ev_mix_join = nullptr;
   int last_launches = 0;
+  // Launch shape of the last fixed-molecule run (ce_gpu.cu fixed_shape), reused
+  // while the atom count, precision mode and effective tuning are unchanged, so
+  // the chunks of a ce_run set kernel attributes and query occupancy once.
+  struct FixedShapeCache {
+    bool valid = false;
+    int n = 0, mode = 0;
+    ce_tuning t{};
+    ce::FixedKernelFn fn = nullptr;
+    int block = 0;
+    size_t smem = 0;
+    int per_sm = 0;
+    unsigned long long sims_per_block = 0;
+    int layout = 0;
+  } shape_cache;
+  // Streamed ce_run (ce_gpu.cu run_streamed): mapped pinned host words, words
+  // [0, kIoMaxChunks) the per-chunk done flags the kernel raises, then the abort
+  // word the host raises, the constant 1 the input-ready copies read, and the
+  // kernel's error word copied back.
+  unsigned* h_io = nullptr;
+  unsigned* h_io_dev = nullptr;
   std::string err;
 };
+
+namespace ce {
+constexpr int kIoMaxChunks = 64;
+constexpr int kIoAbort = kIoMaxChunks, kIoOne = kIoMaxChunks + 1, kIoError = kIoMaxChunks + 2;
+constexpr int kIoWords = kIoMaxChunks + 4;
+}  // namespace ce
 
 namespace ce {
 
@@ -110,6 +136,15 @@ inline FixedKernelFn select_pair_kernel(int n, int mode) {
     case 1: return pair_kernel_m1(n);
     case 2: return pair_kernel_m2(n);
     default: return pair_kernel_m3(n);
+  }
+}
+
+inline FixedKernelFn select_io_kernel(int n, int mode, bool pair) {
+  switch (mode & 3) {
+    case 0: return io_kernel_m0(n, pair);
+    case 1: return io_kernel_m1(n, pair);
+    case 2: return io_kernel_m2(n, pair);
+    default: return io_kernel_m3(n, pair);
   }
 }
 

@@ -113,6 +113,20 @@ struct RunParams {
   const uint32_t* res_rejects;
   const double* res_e0;
   const float* res_comp;
+  // Streamed host-buffer run (ce_run, the *_io kernels): positions arrive in
+  // chunks of 2^io_shift sims, io_ready[j] != 0 once chunk j is in device memory
+  // (written by a copy after the chunk's own copy). Every finished sim is
+  // counted in io_done[j] (one count per thread of the sim); the count that
+  // completes chunk j raises io_host_done[j] in mapped host memory, and the host
+  // then copies that chunk's results out. io_abort (mapped host memory) != 0 ends
+  // every input wait at once; a wait that ends without its input sets io_error
+  // (mapped host memory) and its sims finish as CE_SIM_BAD_INPUT.
+  const unsigned* io_ready;
+  unsigned long long* io_done;
+  unsigned* io_host_done;
+  const unsigned* io_abort;
+  unsigned* io_error;
+  unsigned io_shift;  // chunks of 2^io_shift sims
 };
 
 
@@ -546,7 +560,7 @@ __device__ __forceinline__ void thread_finalize(const ThreadSim<N, MODE, T>& s, 
 // the fast forms, as the initial step is a heuristic). Returns false when the
 // sim is already finished (written out). In the two-thread layout both
 // threads of the pair run it for their own atoms.
-template <int N, int MODE, int T>
+template <int N, int MODE, int T, bool IO>
 __device__ __forceinline__ bool thread_init(ThreadSim<N, MODE, T>& s, unsigned long long sim, const RunParams& P,
                                             const FixedMol& M, const SimConsts<N, T>& C, float4* ks, int B) {
   using S = ThreadSim<N, MODE, T>;
@@ -565,6 +579,9 @@ __device__ __forceinline__ bool thread_init(ThreadSim<N, MODE, T>& s, unsigned l
     if (!sim_real<N, T>(2 * i, half)) {  // the phantom: zero charge, parked far from every atom
       s.x[i] = make_float2(1e15f, 1e15f);
       fl_set<NP>(s.x, 2 * A + i, 1e15f);
+    } else if (IO) {  // written by a copy while the kernel runs: load through L2, not the read-only path
+      s.x[i] = make_float2(__ldcg(src + 3 * i), __ldcg(src + 3 * i + 1));
+      fl_set<NP>(s.x, 2 * A + i, __ldcg(src + 3 * i + 2));
     } else {
       s.x[i] = make_float2(__ldg(src + 3 * i), __ldg(src + 3 * i + 1));
       fl_set<NP>(s.x, 2 * A + i, __ldg(src + 3 * i + 2));
@@ -831,12 +848,72 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE, T>& s, const R
   return true;
 }
 
+// Streamed-run helpers (RunParams io_*).
+__device__ __forceinline__ unsigned ld_acquire_sys(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.sys.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Waits until chunk j's positions are in device memory. Bounded: about 4 s of
+// 256 ns sleeps, or until the host raises io_abort; then io_error is set and
+// false returned. The abort word lives in host memory, so it is read only every
+// 1024th poll: thousands of waiting warps reading across PCIe at every poll
+// starve the very copies they wait for.
+static __device__ __noinline__ bool io_wait_input(const unsigned* ready, const unsigned* abort_flag, unsigned* error) {
+  constexpr unsigned kMaxPolls = 1u << 24;
+  for (unsigned i = 0; i < kMaxPolls; ++i) {
+    if (ld_acquire_gpu(ready) != 0u) return true;  // device memory, written by a copy
+    if ((i & 1023u) == 1023u && ld_acquire_sys(abort_flag) != 0u) break;
+    __nanosleep(256);
+  }
+  *reinterpret_cast<volatile unsigned*>(error) = 1u;
+  __threadfence_system();
+  return false;
+}
+
+// Counts the sims the warp's threads finished in this iteration (fin) toward
+// their chunks (chunk = sim >> io_shift): the finishing lanes are grouped by
+// chunk, and after a __syncwarp one lane per group fences (covering the
+// outputs its group wrote) and adds the group's count; the count that
+// completes a chunk raises its host flag. Warp-collective; one ballot per
+// iteration when nothing finished.
+template <int T>
+__device__ __forceinline__ void io_count(const RunParams& P, bool fin, unsigned long long sim) {
+  unsigned rem = __ballot_sync(0xffffffffu, fin);
+  if (rem == 0u) return;
+  const unsigned j = static_cast<unsigned>(sim >> P.io_shift);
+  __syncwarp();
+  while (rem != 0u) {
+    const int l = __ffs(rem) - 1;
+    const unsigned jl = __shfl_sync(0xffffffffu, j, l);
+    const unsigned grp = __ballot_sync(0xffffffffu, fin && j == jl);
+    rem &= ~grp;
+    if ((threadIdx.x & 31u) == static_cast<unsigned>(l)) {
+      __threadfence();
+      const unsigned long long lo = static_cast<unsigned long long>(jl) << P.io_shift;
+      const unsigned long long hi = lo + (1ull << P.io_shift) < P.S ? lo + (1ull << P.io_shift) : P.S;
+      const unsigned long long add = static_cast<unsigned long long>(__popc(grp));
+      if (atomicAdd(P.io_done + jl, add) + add == static_cast<unsigned long long>(T) * (hi - lo)) {
+        __threadfence_system();
+        *reinterpret_cast<volatile unsigned*>(P.io_host_done + jl) = 1u;
+      }
+    }
+  }
+}
+
 // Persistent loop: each warp keeps its sims busy by pulling sim indices from a
 // global cursor (one warp-aggregated atomicAdd per refill) whenever at least
 // `refill_threshold` of its sims are idle (or all of them). A sim is one lane
 // (T = 1, 32 sims a warp) or one even/odd lane pair (T = 2, 16 sims a warp; the
-// pair's lanes are always active or idle together).
-template <int N, int MODE, int T>
+// pair's lanes are always active or idle together). With IO the claimed sims'
+// inputs are awaited (io_wait_input) and finished sims are counted (io_count).
+template <int N, int MODE, int T, bool IO>
 __device__ __forceinline__ void fixed_loop(const RunParams& P, const FixedMol& M) {
   extern __shared__ float4 ce_stage_slots[];
   ThreadSim<N, MODE, T> s;
@@ -850,9 +927,16 @@ __device__ __forceinline__ void fixed_loop(const RunParams& P, const FixedMol& M
   const unsigned lt_mask = (1u << first) - 1u;
   float4* ks = ce_stage_slots + threadIdx.x;
   const int B = static_cast<int>(blockDim.x);
+  // IO: chunks [0, io_known) seen present by this warp. Chunks hold 2^io_shift
+  // sims, so a sim's chunk is a shift (a 64-bit division per iteration cost the
+  // kernel ~5 %), and the one register of state keeps the CH4 kernel within
+  // its 128.
+  unsigned io_known = 0u;
   for (;;) {
     const unsigned idle = __ballot_sync(0xffffffffu, !active);
     const unsigned idle_s = idle & kSimLanes;
+    bool fin = false;  // IO: this thread's sim finished at its claim
+    unsigned long long fin_sim = 0ull;
     if (!queue_empty && idle != 0u && (idle == 0xffffffffu || __popc(idle_s) >= P.refill_threshold)) {
       const int cnt = __popc(idle_s);
       const int leader = __ffs(idle_s) - 1;
@@ -860,16 +944,45 @@ __device__ __forceinline__ void fixed_loop(const RunParams& P, const FixedMol& M
       if (static_cast<int>(lane) == leader) base = atomicAdd(P.cursor, static_cast<unsigned long long>(cnt));
       base = __shfl_sync(0xffffffffu, base, leader);
       queue_empty = (base + static_cast<unsigned long long>(cnt) >= P.S);
+      bool in_ok = true;
+      if constexpr (IO) {
+        // The claimed range's inputs. Chunks arrive in order, so the wait is for
+        // its last chunk, and only for chunks this warp has not yet seen present
+        // (an acquire per refill cost the kernel ~8 %).
+        if (base < P.S) {
+          const unsigned long long last = (base + cnt < P.S ? base + cnt : P.S) - 1ull;
+          const unsigned lc = static_cast<unsigned>(last >> P.io_shift);
+          if (lc >= io_known) {
+            if (static_cast<int>(lane) == leader) in_ok = io_wait_input(P.io_ready + lc, P.io_abort, P.io_error);
+            in_ok = __shfl_sync(0xffffffffu, in_ok, leader);
+            if (in_ok) io_known = lc + 1u;
+          }
+        }
+      }
       if (!active) {
         const unsigned long long sim = base + static_cast<unsigned long long>(__popc(idle_s & lt_mask));
-        if (sim < P.S) active = thread_init<N, MODE, T>(s, sim, P, M, C, ks, B);
+        if (sim < P.S) {
+          if (in_ok) {
+            active = thread_init<N, MODE, T, IO>(s, sim, P, M, C, ks, B);
+          } else if (P.status && lane == first) {
+            P.status[sim] = static_cast<uint8_t>(CE_SIM_BAD_INPUT);
+          }
+          fin = !active;
+          fin_sim = sim;
+        }
       }
     }
+    if constexpr (IO) io_count<T>(P, fin, fin_sim);
     if (!__any_sync(0xffffffffu, active)) {
       if (queue_empty) break;
       continue;
     }
-    if (active) active = thread_attempt<N, MODE, T>(s, P, M, C, ks);
+    bool done = false;
+    if (active) {
+      active = thread_attempt<N, MODE, T>(s, P, M, C, ks);
+      done = !active;
+    }
+    if constexpr (IO) io_count<T>(P, done, s.sim);
   }
 }
 
@@ -878,7 +991,7 @@ __device__ __forceinline__ void fixed_loop(const RunParams& P, const FixedMol& M
 template <int N, int MODE>
 __global__ void __launch_bounds__(thread_block(N), (thread_min_blocks<N, MODE>()))
     rk45_fixed_kernel(const RunParams P, const FixedMol M) {
-  fixed_loop<N, MODE, 1>(P, M);
+  fixed_loop<N, MODE, 1, false>(P, M);
 }
 
 // Two threads per sim (N >= 3): kPairBlock threads per block and
@@ -886,7 +999,19 @@ __global__ void __launch_bounds__(thread_block(N), (thread_min_blocks<N, MODE>()
 template <int N, int MODE>
 __global__ void __launch_bounds__(kPairBlock, (pair_min_blocks<N, MODE>()))
     rk45_pair_kernel(const RunParams P, const FixedMol M) {
-  fixed_loop<N, MODE, 2>(P, M);
+  fixed_loop<N, MODE, 2, false>(P, M);
+}
+
+// The same two kernels with streamed host-buffer I/O (RunParams io_*).
+template <int N, int MODE>
+__global__ void __launch_bounds__(thread_block(N), (thread_min_blocks<N, MODE>()))
+    rk45_fixed_io_kernel(const RunParams P, const FixedMol M) {
+  fixed_loop<N, MODE, 1, true>(P, M);
+}
+template <int N, int MODE>
+__global__ void __launch_bounds__(kPairBlock, (pair_min_blocks<N, MODE>()))
+    rk45_pair_io_kernel(const RunParams P, const FixedMol M) {
+  fixed_loop<N, MODE, 2, true>(P, M);
 }
 
 using FixedKernelFn = void (*)(RunParams, FixedMol);
@@ -900,5 +1025,11 @@ FixedKernelFn pair_kernel_m0(int n);
 FixedKernelFn pair_kernel_m1(int n);
 FixedKernelFn pair_kernel_m2(int n);
 FixedKernelFn pair_kernel_m3(int n);
+// The streamed-I/O variants: pair = false for one thread per sim (N = 1..10),
+// true for two threads per sim (N = 3..10).
+FixedKernelFn io_kernel_m0(int n, bool pair);
+FixedKernelFn io_kernel_m1(int n, bool pair);
+FixedKernelFn io_kernel_m2(int n, bool pair);
+FixedKernelFn io_kernel_m3(int n, bool pair);
 
 }  // namespace ce

@@ -142,11 +142,16 @@ int ce_get_tuning(const ce_engine* e, ce_tuning* t);
 
 /* Integrate S explosions of the fixed molecule from rest.
  * pos: [S][N][3] float initial positions (host for ce_run, device for
- * ce_run_device). ce_run copies in, runs and copies out synchronously, in up to
- * sixteen chunks (smaller at both ends) whose copies overlap the integration of
- * the neighbouring chunks when the host buffers are pinned (neighbouring chunks
- * integrate on two streams, so one chunk's last simulations overlap the next
- * chunk's first);
+ * ce_run_device). ce_run copies in, runs and copies out synchronously. In the
+ * one-thread and two-thread layouts (2^15 <= S < 2^31, device buffers up to
+ * 8 GiB) it is ONE launch over the whole batch with its copies streamed around
+ * it: positions go up in up to 32 chunks that the kernel's warps wait for
+ * (bounded), and each chunk's results come down as soon as the kernel has
+ * finished its last sim (mapped-memory flags the host polls, bounded). Otherwise
+ * it runs up to sixteen chunks (smaller at both ends) whose copies overlap the
+ * integration of the neighbouring chunks (neighbouring chunks integrate on two
+ * streams, so one chunk's last simulations overlap the next chunk's first).
+ * Pinned host buffers let the copies overlap the integration;
  * ce_run_device enqueues on `stream` (cudaStream_t, NULL = legacy default) and
  * returns without synchronizing. S == 0 is a no-op. */
 int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,

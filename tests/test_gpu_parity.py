@@ -237,27 +237,38 @@ def test_ragged_sizes_and_empty(engine, ce, wl):
         np.testing.assert_array_equal(part.steps, full.steps[:S])
 
 
-def test_chunked_host_path_matches_device_path(engine, ce, wl):
-    # ce_run cuts a batch above 2^17 sims into chunks that alternate between two
-    # device slots, each integrated on its own stream with its own work queue (7
-    # chunks here, the two at each end tapered); the batch must give bit for bit
-    # what one ce_run_device launch gives, in every output.
+@pytest.mark.parametrize("case", ["ch4_thread_streamed", "c2h6_pair_streamed", "ch4_lane_chunked"])
+def test_host_buffer_paths_match_device_path(engine, ce, wl, case):
+    # ce_run, host buffers (pageable here), must give bit for bit what one
+    # ce_run_device launch gives, in every output. The thread-per-sim and
+    # two-thread layouts stream their I/O around one launch (positions up in
+    # chunks the kernel waits for, results down chunk by chunk as the kernel
+    # completes them: 29 chunks here, the last one short); the lane-per-atom
+    # layout cuts the batch into chunks that alternate between two device slots,
+    # each integrated on its own stream with its own work queue (7 chunks here,
+    # the two at each end tapered).
     torch = pytest.importorskip("torch")
-    mol = wl.CH4
+    mol, lanes, mode = {"ch4_thread_streamed": (wl.CH4, 0, 3), "c2h6_pair_streamed": (wl.C2H6_LIKE, 0, 0),
+                        "ch4_lane_chunked": (wl.CH4, 5, 3)}[case]
     engine.set_molecule(mol.masses_me, mol.charge_array)
     S = 7 * 65536 + 777
     pos = wl.sample_molecule(mol, S, seed=41).astype(np.float32)
-    cfg = cfg_for(ce, wl.TIGHT, 3)
-    host = engine.run(pos, cfg, diagnostics=True)
+    cfg = cfg_for(ce, wl.TIGHT, mode)
     dev = torch.device("cuda", 0)
     x = torch.from_numpy(pos).to(dev)
     names = ("momenta", "ker", "steps", "status", "rejects", "t_final", "pe_final", "ke_before", "positions", "e0")
-    # raw byte buffers on the device, read back with each output's dtype and shape
-    d = {k: torch.zeros(getattr(host, k).nbytes, dtype=torch.uint8, device=dev) for k in names}
-    out = ce.CeOutputs(*(d[k].data_ptr() for k in names))
-    stream = torch.cuda.Stream(device=dev)
-    engine.run_device(S, x.data_ptr(), cfg, out, stream.cuda_stream)
-    stream.synchronize()
+    engine.set_tuning(lanes_per_sim=lanes)
+    try:
+        host = engine.run(pos, cfg, diagnostics=True)
+        assert engine.last_launch_count() == (1 if lanes == 0 else 7)
+        # raw byte buffers on the device, read back with each output's dtype and shape
+        d = {k: torch.zeros(getattr(host, k).nbytes, dtype=torch.uint8, device=dev) for k in names}
+        out = ce.CeOutputs(*(d[k].data_ptr() for k in names))
+        stream = torch.cuda.Stream(device=dev)
+        engine.run_device(S, x.data_ptr(), cfg, out, stream.cuda_stream)
+        stream.synchronize()
+    finally:
+        engine.set_tuning()
     assert (host.status == 0).all()
     for k in names:
         h = getattr(host, k)
