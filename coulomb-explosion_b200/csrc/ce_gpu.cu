@@ -10,6 +10,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <thread>
@@ -295,6 +296,19 @@ int launch_fixed(ce_engine* e, uint64_t S, const float* pos, const ce_run_config
 // slot reuse. Every wait the host makes is bounded and a failure raises the
 // abort word, which ends the kernel's input waits.
 constexpr uint64_t kIoMinChunk = 16384;
+// run_streamed's result when the kernel's input waits ran out (no other error).
+constexpr int kIoWaitRanOut = 1000;
+
+// Whether the GPU's work may be serialised for this process: blocking launches,
+// or a tool injected into the CUDA runtime (profilers and checkers serialise
+// kernels and copies). The streamed run needs its copies to run beside its
+// kernel, so ce_run then uses the chunked pipeline.
+bool gpu_work_serialised() {
+  const char* blocking = std::getenv("CUDA_LAUNCH_BLOCKING");
+  if (blocking && std::strcmp(blocking, "0") != 0) return true;
+  const char* injected = std::getenv("CUDA_INJECTION64_PATH");
+  return injected && injected[0] != '\0';
+}
 constexpr size_t kIoHeader = 4096;  // cursor, error, ready flags, done counters
 constexpr size_t kIoMaxArena = 8ull << 30;
 
@@ -464,7 +478,7 @@ int run_streamed(ce_engine* e, uint64_t S, const float* pos, const ce_run_config
   if (st == cudaSuccess) st = cudaStreamSynchronize(e->stream);
   if (st == cudaSuccess) st = cudaStreamSynchronize(e->s_in);
   if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaStreamSynchronize");
-  if (hio[ce::kIoError] != 0u) return ce::fail(e, CE_ERR_CUDA, "ce_run: a streamed input wait ran out");
+  if (hio[ce::kIoError] != 0u) return kIoWaitRanOut;
   return CE_OK;
 }
 
@@ -524,9 +538,14 @@ int ce_run(ce_engine* e, uint64_t S, const float* pos, const ce_run_config* cfg,
   if (rc != CE_OK) return rc;
   // The thread-per-sim and two-thread layouts stream their I/O around one
   // launch (run_streamed) when the whole batch fits the device arena bound.
-  if (sh.layout != ce::kLayoutAtom && S >= 2 * kIoMinChunk && S < (1ull << 31) &&
-      streamed_bytes(e, S, out) <= kIoMaxArena)
-    return run_streamed(e, S, pos, cfg, out, sh);
+  // If its input waits run out (the copies did not run beside the kernel), the
+  // call is redone by the chunked pipeline and the engine stops streaming.
+  if (sh.layout != ce::kLayoutAtom && S >= 2 * kIoMinChunk && S < (1ull << 31) && !e->streamed_off &&
+      !gpu_work_serialised() && streamed_bytes(e, S, out) <= kIoMaxArena) {
+    rc = run_streamed(e, S, pos, cfg, out, sh);
+    if (rc != kIoWaitRanOut) return rc;
+    e->streamed_off = true;
+  }
   const uint64_t resident = static_cast<uint64_t>(e->sms) * static_cast<uint64_t>(sh.per_sm) * sh.sims_per_block;
   const uint64_t min_chunk = std::max<uint64_t>(1ull << 16, kResidentQuartersPerChunk * resident / 4);
   uint64_t bnd[17], C = 0;

@@ -66,6 +66,10 @@ struct ce_engine {
   // kernel's error word copied back.
   unsigned* h_io = nullptr;
   unsigned* h_io_dev = nullptr;
+  // Set once a streamed run's input waits ran out (the copies it waits for did
+  // not run beside the kernel: a tool that serialises the GPU's work); ce_run
+  // then uses the chunked pipeline.
+  bool streamed_off = false;
   std::string err;
 };
 

@@ -861,15 +861,15 @@ __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
 }
 
 // Waits until chunk j's positions are in device memory. Bounded: about 4 s of
-// 256 ns sleeps, or until the host raises io_abort; then io_error is set and
-// false returned. The abort word lives in host memory, so it is read only every
-// 1024th poll: thousands of waiting warps reading across PCIe at every poll
-// starve the very copies they wait for.
+// 256 ns sleeps, or until the host raises io_abort or another wait has already
+// run out (io_error); then io_error is set and false returned. Both words live
+// in host memory, so they are read only every 1024th poll: thousands of waiting
+// warps reading across PCIe at every poll starve the very copies they wait for.
 static __device__ __noinline__ bool io_wait_input(const unsigned* ready, const unsigned* abort_flag, unsigned* error) {
   constexpr unsigned kMaxPolls = 1u << 24;
   for (unsigned i = 0; i < kMaxPolls; ++i) {
     if (ld_acquire_gpu(ready) != 0u) return true;  // device memory, written by a copy
-    if ((i & 1023u) == 1023u && ld_acquire_sys(abort_flag) != 0u) break;
+    if ((i & 1023u) == 1023u && (ld_acquire_sys(abort_flag) != 0u || ld_acquire_sys(error) != 0u)) break;
     __nanosleep(256);
   }
   *reinterpret_cast<volatile unsigned*>(error) = 1u;

@@ -275,6 +275,47 @@ def test_host_buffer_paths_match_device_path(engine, ce, wl, case):
         np.testing.assert_array_equal(h, d[k].cpu().numpy().view(h.dtype).reshape(h.shape), err_msg=k)
 
 
+def test_host_buffer_path_with_blocking_launches(ce, wl, tmp_path):
+    # With blocking launches (or a tool injected into the CUDA runtime, which
+    # serialises kernels and copies) the streamed ce_run could not overlap its
+    # copies with its kernel; ce_run then takes the chunked pipeline. A child
+    # process with CUDA_LAUNCH_BLOCKING=1 must finish promptly with the same bits
+    # as this process's streamed run.
+    import os
+    import subprocess
+    import sys
+
+    from conftest import ROOT
+
+    mol = wl.CH4
+    S = 1 << 19  # three chunks in the chunked pipeline
+    pos = wl.sample_molecule(mol, S, seed=43).astype(np.float32)
+    np.save(tmp_path / "pos.npy", pos)
+    eng = ce.Engine(0)
+    try:
+        eng.set_molecule(mol.masses_me, mol.charge_array)
+        here = eng.run(pos, cfg_for(ce, wl.TIGHT, 0))
+        assert eng.last_launch_count() == 1  # streamed: one launch
+    finally:
+        eng.close()
+    script = (
+        "import sys, numpy as np\n"
+        f"sys.path.insert(0, {str(ROOT)!r})\n"
+        "import __graft_entry__ as g\n"
+        "ce = g.load_package()\n"
+        "from coulomb_explosion_b200 import workloads as wl\n"
+        f"pos = np.load({str(tmp_path / 'pos.npy')!r})\n"
+        "e = ce.Engine(0)\n"
+        "e.set_molecule(wl.CH4.masses_me, wl.CH4.charge_array)\n"
+        "r = e.run(pos, ce.RunConfig(rtol=1e-6, atol=1e-7, pe_stop_fraction=1e-7, precision_mode=0))\n"
+        "assert e.last_launch_count() > 1, e.last_launch_count()\n"
+        f"np.save({str(tmp_path / 'mom.npy')!r}, r.momenta)\n"
+        "e.close()\n")
+    env = dict(os.environ, CUDA_LAUNCH_BLOCKING="1")
+    subprocess.run([sys.executable, "-c", script], env=env, check=True, timeout=300)
+    np.testing.assert_array_equal(np.load(tmp_path / "mom.npy"), here.momenta)
+
+
 def test_full_size_invariants(engine, ce, wl):
     # The benchmark's full size (1e6 CH4 explosions, tight point, plain FP32),
     # checked per sim through properties that hold at any size: every sim
