@@ -38,17 +38,19 @@ def _outputs(ce, b):
                         b["status"].data_ptr(), None, None, None, None)
 
 
-def test_noalloc_entry_point_matches_ce_run_device(ce, wl):
+@pytest.mark.parametrize("case", ["ch4_full_precision", "c2h6_fp32"])
+def test_noalloc_entry_point_matches_ce_run_device(ce, wl, case):
+    # CH4 in the full precision form runs one thread per sim, the 10-atom
+    # C2H6-like molecule in plain FP32 two threads per sim.
     torch = pytest.importorskip("torch")
     lib = ce.load_library()
-    mol = wl.CH4
+    mol, mode = {"ch4_full_precision": (wl.CH4, 3), "c2h6_fp32": (wl.C2H6_LIKE, 0)}[case]
     S = 20_000
     pos = torch.from_numpy(wl.sample_molecule(mol, S, seed=99).astype(np.float32)).cuda()
-    cfg = ce.RunConfig(rtol=wl.TIGHT[0], atol=wl.TIGHT[1], pe_stop_fraction=wl.TIGHT[2],
-                       precision_mode=ce.CE_PREC_KAHAN | ce.CE_PREC_FP64)
+    cfg = ce.RunConfig(rtol=wl.TIGHT[0], atol=wl.TIGHT[1], pe_stop_fraction=wl.TIGHT[2], precision_mode=mode)
 
-    # Ordinary path: engine-owned scratch, default launch shape (one lane per
-    # atom, the kernel the allocation-free entry point launches too).
+    # Ordinary path: engine-owned scratch, default launch shape (the layout the
+    # allocation-free entry point launches too).
     eng = ce.Engine(0)
     eng.set_molecule(mol.masses_me, mol.charge_array)
     ref = _device_buffers(torch, S, mol.n)
