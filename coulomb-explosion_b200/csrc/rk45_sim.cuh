@@ -579,9 +579,10 @@ __device__ __forceinline__ bool thread_init(ThreadSim<N, MODE, T>& s, unsigned l
     if (!sim_real<N, T>(2 * i, half)) {  // the phantom: zero charge, parked far from every atom
       s.x[i] = make_float2(1e15f, 1e15f);
       fl_set<NP>(s.x, 2 * A + i, 1e15f);
-    } else if (IO) {  // written by a copy while the kernel runs: load through L2, not the read-only path
-      s.x[i] = make_float2(__ldcg(src + 3 * i), __ldcg(src + 3 * i + 1));
-      fl_set<NP>(s.x, 2 * A + i, __ldcg(src + 3 * i + 2));
+    } else if (IO) {  // written by a copy while the kernel runs: plain (coherent) loads after the
+                      // acquire that saw the chunk present, not the read-only path
+      s.x[i] = make_float2(src[3 * i], src[3 * i + 1]);
+      fl_set<NP>(s.x, 2 * A + i, src[3 * i + 2]);
     } else {
       s.x[i] = make_float2(__ldg(src + 3 * i), __ldg(src + 3 * i + 1));
       fl_set<NP>(s.x, 2 * A + i, __ldg(src + 3 * i + 2));
