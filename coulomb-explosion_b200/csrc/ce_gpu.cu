@@ -295,7 +295,7 @@ int launch_fixed(ce_engine* e, uint64_t S, const float* pos, const ce_run_config
 // chunk's download waits on a chunk boundary: no per-chunk kernel tails, no
 // slot reuse. Every wait the host makes is bounded and a failure raises the
 // abort word, which ends the kernel's input waits.
-constexpr uint64_t kIoMinChunk = 16384;
+using ce::kIoMinChunk;
 // run_streamed's result when the kernel's input waits ran out (no other error).
 constexpr int kIoWaitRanOut = 1000;
 
@@ -349,10 +349,7 @@ int run_streamed(ce_engine* e, uint64_t S, const float* pos, const ce_run_config
     st = cudaHostGetDevicePointer(reinterpret_cast<void**>(&e->h_io_dev), e->h_io, 0);
     if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaHostGetDevicePointer(io flags)");
   }
-  // chunks: a power of two of sims (the kernel shifts instead of dividing), at
-  // least kIoMinChunk, at most kIoMaxChunks / 2 of them
-  unsigned io_shift = 0;
-  while ((1ull << io_shift) < kIoMinChunk || (S >> io_shift) >= static_cast<uint64_t>(ce::kIoMaxChunks / 2)) ++io_shift;
+  const unsigned io_shift = ce::io_chunk_shift(S);
   const uint64_t io_chunk = 1ull << io_shift;
   const uint64_t J = (S + io_chunk - 1) / io_chunk;
 

@@ -75,6 +75,16 @@ struct ce_engine {
 
 namespace ce {
 constexpr int kIoMaxChunks = 64;
+constexpr uint64_t kIoMinChunk = 16384;
+// Chunk size of a streamed ce_run of S sims, as a power of two 2^shift (the
+// kernel shifts instead of dividing): at least kIoMinChunk sims, fewer than
+// kIoMaxChunks / 2 chunks. A chunk of 2^shift sims is a whole number of 128-byte
+// lines of positions for any atom count, so no cache line spans two chunks.
+inline unsigned io_chunk_shift(uint64_t S) {
+  unsigned shift = 0;
+  while ((1ull << shift) < kIoMinChunk || (S >> shift) >= static_cast<uint64_t>(kIoMaxChunks / 2)) ++shift;
+  return shift;
+}
 constexpr int kIoAbort = kIoMaxChunks, kIoOne = kIoMaxChunks + 1, kIoError = kIoMaxChunks + 2;
 constexpr int kIoWords = kIoMaxChunks + 4;
 }  // namespace ce

@@ -1,4 +1,5 @@
 // Prints the chunk schedule of the pipelined host-buffer paths (ce::chunk_bounds)
+// (with the first argument "stream", the streamed ce_run's chunking instead)
 // for the sizes given on the command line: "S nchunks cmax b0 b1 ... bn" per line;
 // with the single argument "refill", per atom count n = 1..10 the default refill
 // granularity (ce::default_refill) of the lane-per-atom, thread-per-sim and
@@ -12,6 +13,15 @@
 #include "engine.hpp"
 
 int main(int argc, char** argv) {
+  if (argc >= 2 && argv[1][0] == 's') {  // "stream S...": S, the streamed chunk shift and chunk count
+    for (int a = 2; a < argc; ++a) {
+      const uint64_t S = std::strtoull(argv[a], nullptr, 10);
+      const unsigned sh = ce::io_chunk_shift(S);
+      std::printf("%llu %u %llu\n", static_cast<unsigned long long>(S), sh,
+                  static_cast<unsigned long long>((S + (1ull << sh) - 1) >> sh));
+    }
+    return 0;
+  }
   if (argc == 2 && argv[1][0] == 'r') {
     for (int n = 1; n <= 10; ++n)
       std::printf("%d %d %d %d %d %d %d\n", n, ce::default_refill(n, n), ce::default_refill(n, 1),

@@ -27,7 +27,12 @@ def schedule(tmp_path_factory):
                     str(ROOT / "tests" / "cpp" / "chunk_bounds_main.cu")], check=True, capture_output=True)
 
     def run(min_chunk, max_chunks=None):
-        args = [str(min_chunk)] if max_chunks is None else [str(min_chunk), str(max_chunks), *map(str, SIZES)]
+        if min_chunk == "stream":
+            args = ["stream", *map(str, [1 << 15, 65536, 459529, 1_000_000, 10_000_000, 123_456_789, (1 << 31) - 1])]
+        elif max_chunks is None:
+            args = [str(min_chunk)]
+        else:
+            args = [str(min_chunk), str(max_chunks), *map(str, SIZES)]
         out = subprocess.run([str(exe), *args], check=True, capture_output=True, text=True).stdout
         return [list(map(int, line.split())) for line in out.splitlines()]
     return run
@@ -71,3 +76,16 @@ def test_default_layout(schedule):
     assert full == {1: 1, 2: 2, 3: 3, 4: 1, 5: 1, 6: 1, 7: 7, 8: 2, 9: 9, 10: 2}
     # layout_of(n, 2): 0 thread, 1 two threads, 2 lane per atom
     assert {n: rows[n][2] for n in rows} == {1: 0, 2: 2, **{n: 1 for n in range(3, 11)}}
+
+
+def test_streamed_chunks(schedule):
+    # The streamed ce_run (batches of 2^15 .. 2^31 - 1 sims) cuts the positions
+    # into chunks of 2^shift sims: at least 2^14 of them, fewer than 32 chunks,
+    # and for any atom count a whole number of 128-byte lines (12 N 2^shift bytes).
+    for S, shift, J in schedule("stream"):
+        assert shift >= 14 and J == -(-S // (1 << shift)) and J <= 32 and S >> shift < 32, (S, shift, J)
+        assert shift == 14 or S >> (shift - 1) >= 32, (S, shift)  # the smallest such chunk
+        for n in range(1, 11):
+            assert (12 * n << shift) % 128 == 0
+    rows = {S: (shift, J) for S, shift, J in schedule("stream")}
+    assert rows[1_000_000] == (15, 31) and rows[459529] == (14, 29) and rows[1 << 15] == (14, 2)
