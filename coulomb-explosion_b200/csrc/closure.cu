@@ -39,6 +39,7 @@ constexpr int kA = CE_MAX_ATOMS;  // atoms per padded row
 constexpr int kFeat = CE_CLOSURE_FEATURES;
 constexpr int kOut = CE_CLOSURE_OUTPUTS;
 constexpr double kMassUnit = 1822.888486209;  // m_e per amu (include/coulomb/units.hpp:11)
+constexpr float kInvMassUnit = static_cast<float>(1.0 / kMassUnit);
 constexpr float kLogMassScale = 1.0f / 3.5f;  // ln(32.06 amu / 1 amu) ~ 3.47
 constexpr int kPerAtom = 12;                  // features per atom
 constexpr float kRelRef = 1e-2f;              // typical RMS residual (units of Q)
@@ -92,7 +93,10 @@ __device__ __forceinline__ void feat_one(const FeatArgs& A, uint64_t s, bool liv
     for (int i = 0; i < kA; ++i) {
       const bool on = i < n;
       const double mi = on ? ms[i] : 1.0;
-      im[i] = on ? static_cast<float>(1.0 / mi) : 0.0f;
+      // FP32 reciprocal (IEEE, of the mass rounded to FP32): within 2 ulp of the
+      // rounded FP64 quotient, and ten FP64 divisions a sim cost the kernel more
+      // than its 45 pair terms
+      im[i] = on ? __frcp_rn(static_cast<float>(mi)) : 0.0f;
       q[i] = on ? static_cast<float>(qs[i]) : 0.0f;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
@@ -106,9 +110,10 @@ __device__ __forceinline__ void feat_one(const FeatArgs& A, uint64_t s, bool liv
         cz += mi * x[i][2];
       }
     }
-    com[0] = static_cast<float>(cx / msum);
-    com[1] = static_cast<float>(cy / msum);
-    com[2] = static_cast<float>(cz / msum);
+    const double imsum = 1.0 / msum;
+    com[0] = static_cast<float>(cx * imsum);
+    com[1] = static_cast<float>(cy * imsum);
+    com[2] = static_cast<float>(cz * imsum);
 
     // Ballistic pair impulses from the stop to t -> infinity.
 #pragma unroll
@@ -164,7 +169,7 @@ __device__ __forceinline__ void feat_one(const FeatArgs& A, uint64_t s, bool liv
       }
     }
     e0 = A.e0[s];
-    const float scl = static_cast<float>(sqrt(e0 / ke));
+    const float scl = sqrtf(static_cast<float>(e0 / ke));
     double p2 = 0.0, r2 = 0.0, q2 = 0.0;
 #pragma unroll
     for (int i = 0; i < kA; ++i) {
@@ -180,9 +185,10 @@ __device__ __forceinline__ void feat_one(const FeatArgs& A, uint64_t s, bool liv
         }
       }
     }
-    P = static_cast<float>(sqrt(p2 / n));
-    Q = static_cast<float>(sqrt(q2 / n));  // RMS per-atom size of the analytic step p -> p_base
-    L = static_cast<float>(sqrt(r2 / n));
+    const float in = 1.0f / static_cast<float>(n);
+    P = sqrtf(static_cast<float>(p2) * in);
+    Q = sqrtf(static_cast<float>(q2) * in);  // RMS per-atom size of the analytic step p -> p_base
+    L = sqrtf(static_cast<float>(r2) * in);
     if (bad || !(ke > 0.0) || !isfinite(scl) || !(P > 0.0f) || !isfinite(P) || !(Q > 0.0f) || !isfinite(Q) ||
         !(L > 0.0f)) {
       ok = false;
@@ -211,7 +217,7 @@ __device__ __forceinline__ void feat_one(const FeatArgs& A, uint64_t s, bool liv
       const float v4 = on ? p[i][1] * iP : 0.0f, v5 = on ? p[i][2] * iP : 0.0f;
       const float v6 = on ? (dp[i][0] - p[i][0]) * iP : 0.0f, v7 = on ? (dp[i][1] - p[i][1]) * iP : 0.0f;
       const float v8 = on ? (dp[i][2] - p[i][2]) * iP : 0.0f, v9 = on ? q[i] * (1.0f / 3.0f) : 0.0f;
-      const float v10 = on ? logf(static_cast<float>(ms[i] / kMassUnit)) * kLogMassScale : 0.0f;
+      const float v10 = on ? logf(static_cast<float>(ms[i]) * kInvMassUnit) * kLogMassScale : 0.0f;
       const float v11 = on ? 1.0f : 0.0f;
       f2[0] = __floats2bfloat162_rn(v0, v1);
       f2[1] = __floats2bfloat162_rn(v2, v3);
@@ -344,7 +350,7 @@ __global__ void __launch_bounds__(128) closure_apply_kernel(const ApplyArgs A) {
         for (int i = 0; i < kA; ++i) {
           const bool on = i < n;
           const double mi = on ? ms[i] : 1.0;
-          im[i] = on ? static_cast<float>(1.0 / mi) : 0.0f;
+          im[i] = on ? __frcp_rn(static_cast<float>(mi)) : 0.0f;  // as in the features kernel
           if (on) msum += mi;
           double pi2 = 0.0;
 #pragma unroll
@@ -357,7 +363,7 @@ __global__ void __launch_bounds__(128) closure_apply_kernel(const ApplyArgs A) {
             pi2 += static_cast<double>(p[i][c]) * p[i][c];
           }
           ke += 0.5 * pi2 * im[i];
-          pabs += sqrt(pi2);
+          pabs += sqrtf(static_cast<float>(pi2));  // no cancellation in this sum: FP32 is enough
           sx += p[i][0];
           sy += p[i][1];
           sz += p[i][2];
@@ -373,10 +379,11 @@ __global__ void __launch_bounds__(128) closure_apply_kernel(const ApplyArgs A) {
           // Project onto the conservation laws: remove the net momentum (mass
           // weighted, so the centre of mass stays at rest), then rescale to KE = E_0.
           double ke2 = 0.0;
+          const double imsum = 1.0 / msum;
 #pragma unroll
           for (int i = 0; i < kA; ++i) {
             if (i < n) {
-              const double w = ms[i] / msum;
+              const double w = ms[i] * imsum;
               p[i][0] -= static_cast<float>(w * sx);
               p[i][1] -= static_cast<float>(w * sy);
               p[i][2] -= static_cast<float>(w * sz);
