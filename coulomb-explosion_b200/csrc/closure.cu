@@ -88,6 +88,27 @@ __device__ __forceinline__ void feat_one(const FeatArgs& A, uint64_t s, bool liv
   float P = 0.0f, Q = 0.0f, L = 0.0f;
   double e0 = 1.0;
   if (ok) {
+    // The rows of 30 floats (120 B) are read with 8-byte loads when their base
+    // allows it (15 loads a row instead of up to 30; the padded atoms' entries
+    // are valid memory and masked below).
+    float xr[3 * kA], pr[3 * kA];
+    if (((reinterpret_cast<uintptr_t>(xs) | reinterpret_cast<uintptr_t>(ps)) & 7u) == 0u) {
+#pragma unroll
+      for (int k = 0; k < 3 * kA / 2; ++k) {
+        const float2 a = reinterpret_cast<const float2*>(xs)[k];
+        const float2 b = reinterpret_cast<const float2*>(ps)[k];
+        xr[2 * k] = a.x;
+        xr[2 * k + 1] = a.y;
+        pr[2 * k] = b.x;
+        pr[2 * k + 1] = b.y;
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 3 * kA; ++k) {
+        xr[k] = xs[k];
+        pr[k] = ps[k];
+      }
+    }
     double msum = 0.0, cx = 0.0, cy = 0.0, cz = 0.0;
 #pragma unroll
     for (int i = 0; i < kA; ++i) {
@@ -100,8 +121,8 @@ __device__ __forceinline__ void feat_one(const FeatArgs& A, uint64_t s, bool liv
       q[i] = on ? static_cast<float>(qs[i]) : 0.0f;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        x[i][c] = on ? xs[3 * i + c] : 0.0f;
-        p[i][c] = on ? ps[3 * i + c] : 0.0f;
+        x[i][c] = on ? xr[3 * i + c] : 0.0f;
+        p[i][c] = on ? pr[3 * i + c] : 0.0f;
       }
       if (on) {
         msum += mi;
