@@ -237,7 +237,8 @@ def test_ragged_sizes_and_empty(engine, ce, wl):
         np.testing.assert_array_equal(part.steps, full.steps[:S])
 
 
-@pytest.mark.parametrize("case", ["ch4_thread_streamed", "c2h6_pair_streamed", "ch4_lane_chunked"])
+@pytest.mark.parametrize("case", ["ch4_thread_streamed", "c2h6_pair_streamed", "nine_atoms_pair_streamed",
+                                  "ch4_lane_chunked"])
 def test_host_buffer_paths_match_device_path(engine, ce, wl, case):
     # ce_run, host buffers (pageable here), must give bit for bit what one
     # ce_run_device launch gives, in every output. The thread-per-sim and
@@ -248,11 +249,19 @@ def test_host_buffer_paths_match_device_path(engine, ce, wl, case):
     # each integrated on its own stream with its own work queue (7 chunks here,
     # the two at each end tapered).
     torch = pytest.importorskip("torch")
-    mol, lanes, mode = {"ch4_thread_streamed": (wl.CH4, 0, 3), "c2h6_pair_streamed": (wl.C2H6_LIKE, 0, 0),
-                        "ch4_lane_chunked": (wl.CH4, 5, 3)}[case]
-    engine.set_molecule(mol.masses_me, mol.charge_array)
     S = 7 * 65536 + 777
-    pos = wl.sample_molecule(mol, S, seed=41).astype(np.float32)
+    if case == "nine_atoms_pair_streamed":  # an odd count: the second thread carries a phantom slot
+        rng = np.random.default_rng(909)
+        mass = rng.choice([1.008, 12.011, 14.007, 15.999, 32.06], 9) * wl.AMU_TO_ME
+        q = rng.integers(1, 4, 9).astype(float)
+        engine.set_molecule(mass, q)
+        pos = wl.sample_ball(rng, S, 9, 2.0 * 9 ** (1 / 3), 0.5).astype(np.float32)
+        lanes, mode = 0, 0
+    else:
+        mol, lanes, mode = {"ch4_thread_streamed": (wl.CH4, 0, 3), "c2h6_pair_streamed": (wl.C2H6_LIKE, 0, 0),
+                            "ch4_lane_chunked": (wl.CH4, 5, 3)}[case]
+        engine.set_molecule(mol.masses_me, mol.charge_array)
+        pos = wl.sample_molecule(mol, S, seed=41).astype(np.float32)
     cfg = cfg_for(ce, wl.TIGHT, mode)
     dev = torch.device("cuda", 0)
     x = torch.from_numpy(pos).to(dev)
