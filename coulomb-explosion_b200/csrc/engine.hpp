@@ -162,6 +162,15 @@ inline FixedKernelFn select_io_kernel(int n, int mode, bool pair) {
   }
 }
 
+inline PairBucketFn select_pair_bucket_kernel(int n, int mode) {
+  switch (mode & 3) {
+    case 0: return pair_bucket_kernel_m0(n);
+    case 1: return pair_bucket_kernel_m1(n);
+    case 2: return pair_bucket_kernel_m2(n);
+    default: return pair_bucket_kernel_m3(n);
+  }
+}
+
 inline AtomKernelFn select_atom_kernel(int n, int mode) {
   switch (mode & 3) {
     case 0: return atom_kernel_m0(n);

@@ -138,7 +138,23 @@ ce_tuning mixed_tuning(const ce_engine* e) {
   if (t.block_threads == 0) t.block_threads = a.valid && a.t.block_threads ? a.t.block_threads : 128;
   if (t.blocks_per_sm == 0 && a.valid) t.blocks_per_sm = a.t.blocks_per_sm;
   if (t.refill_threshold == 0 && a.valid) t.refill_threshold = a.t.refill_threshold;
+  if (t.lanes_per_sim == 0 && a.valid) t.lanes_per_sim = a.t.lanes_per_sim;
   return t;
+}
+
+// Whether the n-atom bucket runs two threads per sim (mixed lanes_per_sim = 2,
+// 3 or more atoms) rather than one lane per atom.
+bool pair_bucket(const ce_tuning& t, int n) { return t.lanes_per_sim == 2 && n >= 3; }
+
+// Dynamic shared memory above the default 48 KB, and all of the SM's unified
+// L1 / shared storage as shared memory, for a kernel that takes `smem` bytes.
+int prepare_smem(ce_engine* e, const void* fn, size_t smem) {
+  if (smem == 0) return CE_OK;
+  cudaError_t st = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaFuncSetAttribute(max dynamic shared memory)");
+  st = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaFuncSetAttribute(shared memory carveout)");
+  return CE_OK;
 }
 
 int check_mixed_args(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double k, const ce_run_config* cfg,
@@ -224,9 +240,11 @@ int run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double 
       return ce::fail(e, CE_ERR_INVALID, "ce_run_mixed_device_state: a state pointer is NULL");
   if (schedule != CE_SCHEDULE_ONE_LAUNCH && schedule != CE_SCHEDULE_PER_SIZE && schedule != CE_SCHEDULE_OVERLAP)
     return ce::fail(e, CE_ERR_INVALID, "ce_run_mixed: unknown schedule");
+  const ce_tuning t = mixed_tuning(e);
   // Saving and resuming integrator state is built into the per-size kernels only
-  // (in the one-launch kernel the extra registers cost 6 %).
-  if ((resume || save) && schedule == CE_SCHEDULE_ONE_LAUNCH) schedule = CE_SCHEDULE_PER_SIZE;
+  // (in the one-launch kernel the extra registers cost 6 %), and so are the
+  // two-thread buckets (lanes_per_sim = 2).
+  if ((resume || save || t.lanes_per_sim == 2) && schedule == CE_SCHEDULE_ONE_LAUNCH) schedule = CE_SCHEDULE_PER_SIZE;
   cudaError_t st = cudaSetDevice(e->device);
   if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaSetDevice");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -238,7 +256,6 @@ int run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double 
     if (rc != CE_OK) return rc;
   }
   const BucketTables T = tables_of(e->d_mixed);
-  const ce_tuning t = mixed_tuning(e);
 
   ce::RunParams P{};
   ce::fill_run_params(P, cfg, out, t.refill_threshold);  // 0: each size's default
@@ -306,18 +323,25 @@ int run_mixed_device(ce_engine* e, uint64_t S, const ce_mixed_batch* in, double 
     }
     for (int n = CE_MAX_ATOMS; n >= 2; --n) {
       const cudaStream_t sn = (overlap && (n & 1)) ? e->s_mix2 : s;
-      const ce::MixedKernelFn fn = ce::select_mixed_kernel(n, cfg->precision_mode);
+      const bool pair = pair_bucket(t, n);
+      const ce::MixedKernelFn fn = pair ? ce::select_pair_bucket_kernel(n, cfg->precision_mode)
+                                        : ce::select_mixed_kernel(n, cfg->precision_mode);
+      const int bn = pair ? ce::kPairBlock : block;
+      const size_t smem = pair ? ce::pair_smem_bytes(n, cfg->precision_mode) : 0;
+      rc = prepare_smem(e, reinterpret_cast<const void*>(fn), smem);
+      if (rc != CE_OK) return rc;
       int per_sm = t.blocks_per_sm;
       if (per_sm == 0) {
-        st = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, 0);
+        st = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, bn, smem);
         if (st != cudaSuccess) return ce::cuda_fail(e, st, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
         if (per_sm < 1) per_sm = 1;
       }
-      const uint64_t sims_per_block = static_cast<uint64_t>(block / 32) * (32 / n);
+      const uint64_t sims_per_block =
+          pair ? static_cast<uint64_t>(bn / 2) : static_cast<uint64_t>(bn / 32) * (32 / n);
       const uint64_t grid = std::min<uint64_t>(static_cast<uint64_t>(e->sms) * per_sm, (S + sims_per_block - 1) / sims_per_block);
       ce::RunParams Pn = P;
-      if (t.refill_threshold == 0) Pn.refill_threshold = ce::default_refill(n, n);
-      fn<<<static_cast<unsigned>(std::max<uint64_t>(grid, 1)), block, 0, sn>>>(Pn, X, B);
+      if (t.refill_threshold == 0) Pn.refill_threshold = ce::default_refill(n, pair ? 2 : n);
+      fn<<<static_cast<unsigned>(std::max<uint64_t>(grid, 1)), bn, smem, sn>>>(Pn, X, B);
       ++launches;
     }
     if (overlap) {
@@ -646,10 +670,15 @@ int ce_autotune_mixed(ce_engine* e, uint64_t S, const ce_mixed_batch* dev_in, do
   ce_tuning best_t{};
   int best_s = CE_SCHEDULE_ONE_LAUNCH;
   int count = 0;
-  for (int sch : schedules)
-    for (int B : blocks)
-      for (int R : refills) {
-        ce_tuning t{B, 0, R, 0};
+  // One lane per atom in every schedule and block size; two threads per sim
+  // (lanes 2: 3+ atoms; its buckets fix their block, the 2-atom bucket keeps
+  // 128 threads) in the two per-size schedules.
+  for (int L : {0, 2})
+    for (int sch : schedules)
+      for (int B : blocks)
+        for (int R : refills) {
+        if (L == 2 && (sch == CE_SCHEDULE_ONE_LAUNCH || B != ce::kAtomMaxBlock)) continue;
+        ce_tuning t{B, 0, R, L};
         e->tuning = t;
         double ms = 0.0;
         rc = time_call(e, [&] { return ce_run_mixed_device(e, S, dev_in, coulomb_k, cfg, &out.o, sch, e->stream); },

@@ -38,7 +38,6 @@
 
 namespace ce {
 
-constexpr int kMixedStride = CE_MAX_ATOMS;  // atoms per sim row in the mixed layout
 // Largest block of the lane-per-atom kernels. Declaring it as the launch bound
 // lets the register allocator size for 128-thread blocks (N = 5: 92 registers,
 // 5 blocks per SM) instead of for 256-thread ones (80 registers with spills, so
@@ -117,23 +116,6 @@ struct AtomShape {
 struct AtomConsts {
   float inv_m;   // 1 / m_i
   double mass;   // m_i
-};
-
-// Per-sim molecule arrays of the mixed layout (rows of kMixedStride atoms).
-struct MixedIn {
-  const uint8_t* n_per;   // [S] atoms per sim
-  const double* mass;     // [S][10] electron masses
-  const double* charge;   // [S][10]
-  double coulomb_k;
-};
-
-// Size buckets produced by the device counting sort (ce_gpu.cu): sims of size n
-// are perm[off[n] .. off[n] + cnt[n]); cursor[n] is that bucket's work queue.
-struct Buckets {
-  const uint32_t* perm;
-  const unsigned long long* off;  // [11]
-  const unsigned long long* cnt;  // [11]
-  unsigned long long* cursor;     // [11]
 };
 
 // Fixed-order sum over the N lanes [base, base + N) of a group; every lane of

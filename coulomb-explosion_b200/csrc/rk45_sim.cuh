@@ -129,6 +129,32 @@ struct RunParams {
   unsigned io_shift;  // chunks of 2^io_shift sims
 };
 
+constexpr int kMixedStride = CE_MAX_ATOMS;  // atoms per sim row in the mixed layout
+
+// Per-sim molecule arrays of the mixed layout (rows of kMixedStride atoms).
+struct MixedIn {
+  const uint8_t* n_per;   // [S] atoms per sim
+  const double* mass;     // [S][10] electron masses
+  const double* charge;   // [S][10]
+  double coulomb_k;
+};
+
+// Size buckets produced by the device counting sort (mixed.cu): sims of size n
+// are perm[off[n] .. off[n] + cnt[n]); cursor[n] is that bucket's work queue.
+struct Buckets {
+  const uint32_t* perm;
+  const unsigned long long* off;  // [11]
+  const unsigned long long* cnt;  // [11]
+  unsigned long long* cursor;     // [11]
+};
+
+// Variants of the thread-per-sim / two-thread loop (template flags):
+//   kLoopIO     streamed host-buffer I/O (RunParams io_*)
+//   kLoopMixed  a mixed batch: rows of kMixedStride atoms, each sim's masses and
+//               charges from its row (two threads per sim only)
+//   kLoopState  saved / resumed integrator state (RunParams save_* / res_*)
+constexpr int kLoopIO = 1, kLoopMixed = 2, kLoopState = 4;
+
 
 // Packed-FP32x2 helpers (sm_100: FFMA2 / FMUL2 / FADD2; every element rounds
 // exactly like the scalar instruction) and the approximate MUFU forms.
@@ -342,6 +368,49 @@ __device__ __forceinline__ void load_pair_consts(PairConsts<N>& C, const FixedMo
   for (int a = 0; a < A; ++a) C.inv_m[a] = (o + a < N) ? M.inv_m[o + a] : 1.0f;
 }
 
+// The same constants for mixed-batch sim `sim`, from its row: k q_i q_j formed
+// in double and narrowed, 1/m narrowed, as ce_set_molecule forms them for the
+// fixed path. C.half and C.pmask are already set.
+template <int N>
+__device__ __forceinline__ void load_pair_consts_mixed(PairConsts<N>& C, const MixedIn& X, unsigned long long sim) {
+  constexpr int A = PairConsts<N>::A;
+  const int o = C.half * A, po = (1 - C.half) * A;
+  const double* q = X.charge + sim * kMixedStride;
+  const double* m = X.mass + sim * kMixedStride;
+  double qo[A], qp[A];
+#pragma unroll
+  for (int a = 0; a < A; ++a) {
+    qo[a] = (o + a < N) ? __ldg(q + o + a) : 0.0;
+    qp[a] = (po + a < N) ? __ldg(q + po + a) : 0.0;
+    C.inv_m[a] = (o + a < N) ? static_cast<float>(1.0 / __ldg(m + o + a)) : 1.0f;
+  }
+  int k = 0;
+#pragma unroll
+  for (int i = 0; i < A; ++i)
+#pragma unroll
+    for (int j = 0; j < A; ++j) {
+      if (j <= i) continue;
+      C.pcI[k++] = static_cast<float>(X.coulomb_k * qo[i] * qo[j]);
+    }
+  k = 0;
+#pragma unroll
+  for (int b = 0; b < A; ++b)
+#pragma unroll
+    for (int d = 0; d < A; ++d) {
+      if (!pair_cross(A, b, d)) continue;
+      C.pcX[k++] = static_cast<float>(X.coulomb_k * qo[(b - d + A) % A] * qp[b]);
+    }
+}
+
+// m_i (double) of atom i of sim `sim`.
+template <bool MIXED>
+__device__ __forceinline__ double sim_mass(const FixedMol& M, const MixedIn& X, unsigned long long sim, int i) {
+  if constexpr (MIXED)
+    return __ldg(X.mass + sim * kMixedStride + i);
+  else
+    return M.mass[i];
+}
+
 // a for this thread's A atoms in the two-thread layout: its own pairs as in
 // thread_forces, then the cross pairs partner slot by partner slot: the
 // partner's position of slot b arrives by three shuffles, the pairs
@@ -488,15 +557,27 @@ __device__ __forceinline__ void store_record(float* dst, const float (&v)[L]) {
   }
 }
 
+// Flat float f of the 16-byte-chunked stage slot `slot` of this thread (B
+// threads per block).
+template <int NC, int B>
+__device__ __forceinline__ float slot_float(const float4* ks, int slot, int f) {
+  return reinterpret_cast<const float*>(ks + (slot * NC + (f >> 2)) * B)[f & 3];
+}
+
 // FP64 finalize: KE, s = sqrt(E0/KE), p_i = (m_i s) v_i, KER = s^2 KE; then the
-// per-sim output record. A converged sim with non-finite momenta is
-// CE_SIM_NONFINITE. In the two-thread layout each thread writes its own atoms'
-// momenta (the record from atom h A on) and thread 0 the per-sim scalars.
-template <int N, int MODE, int T>
+// per-sim output record (rows of N atoms, or kMixedStride in a mixed batch)
+// and, with kLoopState, the integrator state the sim stopped in (RunParams
+// save_*). A converged sim with non-finite momenta is CE_SIM_NONFINITE. In the
+// two-thread layout each thread writes its own atoms' rows and thread 0 the
+// per-sim scalars.
+template <int N, int MODE, int T, int F>
 __device__ __forceinline__ void thread_finalize(const ThreadSim<N, MODE, T>& s, int status, double pe_final,
-                                                const RunParams& P, const FixedMol& M, const SimConsts<N, T>& C) {
+                                                const RunParams& P, const FixedMol& M, const MixedIn& X,
+                                                const SimConsts<N, T>& C, const float4* ks) {
   constexpr int A = SimShape<N, T>::A;
   constexpr int NP = SimShape<N, T>::NP;
+  constexpr bool MIXED = (F & kLoopMixed) != 0;
+  constexpr int STRIDE = MIXED ? kMixedStride : N;
   int half = 0;
   if constexpr (T == 2) half = C.half;
   const int o = half * A;  // first atom of this thread
@@ -506,7 +587,7 @@ __device__ __forceinline__ void thread_finalize(const ThreadSim<N, MODE, T>& s, 
   for (int i = 0; i < A; ++i) {
     if (!sim_real<N, T>(2 * i, half)) continue;
     const double vx = s.v[i].x, vy = s.v[i].y, vz = flc<NP>(s.v, 2 * A + i);
-    ke += 0.5 * M.mass[o + i] * (vx * vx + vy * vy + vz * vz);
+    ke += 0.5 * sim_mass<MIXED>(M, X, s.sim, o + i) * (vx * vx + vy * vy + vz * vz);
     finite = finite && isfinite(vx) && isfinite(vy) && isfinite(vz);
   }
   if constexpr (T == 2) {
@@ -522,16 +603,16 @@ __device__ __forceinline__ void thread_finalize(const ThreadSim<N, MODE, T>& s, 
   float pm[3 * A];
 #pragma unroll
   for (int i = 0; i < A; ++i) {
-    const double mm = M.mass[o + i] * sc;
+    const double mm = (sim_real<N, T>(2 * i, half) ? sim_mass<MIXED>(M, X, s.sim, o + i) : 0.0) * sc;
     pm[i * 3 + 0] = static_cast<float>(mm * static_cast<double>(s.v[i].x));
     pm[i * 3 + 1] = static_cast<float>(mm * static_cast<double>(s.v[i].y));
     pm[i * 3 + 2] = static_cast<float>(mm * static_cast<double>(flc<NP>(s.v, 2 * A + i)));
   }
-  float* dst = P.momenta + s.sim * (3ull * N) + 3 * o;
+  const unsigned long long row = s.sim * (3ull * STRIDE) + 3 * o;  // this thread's first float of the sim's rows
   if (SimShape<N, T>::kPhantom && half == 1)
-    store_record<3 * (A - 1)>(dst, pm);
+    store_record<3 * (A - 1)>(P.momenta + row, pm);
   else
-    store_record<3 * A>(dst, pm);
+    store_record<3 * A>(P.momenta + row, pm);
   if (half == 0) {
     if (P.ker) P.ker[s.sim] = (sc * sc) * ke;
     if (P.steps) P.steps[s.sim] = s.steps;
@@ -543,13 +624,44 @@ __device__ __forceinline__ void thread_finalize(const ThreadSim<N, MODE, T>& s, 
     if (P.e0) P.e0[s.sim] = e0d;
   }
   if (P.positions) {
-    float* xp = P.positions + s.sim * (3ull * N) + 3 * o;
 #pragma unroll
     for (int i = 0; i < A; ++i) {
       if (!sim_real<N, T>(2 * i, half)) continue;
-      xp[i * 3 + 0] = s.x[i].x;
-      xp[i * 3 + 1] = s.x[i].y;
-      xp[i * 3 + 2] = flc<NP>(s.x, 2 * A + i);
+      P.positions[row + i * 3 + 0] = s.x[i].x;
+      P.positions[row + i * 3 + 1] = s.x[i].y;
+      P.positions[row + i * 3 + 2] = flc<NP>(s.x, 2 * A + i);
+    }
+  }
+  if constexpr ((F & kLoopState) != 0) {
+    if (P.save_h) {  // the integrator state this sim stopped in (a resumable run's input)
+      constexpr int NC = SimShape<N, T>::NC;
+      constexpr int B = sim_block<N, T>();
+#pragma unroll
+      for (int i = 0; i < A; ++i) {
+        if (!sim_real<N, T>(2 * i, half)) continue;
+        P.save_pos[row + i * 3 + 0] = s.x[i].x;
+        P.save_pos[row + i * 3 + 1] = s.x[i].y;
+        P.save_pos[row + i * 3 + 2] = flc<NP>(s.x, 2 * A + i);
+        P.save_vel[row + i * 3 + 0] = s.v[i].x;
+        P.save_vel[row + i * 3 + 1] = s.v[i].y;
+        P.save_vel[row + i * 3 + 2] = flc<NP>(s.v, 2 * A + i);
+        if (ThreadSim<N, MODE, T>::kKahan && P.save_comp) {
+          float* c = P.save_comp + s.sim * (6ull * STRIDE) + 6 * (o + i);
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            const int f = flat_of(A, i, k);
+            c[k] = slot_float<NC, B>(ks, s.cxs, f);
+            c[3 + k] = slot_float<NC, B>(ks, s.cvs, f);
+          }
+        }
+      }
+      if (half == 0) {
+        P.save_h[s.sim] = status == CE_SIM_OK ? s.h : 0.0f;
+        P.save_t[s.sim] = static_cast<double>(s.t);
+        P.save_steps[s.sim] = s.steps;
+        P.save_rejects[s.sim] = s.rejects;
+        P.save_e0[s.sim] = e0d;
+      }
     }
   }
 }
@@ -559,19 +671,34 @@ __device__ __forceinline__ void thread_finalize(const ThreadSim<N, MODE, T>& s, 
 // term is 0, sv = atol, and the probe accelerations equal k1; its quotients use
 // the fast forms, as the initial step is a heuristic). Returns false when the
 // sim is already finished (written out). In the two-thread layout both
-// threads of the pair run it for their own atoms.
-template <int N, int MODE, int T, bool IO>
+// threads of the pair run it for their own atoms. In a mixed batch
+// (kLoopMixed) the sim's constants come from its row of X (C is reloaded);
+// with kLoopState a sim whose res_h > 0 resumes its saved state instead
+// (positions, velocities, compensation, step size, clock, counters, E_0): its
+// k1 = a(x) is bit for bit the k7 of the accepted step the state follows, and
+// the driver's stop test runs again on the current potential
+// (src/driver.cpp:19-30), as the uninterrupted run would.
+template <int N, int MODE, int T, int F>
 __device__ __forceinline__ bool thread_init(ThreadSim<N, MODE, T>& s, unsigned long long sim, const RunParams& P,
-                                            const FixedMol& M, const SimConsts<N, T>& C, float4* ks, int B) {
+                                            const FixedMol& M, const MixedIn& X, SimConsts<N, T>& C, float4* ks,
+                                            int B) {
   using S = ThreadSim<N, MODE, T>;
   using Acc = typename S::Acc;
   constexpr int A = SimShape<N, T>::A;
   constexpr int NP = SimShape<N, T>::NP;
   constexpr int NC = SimShape<N, T>::NC;
+  constexpr bool IO = (F & kLoopIO) != 0;
+  constexpr bool MIXED = (F & kLoopMixed) != 0;
+  constexpr bool STATE = (F & kLoopState) != 0;
+  constexpr int STRIDE = MIXED ? kMixedStride : N;
+  static_assert(!MIXED || T == 2, "mixed batches run the two-thread layout here");
   int half = 0;
   if constexpr (T == 2) half = C.half;
   s.sim = sim;
-  const float* src = P.pos + sim * (3ull * N) + 3 * (half * A);
+  bool resumed = false;
+  if constexpr (STATE) resumed = P.res_h != nullptr && __ldg(P.res_h + sim) > 0.0f;
+  const unsigned long long row = sim * (3ull * STRIDE) + 3 * (half * A);
+  const float* src = (resumed ? P.res_pos : P.pos) + row;
 #pragma unroll
   for (int p = 0; p < NP; ++p) s.x[p] = s.v[p] = make_float2(0.0f, 0.0f);
 #pragma unroll
@@ -588,15 +715,44 @@ __device__ __forceinline__ bool thread_init(ThreadSim<N, MODE, T>& s, unsigned l
       fl_set<NP>(s.x, 2 * A + i, __ldg(src + 3 * i + 2));
     }
   }
-  if (S::kKahan) {  // compensation terms start at zero
-    s.cxs = 7;
-    s.cvs = 9;
+  if constexpr (STATE) {
+    if (resumed) {
 #pragma unroll
-    for (int c = 0; c < NC; ++c) {
-      ks[(7 * NC + c) * B] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-      ks[(9 * NC + c) * B] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      for (int i = 0; i < A; ++i) {
+        if (!sim_real<N, T>(2 * i, half)) continue;
+        const float* vs = P.res_vel + row;
+        s.v[i] = make_float2(__ldg(vs + 3 * i), __ldg(vs + 3 * i + 1));
+        fl_set<NP>(s.v, 2 * A + i, __ldg(vs + 3 * i + 2));
+      }
     }
   }
+  if (S::kKahan) {  // compensation terms start at zero (or from the saved state)
+    s.cxs = 7;
+    s.cvs = 9;
+    float2 cx[NP], cv[NP];
+#pragma unroll
+    for (int p = 0; p < NP; ++p) cx[p] = cv[p] = make_float2(0.0f, 0.0f);
+    if constexpr (STATE) {
+      if (resumed) {
+#pragma unroll
+        for (int i = 0; i < A; ++i) {
+          if (!sim_real<N, T>(2 * i, half)) continue;
+          const float* c = P.res_comp + sim * (6ull * STRIDE) + 6 * (half * A + i);
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            fl_set<NP>(cx, flat_of(A, i, k), __ldg(c + k));
+            fl_set<NP>(cv, flat_of(A, i, k), __ldg(c + 3 + k));
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      ks[(7 * NC + c) * B] = make_float4(cx[2 * c].x, cx[2 * c].y, cx[2 * c + 1].x, cx[2 * c + 1].y);
+      ks[(9 * NC + c) * B] = make_float4(cv[2 * c].x, cv[2 * c].y, cv[2 * c + 1].x, cv[2 * c + 1].y);
+    }
+  }
+  if constexpr (MIXED) load_pair_consts_mixed<N>(C, X, sim);
   Acc pe0 = Acc(0);
   float2 k0[NP];
   sim_forces<N, T, Acc>(s.x, k0, M, C, true, pe0);
@@ -605,6 +761,29 @@ __device__ __forceinline__ bool thread_init(ThreadSim<N, MODE, T>& s, unsigned l
 #pragma unroll
   for (int c = 0; c < NC; ++c)
     ks[(5 * NC + c) * B] = make_float4(k0[2 * c].x, k0[2 * c].y, k0[2 * c + 1].x, k0[2 * c + 1].y);
+  if constexpr (STATE) {
+    if (resumed) {
+      s.h = __ldg(P.res_h + sim);
+      s.t = static_cast<Acc>(P.res_t[sim]);
+      s.steps = P.res_steps[sim];
+      s.rejects = P.res_rejects[sim];
+      s.rej_in_step = 0u;
+      s.rej_once = false;
+      s.e0 = static_cast<Acc>(P.res_e0[sim]);
+      if (S::kF64)
+        s.pe_stop = static_cast<Acc>(P.pe_stop_d * static_cast<double>(s.e0));
+      else
+        s.pe_stop = static_cast<Acc>(P.pe_stop_f * static_cast<float>(s.e0));
+      int fin = -1;
+      if (!(pe0 > s.pe_stop)) fin = CE_SIM_OK;
+      else if (s.steps >= P.max_steps) fin = CE_SIM_MAX_STEPS;
+      if (fin >= 0) {
+        thread_finalize<N, MODE, T, F>(s, fin, static_cast<double>(pe0), P, M, X, C, ks);
+        return false;
+      }
+      return true;
+    }
+  }
   s.t = Acc(0);
   s.steps = s.rejects = s.rej_in_step = 0u;
   s.rej_once = false;
@@ -618,7 +797,7 @@ __device__ __forceinline__ bool thread_init(ThreadSim<N, MODE, T>& s, unsigned l
   else if (!(pe0 > s.pe_stop)) fin = CE_SIM_OK;  // already at or below the stop (driver.cpp:19)
   else if (P.max_steps == 0u) fin = CE_SIM_MAX_STEPS;
   if (fin >= 0) {
-    thread_finalize<N, MODE, T>(s, fin, static_cast<double>(pe0), P, M, C);
+    thread_finalize<N, MODE, T, F>(s, fin, static_cast<double>(pe0), P, M, X, C, ks);
     return false;
   }
   float d0_sq = 0.0f, d1_sq = 0.0f;
@@ -662,9 +841,9 @@ __device__ __forceinline__ bool thread_init(ThreadSim<N, MODE, T>& s, unsigned l
 // chunk in shared memory; chunk c of stage slot l is ks[(l * NC + c) * B], B =
 // sim_block<N, T>(), so every slot offset is an immediate.
 // Returns false once the sim is finished and written out.
-template <int N, int MODE, int T>
+template <int N, int MODE, int T, int F>
 __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE, T>& s, const RunParams& P, const FixedMol& M,
-                                               const SimConsts<N, T>& C, float4* ks) {
+                                               const MixedIn& X, const SimConsts<N, T>& C, float4* ks) {
   using S = ThreadSim<N, MODE, T>;
   using Acc = typename S::Acc;
   constexpr int NC = SimShape<N, T>::NC;
@@ -833,7 +1012,7 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE, T>& s, const R
     if (!(pe_new > s.pe_stop)) fin = CE_SIM_OK;
     else if (s.steps >= P.max_steps) fin = CE_SIM_MAX_STEPS;
     if (fin >= 0) {
-      thread_finalize<N, MODE, T>(s, fin, static_cast<double>(pe_new), P, M, C);
+      thread_finalize<N, MODE, T, F>(s, fin, static_cast<double>(pe_new), P, M, X, C, ks);
       return false;
     }
     return true;
@@ -843,7 +1022,7 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE, T>& s, const R
   s.rejects += 1u;
   s.rej_in_step += 1u;
   if (s.rej_in_step > static_cast<uint32_t>(kMaxRejections)) {
-    thread_finalize<N, MODE, T>(s, CE_SIM_REJECT_LIMIT, static_cast<double>(pe_new), P, M, C);
+    thread_finalize<N, MODE, T, F>(s, CE_SIM_REJECT_LIMIT, static_cast<double>(pe_new), P, M, X, C, ks);
     return false;
   }
   return true;
@@ -908,21 +1087,32 @@ __device__ __forceinline__ void io_count(const RunParams& P, bool fin, unsigned 
   }
 }
 
-// Persistent loop: each warp keeps its sims busy by pulling sim indices from a
-// global cursor (one warp-aggregated atomicAdd per refill) whenever at least
-// `refill_threshold` of its sims are idle (or all of them). A sim is one lane
-// (T = 1, 32 sims a warp) or one even/odd lane pair (T = 2, 16 sims a warp; the
-// pair's lanes are always active or idle together). With IO the claimed sims'
-// inputs are awaited (io_wait_input) and finished sims are counted (io_count).
-template <int N, int MODE, int T, bool IO>
-__device__ __forceinline__ void fixed_loop(const RunParams& P, const FixedMol& M) {
+// Persistent loop: each warp keeps its sims busy by pulling sim indices from the
+// work queue `cursor` over [0, count) (mapped through perm when non-null; one
+// warp-aggregated atomicAdd per refill) whenever at least `refill` of its sims
+// are idle (or all of them). A sim is one lane (T = 1, 32 sims a warp) or one
+// even/odd lane pair (T = 2, 16 sims a warp; the pair's lanes are always active
+// or idle together). With kLoopIO the claimed sims' inputs are awaited
+// (io_wait_input) and finished sims are counted (io_count).
+template <int N, int MODE, int T, int F>
+__device__ __forceinline__ void sim_loop(const RunParams& P, const FixedMol& M, const MixedIn& X,
+                                         unsigned long long* cursor, unsigned long long count, const uint32_t* perm,
+                                         int refill) {
+  constexpr bool IO = (F & kLoopIO) != 0;
   extern __shared__ float4 ce_stage_slots[];
   ThreadSim<N, MODE, T> s;
   SimConsts<N, T> C;
   bool active = false;
-  bool queue_empty = false;
+  bool queue_empty = count == 0ull;
   const unsigned lane = threadIdx.x & 31u;
-  if constexpr (T == 2) load_pair_consts<N>(C, M, lane);
+  if constexpr (T == 2) {
+    if constexpr ((F & kLoopMixed) != 0) {  // per-sim constants are loaded at each claim
+      C.half = static_cast<int>(lane & 1u);
+      C.pmask = 3u << (lane & 30u);
+    } else {
+      load_pair_consts<N>(C, M, lane);
+    }
+  }
   constexpr unsigned kSimLanes = T == 2 ? 0x55555555u : 0xffffffffu;  // one lane per sim
   const unsigned first = T == 2 ? (lane & ~1u) : lane;                // this sim's first lane
   const unsigned lt_mask = (1u << first) - 1u;
@@ -938,20 +1128,20 @@ __device__ __forceinline__ void fixed_loop(const RunParams& P, const FixedMol& M
     const unsigned idle_s = idle & kSimLanes;
     bool fin = false;  // IO: this thread's sim finished at its claim
     unsigned long long fin_sim = 0ull;
-    if (!queue_empty && idle != 0u && (idle == 0xffffffffu || __popc(idle_s) >= P.refill_threshold)) {
+    if (!queue_empty && idle != 0u && (idle == 0xffffffffu || __popc(idle_s) >= refill)) {
       const int cnt = __popc(idle_s);
       const int leader = __ffs(idle_s) - 1;
       unsigned long long base = 0ull;
-      if (static_cast<int>(lane) == leader) base = atomicAdd(P.cursor, static_cast<unsigned long long>(cnt));
+      if (static_cast<int>(lane) == leader) base = atomicAdd(cursor, static_cast<unsigned long long>(cnt));
       base = __shfl_sync(0xffffffffu, base, leader);
-      queue_empty = (base + static_cast<unsigned long long>(cnt) >= P.S);
+      queue_empty = (base + static_cast<unsigned long long>(cnt) >= count);
       bool in_ok = true;
       if constexpr (IO) {
         // The claimed range's inputs. Chunks arrive in order, so the wait is for
         // its last chunk, and only for chunks this warp has not yet seen present
         // (an acquire per refill cost the kernel ~8 %).
-        if (base < P.S) {
-          const unsigned long long last = (base + cnt < P.S ? base + cnt : P.S) - 1ull;
+        if (base < count) {
+          const unsigned long long last = (base + cnt < count ? base + cnt : count) - 1ull;
           const unsigned lc = static_cast<unsigned>(last >> P.io_shift);
           if (lc >= io_known) {
             if (static_cast<int>(lane) == leader) in_ok = io_wait_input(P.io_ready + lc, P.io_abort, P.io_error);
@@ -961,10 +1151,11 @@ __device__ __forceinline__ void fixed_loop(const RunParams& P, const FixedMol& M
         }
       }
       if (!active) {
-        const unsigned long long sim = base + static_cast<unsigned long long>(__popc(idle_s & lt_mask));
-        if (sim < P.S) {
+        const unsigned long long k = base + static_cast<unsigned long long>(__popc(idle_s & lt_mask));
+        if (k < count) {
+          const unsigned long long sim = perm ? static_cast<unsigned long long>(perm[k]) : k;
           if (in_ok) {
-            active = thread_init<N, MODE, T, IO>(s, sim, P, M, C, ks, B);
+            active = thread_init<N, MODE, T, F>(s, sim, P, M, X, C, ks, B);
           } else if (P.status && lane == first) {
             P.status[sim] = static_cast<uint8_t>(CE_SIM_BAD_INPUT);
           }
@@ -980,7 +1171,7 @@ __device__ __forceinline__ void fixed_loop(const RunParams& P, const FixedMol& M
     }
     bool done = false;
     if (active) {
-      active = thread_attempt<N, MODE, T>(s, P, M, C, ks);
+      active = thread_attempt<N, MODE, T, F>(s, P, M, X, C, ks);
       done = !active;
     }
     if constexpr (IO) io_count<T>(P, done, s.sim);
@@ -992,7 +1183,8 @@ __device__ __forceinline__ void fixed_loop(const RunParams& P, const FixedMol& M
 template <int N, int MODE>
 __global__ void __launch_bounds__(thread_block(N), (thread_min_blocks<N, MODE>()))
     rk45_fixed_kernel(const RunParams P, const FixedMol M) {
-  fixed_loop<N, MODE, 1, false>(P, M);
+  const MixedIn none{};
+  sim_loop<N, MODE, 1, 0>(P, M, none, P.cursor, P.S, nullptr, P.refill_threshold);
 }
 
 // Two threads per sim (N >= 3): kPairBlock threads per block and
@@ -1000,19 +1192,33 @@ __global__ void __launch_bounds__(thread_block(N), (thread_min_blocks<N, MODE>()
 template <int N, int MODE>
 __global__ void __launch_bounds__(kPairBlock, (pair_min_blocks<N, MODE>()))
     rk45_pair_kernel(const RunParams P, const FixedMol M) {
-  fixed_loop<N, MODE, 2, false>(P, M);
+  const MixedIn none{};
+  sim_loop<N, MODE, 2, 0>(P, M, none, P.cursor, P.S, nullptr, P.refill_threshold);
 }
 
 // The same two kernels with streamed host-buffer I/O (RunParams io_*).
 template <int N, int MODE>
 __global__ void __launch_bounds__(thread_block(N), (thread_min_blocks<N, MODE>()))
     rk45_fixed_io_kernel(const RunParams P, const FixedMol M) {
-  fixed_loop<N, MODE, 1, true>(P, M);
+  const MixedIn none{};
+  sim_loop<N, MODE, 1, kLoopIO>(P, M, none, P.cursor, P.S, nullptr, P.refill_threshold);
 }
 template <int N, int MODE>
 __global__ void __launch_bounds__(kPairBlock, (pair_min_blocks<N, MODE>()))
     rk45_pair_io_kernel(const RunParams P, const FixedMol M) {
-  fixed_loop<N, MODE, 2, true>(P, M);
+  const MixedIn none{};
+  sim_loop<N, MODE, 2, kLoopIO>(P, M, none, P.cursor, P.S, nullptr, P.refill_threshold);
+}
+
+// One size bucket of a mixed batch in the two-thread layout (the per-size
+// schedule with mixed lanes_per_sim = 2), with saved / resumed integrator state
+// (RunParams save_* / res_*); launched like rk45_pair_kernel.
+template <int N, int MODE>
+__global__ void __launch_bounds__(kPairBlock, (pair_min_blocks<N, MODE>()))
+    rk45_pair_bucket_kernel(const RunParams P, const MixedIn X, const Buckets B) {
+  const FixedMol none{};
+  sim_loop<N, MODE, 2, kLoopMixed | kLoopState>(P, none, X, B.cursor + N, B.cnt[N], B.perm + B.off[N],
+                                                P.refill_threshold);
 }
 
 using FixedKernelFn = void (*)(RunParams, FixedMol);
@@ -1032,5 +1238,11 @@ FixedKernelFn io_kernel_m0(int n, bool pair);
 FixedKernelFn io_kernel_m1(int n, bool pair);
 FixedKernelFn io_kernel_m2(int n, bool pair);
 FixedKernelFn io_kernel_m3(int n, bool pair);
+// The mixed-batch two-thread bucket kernels, N = 3..10 (nullptr otherwise).
+using PairBucketFn = void (*)(RunParams, MixedIn, Buckets);
+PairBucketFn pair_bucket_kernel_m0(int n);
+PairBucketFn pair_bucket_kernel_m1(int n);
+PairBucketFn pair_bucket_kernel_m2(int n);
+PairBucketFn pair_bucket_kernel_m3(int n);
 
 }  // namespace ce

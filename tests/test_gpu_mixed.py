@@ -23,16 +23,26 @@ def tight(ce, wl, mode=3, **kw):
 
 
 def per_sim_err(r, ref, n_per):
+    return per_sim_err_arrays(r.momenta, ref, n_per)
+
+
+def per_sim_err_arrays(p, ref, n_per):
     errs = []
     for s, n in enumerate(n_per):
-        errs.append(ol.config_norm_error(r.momenta[s:s + 1, :n], ref[s:s + 1, :n])[0])
+        errs.append(ol.config_norm_error(p[s:s + 1, :n], ref[s:s + 1, :n])[0])
     return np.array(errs)
 
 
+@pytest.mark.parametrize("lanes", [0, 2])
 @pytest.mark.parametrize("bits", [32, 64])
-def test_mixed_golden_matches_reference_engine(engine, ce, wl, golden_mixed, bits):
+def test_mixed_golden_matches_reference_engine(engine, ce, wl, golden_mixed, bits, lanes):
+    # lanes 0: one lane per atom (the default); 2: two threads per sim from 3 atoms
     g = golden_mixed
-    r = engine.run_mixed(g["n_per"], g["masses"], g["charges"], g["pos"], tight(ce, wl))
+    engine.set_tuning(lanes_per_sim=lanes)
+    try:
+        r = engine.run_mixed(g["n_per"], g["masses"], g["charges"], g["pos"], tight(ce, wl))
+    finally:
+        engine.set_tuning()
     assert (r.status == 0).all()
     err = per_sim_err(r, g[f"p_tight_f{bits}"], g["n_per"])
     assert err.max() <= TIGHT_MAX, err.max()
@@ -72,6 +82,34 @@ def test_mixed_equals_fixed_molecule_path(engine, ce, wl):
     finally:
         engine.set_tuning()
     np.testing.assert_array_equal(rm.momenta[:, :5], rf.momenta)
+    np.testing.assert_array_equal(rm.steps, rf.steps)
+    np.testing.assert_array_equal(rm.ker, rf.ker)
+
+
+@pytest.mark.parametrize("molecule", ["CH4", "C2H6_LIKE"])
+def test_mixed_pair_layout_equals_fixed_pair_path(engine, ce, wl, molecule):
+    # With two threads per sim in both, a mixed batch of one molecule equals the
+    # fixed-molecule path bit for bit (same pair constants, same arithmetic;
+    # CH4's 5 atoms put a phantom in the second thread).
+    mol = getattr(wl, molecule)
+    S, n = 3000, mol.n
+    posn = wl.sample_molecule(mol, S, seed=37).astype(np.float32)
+    n_per = np.full(S, n, np.uint8)
+    m = np.ones((S, 10))
+    q = np.zeros((S, 10))
+    m[:, :n] = mol.masses_me
+    q[:, :n] = mol.charge_array
+    pos = np.zeros((S, 10, 3), np.float32)
+    pos[:, :n] = posn
+    engine.set_tuning(lanes_per_sim=2)
+    try:
+        rm = engine.run_mixed(n_per, m, q, pos, tight(ce, wl, 0))
+        engine.set_molecule(mol.masses_me, mol.charge_array)
+        rf = engine.run(posn, tight(ce, wl, 0))
+    finally:
+        engine.set_tuning()
+    assert (rm.status == 0).all()
+    np.testing.assert_array_equal(rm.momenta[:, :n], rf.momenta)
     np.testing.assert_array_equal(rm.steps, rf.steps)
     np.testing.assert_array_equal(rm.ker, rf.ker)
 
@@ -161,8 +199,19 @@ def test_full_size_mixed_invariants(engine, ce, wl):
     assert 30.0 < float(steps.double().mean()) < 70.0
 
 
-def test_schedules_and_graph_replay_are_bit_identical(engine, ce, wl):
+@pytest.mark.parametrize("lanes", [0, 2])
+def test_schedules_and_graph_replay_are_bit_identical(engine, ce, wl, lanes):
+    # lanes 2 (two threads per sim from 3 atoms) runs the one-launch request as
+    # the per-size schedule
     torch = pytest.importorskip("torch")
+    engine.set_tuning(lanes_per_sim=lanes)
+    try:
+        _schedules_and_graph_replay(engine, ce, wl, torch)
+    finally:
+        engine.set_tuning()
+
+
+def _schedules_and_graph_replay(engine, ce, wl, torch):
     S = 5000
     n_per, m, q, pos = wl.sample_mixed(S, seed=34)
     keep, batch = _device_batch(torch, ce, n_per, m, q, pos)
@@ -217,17 +266,26 @@ def test_autotuner_picks_a_measured_candidate_and_keeps_results(ce, wl):
     keep, batch = _device_batch(torch, ce, n_per, m, q, pos)
     cfg = tight(ce, wl)
     stream = torch.cuda.Stream()
-    d0, o0 = _device_out(torch, ce, S)
-    engine.run_mixed_device(S, batch, cfg, o0, ce.CE_SCHEDULE_ONE_LAUNCH, stream.cuda_stream)
-    stream.synchronize()
     report, best = engine.autotune_mixed(S, batch, cfg)
-    # 3 schedules x 3 block sizes x 4 refill thresholds (0 = each size's default)
-    assert len(report) == 36 and all(r["sims_per_s"] > 0 for r in report)
+    # one lane per atom: 3 schedules x 3 block sizes x 4 refill thresholds (0 =
+    # each size's default); two threads per sim: the 2 per-size schedules x 4
+    assert len(report) == 44 and all(r["sims_per_s"] > 0 for r in report)
+    assert {r["lanes_per_sim"] for r in report} == {0, 2}
     assert best in (ce.CE_SCHEDULE_ONE_LAUNCH, ce.CE_SCHEDULE_PER_SIZE, ce.CE_SCHEDULE_OVERLAP)
     d1, o1 = _device_out(torch, ce, S)
     engine.run_mixed_device(S, batch, cfg, o1, best, stream.cuda_stream)
     stream.synchronize()
-    np.testing.assert_array_equal(d1["m"].cpu().numpy(), d0["m"].cpu().numpy())
+    # the picked layout's results: bit for bit what that layout gives with any
+    # launch shape and schedule (both layouts' parity: the golden tests above)
+    best_r = max(report, key=lambda r: r["sims_per_s"])
+    engine.set_tuning(lanes_per_sim=best_r["lanes_per_sim"])
+    try:
+        d2, o2 = _device_out(torch, ce, S)
+        engine.run_mixed_device(S, batch, cfg, o2, ce.CE_SCHEDULE_PER_SIZE, stream.cuda_stream)
+        stream.synchronize()
+    finally:
+        engine.set_tuning()
+    np.testing.assert_array_equal(d1["m"].cpu().numpy(), d2["m"].cpu().numpy())
     # fixed path
     mol = wl.CH4
     engine.set_molecule(mol.masses_me, mol.charge_array)
@@ -257,14 +315,24 @@ def _state(torch, ce, S):
     return d, st
 
 
+@pytest.mark.parametrize("lanes", [0, 2])
 @pytest.mark.parametrize("schedule", ["one", "per_size", "overlap"])
 @pytest.mark.parametrize("mode", [0, 1, 2, 3])
-def test_saved_state_resumes_bit_for_bit(engine, ce, wl, mode, schedule):
+def test_saved_state_resumes_bit_for_bit(engine, ce, wl, mode, schedule, lanes):
     """A run to a loose stop that saves each sim's integrator state, then a run
     that continues from it, equals one uninterrupted run bit for bit (momenta,
     KER, steps, rejects, status); sims whose saved step is 0 restart from rest
-    and equal it too. The closure continues the sims its gate sends back this way."""
+    and equal it too. The closure continues the sims its gate sends back this way.
+    lanes 2: two threads per sim from 3 atoms (the one-launch request runs per size)."""
     torch = pytest.importorskip("torch")
+    engine.set_tuning(lanes_per_sim=lanes)
+    try:
+        _saved_state_resumes(engine, ce, wl, torch, mode, schedule)
+    finally:
+        engine.set_tuning()
+
+
+def _saved_state_resumes(engine, ce, wl, torch, mode, schedule):
     sch = {"one": ce.CE_SCHEDULE_ONE_LAUNCH, "per_size": ce.CE_SCHEDULE_PER_SIZE,
            "overlap": ce.CE_SCHEDULE_OVERLAP}[schedule]
     S = 6000
