@@ -118,7 +118,10 @@ typedef struct ce_tuning {
                              * 0: a default per molecule size)                       */
   int32_t lanes_per_sim;    /* 1 = one thread per sim; 2 = two threads per sim     *
                              * (3+ atoms; at 2 atoms, one lane per atom); 3..10 =   *
-                             * one lane per atom                                     */
+                             * one lane per atom. Mixed batches: 2 = two threads    *
+                             * per sim in the per-size schedules (a one-launch      *
+                             * request then runs per size), otherwise one lane per  *
+                             * atom                                                  */
 } ce_tuning;
 
 /* Engine lifetime. ce_create selects `device` and allocates the engine's small
@@ -249,9 +252,9 @@ void ce_graph_destroy(ce_graph* g);
 
 /* ---- autotuner -----------------------------------------------------------
  * Time candidate launch shapes on the device -- threads per block (sims per
- * block), refill granularity, and for the fixed path the layout (one thread per
- * sim, two threads per sim or one lane per atom) -- over the caller's device
- * inputs, and keep the
+ * block), refill granularity, and the layout (fixed path: one thread per sim,
+ * two threads per sim or one lane per atom; mixed path: one lane per atom or
+ * two threads per sim) -- over the caller's device inputs, and keep the
  * fastest in the engine; it then applies wherever the matching ce_tuning field
  * is 0 (fixed path: per atom count; mixed path: one entry, plus the faster
  * schedule in *best_schedule). `report` (may be NULL) receives up to `cap`
