@@ -1087,47 +1087,32 @@ __device__ __forceinline__ void io_count(const RunParams& P, bool fin, unsigned 
   }
 }
 
-// Persistent loop: each warp keeps its sims busy by pulling sim indices from the
-// work queue `cursor` over [0, count) (mapped through perm when non-null; one
-// warp-aggregated atomicAdd per refill) whenever at least `refill` of its sims
-// are idle (or all of them). A sim is one lane (T = 1, 32 sims a warp) or one
-// even/odd lane pair (T = 2, 16 sims a warp; the pair's lanes are always active
-// or idle together). With kLoopIO the claimed sims' inputs are awaited
-// (io_wait_input) and finished sims are counted (io_count).
+// Persistent loop of the mixed-batch two-thread buckets: each warp keeps its
+// sims busy by pulling sim indices from the bucket's work queue `cursor` over
+// [0, count), mapped through perm (one warp-aggregated atomicAdd per refill),
+// whenever at least `refill` of its 16 sims are idle (or all of them); a sim is
+// one even/odd lane pair, whose lanes are always active or idle together.
 template <int N, int MODE, int T, int F>
 __device__ __forceinline__ void sim_loop(const RunParams& P, const FixedMol& M, const MixedIn& X,
                                          unsigned long long* cursor, unsigned long long count, const uint32_t* perm,
                                          int refill) {
-  constexpr bool IO = (F & kLoopIO) != 0;
+  static_assert(T == 2 && (F & kLoopMixed) != 0 && (F & kLoopIO) == 0, "the mixed-batch two-thread loop");
   extern __shared__ float4 ce_stage_slots[];
   ThreadSim<N, MODE, T> s;
   SimConsts<N, T> C;
   bool active = false;
   bool queue_empty = count == 0ull;
   const unsigned lane = threadIdx.x & 31u;
-  if constexpr (T == 2) {
-    if constexpr ((F & kLoopMixed) != 0) {  // per-sim constants are loaded at each claim
-      C.half = static_cast<int>(lane & 1u);
-      C.pmask = 3u << (lane & 30u);
-    } else {
-      load_pair_consts<N>(C, M, lane);
-    }
-  }
-  constexpr unsigned kSimLanes = T == 2 ? 0x55555555u : 0xffffffffu;  // one lane per sim
-  const unsigned first = T == 2 ? (lane & ~1u) : lane;                // this sim's first lane
+  C.half = static_cast<int>(lane & 1u);  // per-sim constants are loaded at each claim
+  C.pmask = 3u << (lane & 30u);
+  constexpr unsigned kSimLanes = 0x55555555u;  // one lane per sim
+  const unsigned first = lane & ~1u;           // this sim's first lane
   const unsigned lt_mask = (1u << first) - 1u;
   float4* ks = ce_stage_slots + threadIdx.x;
   const int B = static_cast<int>(blockDim.x);
-  // IO: chunks [0, io_known) seen present by this warp. Chunks hold 2^io_shift
-  // sims, so a sim's chunk is a shift (a 64-bit division per iteration cost the
-  // kernel ~5 %), and the one register of state keeps the CH4 kernel within
-  // its 128.
-  unsigned io_known = 0u;
   for (;;) {
     const unsigned idle = __ballot_sync(0xffffffffu, !active);
     const unsigned idle_s = idle & kSimLanes;
-    bool fin = false;  // IO: this thread's sim finished at its claim
-    unsigned long long fin_sim = 0ull;
     if (!queue_empty && idle != 0u && (idle == 0xffffffffu || __popc(idle_s) >= refill)) {
       const int cnt = __popc(idle_s);
       const int leader = __ffs(idle_s) - 1;
@@ -1135,46 +1120,16 @@ __device__ __forceinline__ void sim_loop(const RunParams& P, const FixedMol& M, 
       if (static_cast<int>(lane) == leader) base = atomicAdd(cursor, static_cast<unsigned long long>(cnt));
       base = __shfl_sync(0xffffffffu, base, leader);
       queue_empty = (base + static_cast<unsigned long long>(cnt) >= count);
-      bool in_ok = true;
-      if constexpr (IO) {
-        // The claimed range's inputs. Chunks arrive in order, so the wait is for
-        // its last chunk, and only for chunks this warp has not yet seen present
-        // (an acquire per refill cost the kernel ~8 %).
-        if (base < count) {
-          const unsigned long long last = (base + cnt < count ? base + cnt : count) - 1ull;
-          const unsigned lc = static_cast<unsigned>(last >> P.io_shift);
-          if (lc >= io_known) {
-            if (static_cast<int>(lane) == leader) in_ok = io_wait_input(P.io_ready + lc, P.io_abort, P.io_error);
-            in_ok = __shfl_sync(0xffffffffu, in_ok, leader);
-            if (in_ok) io_known = lc + 1u;
-          }
-        }
-      }
       if (!active) {
         const unsigned long long k = base + static_cast<unsigned long long>(__popc(idle_s & lt_mask));
-        if (k < count) {
-          const unsigned long long sim = perm ? static_cast<unsigned long long>(perm[k]) : k;
-          if (in_ok) {
-            active = thread_init<N, MODE, T, F>(s, sim, P, M, X, C, ks, B);
-          } else if (P.status && lane == first) {
-            P.status[sim] = static_cast<uint8_t>(CE_SIM_BAD_INPUT);
-          }
-          fin = !active;
-          fin_sim = sim;
-        }
+        if (k < count) active = thread_init<N, MODE, T, F>(s, static_cast<unsigned long long>(perm[k]), P, M, X, C, ks, B);
       }
     }
-    if constexpr (IO) io_count<T>(P, fin, fin_sim);
     if (!__any_sync(0xffffffffu, active)) {
       if (queue_empty) break;
       continue;
     }
-    bool done = false;
-    if (active) {
-      active = thread_attempt<N, MODE, T, F>(s, P, M, X, C, ks);
-      done = !active;
-    }
-    if constexpr (IO) io_count<T>(P, done, s.sim);
+    if (active) active = thread_attempt<N, MODE, T, F>(s, P, M, X, C, ks);
   }
 }
 
