@@ -836,11 +836,31 @@ __device__ __forceinline__ bool thread_init(ThreadSim<N, MODE, T>& s, unsigned l
   return true;
 }
 
+// A sim that stops in thread_attempt is written out later, by the persistent
+// loop's finalize_pending, when its warp next refills: the warp's idle threads
+// then run the FP64 finalize together instead of one at a time (alone, each
+// thread's finalize held up the other 31 for about 5 % of a sim's warp time).
+// Until then the step size and the stop threshold, no longer needed, hold the
+// status and the final potential energy.
+template <int N, int MODE, int T>
+__device__ __forceinline__ void mark_finished(ThreadSim<N, MODE, T>& s, int status,
+                                              typename ThreadSim<N, MODE, T>::Acc pe_final) {
+  s.rej_in_step = static_cast<uint32_t>(status);
+  s.pe_stop = pe_final;
+}
+template <int N, int MODE, int T, int F>
+__device__ __forceinline__ void finalize_pending(const ThreadSim<N, MODE, T>& s, const RunParams& P,
+                                                 const FixedMol& M, const MixedIn& X, const SimConsts<N, T>& C,
+                                                 const float4* ks) {
+  thread_finalize<N, MODE, T, F>(s, static_cast<int>(s.rej_in_step), static_cast<double>(s.pe_stop), P, M, X, C,
+                                 ks);
+}
+
 // One DP5(4) attempt (src/integrators.cpp:83-146) plus, on acceptance, the
 // driver's stop test (src/driver.cpp:19-30). `ks` is this thread's first stage
 // chunk in shared memory; chunk c of stage slot l is ks[(l * NC + c) * B], B =
 // sim_block<N, T>(), so every slot offset is an immediate.
-// Returns false once the sim is finished and written out.
+// Returns false once the sim is finished (mark_finished).
 template <int N, int MODE, int T, int F>
 __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE, T>& s, const RunParams& P, const FixedMol& M,
                                                const MixedIn& X, const SimConsts<N, T>& C, float4* ks) {
@@ -1012,7 +1032,7 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE, T>& s, const R
     if (!(pe_new > s.pe_stop)) fin = CE_SIM_OK;
     else if (s.steps >= P.max_steps) fin = CE_SIM_MAX_STEPS;
     if (fin >= 0) {
-      thread_finalize<N, MODE, T, F>(s, fin, static_cast<double>(pe_new), P, M, X, C, ks);
+      mark_finished(s, fin, pe_new);
       return false;
     }
     return true;
@@ -1022,7 +1042,7 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE, T>& s, const R
   s.rejects += 1u;
   s.rej_in_step += 1u;
   if (s.rej_in_step > static_cast<uint32_t>(kMaxRejections)) {
-    thread_finalize<N, MODE, T, F>(s, CE_SIM_REJECT_LIMIT, static_cast<double>(pe_new), P, M, X, C, ks);
+    mark_finished(s, CE_SIM_REJECT_LIMIT, pe_new);
     return false;
   }
   return true;
@@ -1091,7 +1111,8 @@ __device__ __forceinline__ void io_count(const RunParams& P, bool fin, unsigned 
 // sims busy by pulling sim indices from the bucket's work queue `cursor` over
 // [0, count), mapped through perm (one warp-aggregated atomicAdd per refill),
 // whenever at least `refill` of its 16 sims are idle (or all of them); a sim is
-// one even/odd lane pair, whose lanes are always active or idle together.
+// one even/odd lane pair, whose lanes are always active or idle together. The
+// sims stopped since the last refill are written out first (finalize_pending).
 template <int N, int MODE, int T, int F>
 __device__ __forceinline__ void sim_loop(const RunParams& P, const FixedMol& M, const MixedIn& X,
                                          unsigned long long* cursor, unsigned long long count, const uint32_t* perm,
@@ -1110,10 +1131,16 @@ __device__ __forceinline__ void sim_loop(const RunParams& P, const FixedMol& M, 
   const unsigned lt_mask = (1u << first) - 1u;
   float4* ks = ce_stage_slots + threadIdx.x;
   const int B = static_cast<int>(blockDim.x);
+  bool pending = false;  // this thread's stopped sim is not yet written out
   for (;;) {
     const unsigned idle = __ballot_sync(0xffffffffu, !active);
     const unsigned idle_s = idle & kSimLanes;
-    if (!queue_empty && idle != 0u && (idle == 0xffffffffu || __popc(idle_s) >= refill)) {
+    const bool claim = !queue_empty && idle != 0u && (idle == 0xffffffffu || __popc(idle_s) >= refill);
+    if ((claim || queue_empty) && pending) {
+      finalize_pending<N, MODE, T, F>(s, P, M, X, C, ks);
+      pending = false;
+    }
+    if (claim) {
       const int cnt = __popc(idle_s);
       const int leader = __ffs(idle_s) - 1;
       unsigned long long base = 0ull;
@@ -1129,13 +1156,21 @@ __device__ __forceinline__ void sim_loop(const RunParams& P, const FixedMol& M, 
       if (queue_empty) break;
       continue;
     }
-    if (active) active = thread_attempt<N, MODE, T, F>(s, P, M, X, C, ks);
+    if (active) {
+      active = thread_attempt<N, MODE, T, F>(s, P, M, X, C, ks);
+      pending = !active;
+    }
   }
 }
 
-// The fixed-molecule form of the persistent loop (work queue P.cursor over
-// [0, P.S), refill threshold P.refill_threshold), kept apart from sim_loop: the
-// same loop with the queue passed as arguments ran the CH4 kernel 0.5 % slower.
+// Persistent loop of the fixed-molecule kernels: each warp pulls sim indices from
+// the work queue P.cursor over [0, P.S) (one warp-aggregated atomicAdd per
+// refill) whenever at least P.refill_threshold of its sims are idle (or all of
+// them); a sim is one lane (T = 1) or one even/odd lane pair (T = 2). The sims
+// stopped since the last refill are written out first (finalize_pending). With
+// kLoopIO the claimed sims' inputs are awaited (io_wait_input) and written-out
+// sims counted (io_count). Kept apart from sim_loop: the same loop with the
+// queue passed as arguments ran the CH4 kernel 0.5 % slower.
 template <int N, int MODE, int T, int F>
 __device__ __forceinline__ void fixed_loop(const RunParams& P, const FixedMol& M) {
   constexpr bool IO = (F & kLoopIO) != 0;
@@ -1153,12 +1188,19 @@ __device__ __forceinline__ void fixed_loop(const RunParams& P, const FixedMol& M
   float4* ks = ce_stage_slots + threadIdx.x;
   const int B = static_cast<int>(blockDim.x);
   unsigned io_known = 0u;  // IO: chunks [0, io_known) seen present by this warp
+  bool pending = false;    // this thread's stopped sim is not yet written out
   for (;;) {
     const unsigned idle = __ballot_sync(0xffffffffu, !active);
     const unsigned idle_s = idle & kSimLanes;
+    const bool claim = !queue_empty && idle != 0u && (idle == 0xffffffffu || __popc(idle_s) >= P.refill_threshold);
+    if (claim || queue_empty) {  // warp-uniform: the stopped sims are written out together
+      if (pending) finalize_pending<N, MODE, T, F>(s, P, M, X, C, ks);
+      if constexpr (IO) io_count<T>(P, pending, s.sim);
+      pending = false;
+    }
     bool fin = false;  // IO: this thread's sim finished at its claim
     unsigned long long fin_sim = 0ull;
-    if (!queue_empty && idle != 0u && (idle == 0xffffffffu || __popc(idle_s) >= P.refill_threshold)) {
+    if (claim) {
       const int cnt = __popc(idle_s);
       const int leader = __ffs(idle_s) - 1;
       unsigned long long base = 0ull;
@@ -1195,12 +1237,10 @@ __device__ __forceinline__ void fixed_loop(const RunParams& P, const FixedMol& M
       if (queue_empty) break;
       continue;
     }
-    bool done = false;
     if (active) {
       active = thread_attempt<N, MODE, T, F>(s, P, M, X, C, ks);
-      done = !active;
+      pending = !active;
     }
-    if constexpr (IO) io_count<T>(P, done, s.sim);
   }
 }
 
