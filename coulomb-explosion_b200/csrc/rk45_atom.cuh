@@ -361,12 +361,23 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
   bool queue_empty = count == 0ull;
   const unsigned lt_mask = (1u << lane) - 1u;
 
+  // A group whose sim stopped is written out at the warp's next refill (or once
+  // the queue is empty): the finalize is a whole-warp step, so the groups that
+  // stopped since the last refill share one. Until then the group's rejection
+  // counter and stop threshold, no longer needed, hold the status and the final
+  // potential energy.
+  bool pending = false;
   for (;;) {
     // ---- refill: one claim per idle group, warp-aggregated ----
     bool fresh = false;
     const unsigned idle = __ballot_sync(0xffffffffu, leader && !active);
-    if (!queue_empty && idle != 0u &&
-        (__popc(idle) >= refill || __ballot_sync(0xffffffffu, active) == 0u)) {
+    const bool claim = !queue_empty && idle != 0u && (__popc(idle) >= refill || __ballot_sync(0xffffffffu, active) == 0u);
+    if ((claim || queue_empty) && __ballot_sync(0xffffffffu, pending) != 0u) {
+      atom_finalize<N, MODE, STRIDE, STATE>(s, pending ? static_cast<int>(s.rej_in_step) : -1,
+                                            static_cast<double>(s.pe_stop), ac, ai, base, P);
+      pending = false;
+    }
+    if (claim) {
       const int cnt = __popc(idle);
       const int first = __ffs(idle) - 1;
       unsigned long long b0 = 0ull;
@@ -594,10 +605,13 @@ __device__ __forceinline__ void atom_loop(const RunParams& P, const FixedMol& M,
         s.rej_in_step += 1u;
         if (s.rej_in_step > static_cast<uint32_t>(kMaxRejections)) fin_st = CE_SIM_REJECT_LIMIT;
       }
-      if (fin_st >= 0) active = false;
+      if (fin_st >= 0) {
+        active = false;
+        pending = true;
+        s.rej_in_step = static_cast<uint32_t>(fin_st);
+        s.pe_stop = pe_new;
+      }
     }
-    if (__ballot_sync(0xffffffffu, fin_st >= 0) != 0u)
-      atom_finalize<N, MODE, STRIDE, STATE>(s, fin_st, static_cast<double>(pe_new), ac, ai, base, P);
   }
 }
 
