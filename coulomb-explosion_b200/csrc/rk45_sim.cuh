@@ -160,6 +160,30 @@ constexpr int kLoopIO = 1, kLoopMixed = 2, kLoopState = 4;
 // exactly like the scalar instruction) and the approximate MUFU forms.
 __device__ __forceinline__ float2 bcast(float s) { return make_float2(s, s); }
 
+// Packed operations on float pair p of a register vector with NF real floats
+// (p a compile-time index after unrolling): both halves in one FFMA2 / FMUL2 /
+// FADD2 while both are real; when NF is odd the last real float alone in a
+// scalar instruction, its padding half left as it is; a pair of padding alone is
+// left untouched. A padding half would otherwise take an FMA-pipe slot of its own.
+template <int NF>
+__device__ __forceinline__ float2 pfma(int p, float2 a, float2 b, float2 c) {
+  if (2 * p + 1 < NF) return __ffma2_rn(a, b, c);
+  if (2 * p < NF) return make_float2(fmaf(a.x, b.x, c.x), c.y);
+  return c;
+}
+template <int NF>
+__device__ __forceinline__ float2 pmul(int p, float2 a, float2 b) {
+  if (2 * p + 1 < NF) return __fmul2_rn(a, b);
+  if (2 * p < NF) return make_float2(a.x * b.x, 0.0f);
+  return make_float2(0.0f, 0.0f);
+}
+template <int NF>
+__device__ __forceinline__ float2 padd(int p, float2 a, float2 b) {
+  if (2 * p + 1 < NF) return __fadd2_rn(a, b);
+  if (2 * p < NF) return make_float2(a.x + b.x, a.y);
+  return a;
+}
+
 // Approximate reciprocal and square root (PTX rcp.approx / sqrt.approx, flush
 // to zero): for the error-norm scales and the initial-step heuristic, where a
 // relative error of a few 1e-7 changes no decision the integrator relies on.
@@ -884,15 +908,15 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE, T>& s, const R
       // (stage 2 has no k term)
       const float chh = c_c[si + 1] * hh;
 #pragma unroll
-      for (int p = 0; p < NP; ++p) xs[p] = __ffma2_rn(bcast(chh), s.v[p], s.x[p]);
+      for (int p = 0; p < NP; ++p) xs[p] = pfma<NF>(p, bcast(chh), s.v[p], s.x[p]);
       if (si > 1) {
         const float a1 = c_abar[si + 1][1] * hh2;
         const float4* k1 = ks + s.k1s * NC * B;
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
           const float4 q = k1[c * B];
-          xs[2 * c] = __ffma2_rn(bcast(a1), make_float2(q.x, q.y), xs[2 * c]);
-          xs[2 * c + 1] = __ffma2_rn(bcast(a1), make_float2(q.z, q.w), xs[2 * c + 1]);
+          xs[2 * c] = pfma<NF>(2 * c, bcast(a1), make_float2(q.x, q.y), xs[2 * c]);
+          xs[2 * c + 1] = pfma<NF>(2 * c + 1, bcast(a1), make_float2(q.z, q.w), xs[2 * c + 1]);
         }
       }
 #pragma unroll 1
@@ -902,8 +926,8 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE, T>& s, const R
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
           const float4 q = kl[c * B];
-          xs[2 * c] = __ffma2_rn(bcast(al), make_float2(q.x, q.y), xs[2 * c]);
-          xs[2 * c + 1] = __ffma2_rn(bcast(al), make_float2(q.z, q.w), xs[2 * c + 1]);
+          xs[2 * c] = pfma<NF>(2 * c, bcast(al), make_float2(q.x, q.y), xs[2 * c]);
+          xs[2 * c + 1] = pfma<NF>(2 * c + 1, bcast(al), make_float2(q.z, q.w), xs[2 * c + 1]);
         }
       }
       sim_forces<N, T, Acc>(xs, a, M, C, false, no_pe);
@@ -922,11 +946,11 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE, T>& s, const R
     for (int p = 0; p < NP; ++p) {
       // one chunk's k2..k6 at a time keeps the stage-7 sums' live range short
       const float4 q1 = ks[(s.k1s * NC + (p >> 1)) * B];
-      float2 sum = __fmul2_rn(bcast(c_abar[7][1]), (p & 1) ? make_float2(q1.z, q1.w) : make_float2(q1.x, q1.y));
+      float2 sum = pmul<NF>(p, bcast(c_abar[7][1]), (p & 1) ? make_float2(q1.z, q1.w) : make_float2(q1.x, q1.y));
 #pragma unroll
       for (int l = 1; l < 6; ++l) {
         const float4 q = ks[((l - 1) * NC + (p >> 1)) * B];
-        sum = __ffma2_rn(bcast(c_abar[7][l + 1]), (p & 1) ? make_float2(q.z, q.w) : make_float2(q.x, q.y), sum);
+        sum = pfma<NF>(p, bcast(c_abar[7][l + 1]), (p & 1) ? make_float2(q.z, q.w) : make_float2(q.x, q.y), sum);
       }
       if (S::kKahan) {  // compensated update; the new compensation goes to the other cx slot
         const float2 inc = __ffma2_rn(bcast(hh2), sum, __fmul2_rn(bcast(hh), s.v[p]));
@@ -936,7 +960,7 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE, T>& s, const R
         const float2 cn = __ffma2_rn(bcast(-1.0f), y, __ffma2_rn(bcast(-1.0f), s.x[p], xs[p]));
         reinterpret_cast<float2*>(ks + ((15 - s.cxs) * NC + (p >> 1)) * B)[p & 1] = cn;
       } else {
-        xs[p] = __ffma2_rn(bcast(hh2), sum, __ffma2_rn(bcast(hh), s.v[p], s.x[p]));  // c_7 = 1
+        xs[p] = pfma<NF>(p, bcast(hh2), sum, pfma<NF>(p, bcast(hh), s.v[p], s.x[p]));  // c_7 = 1
       }
     }
     sim_forces<N, T, Acc>(xs, a, M, C, true, pe_new);
@@ -962,17 +986,17 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE, T>& s, const R
     for (int hp = 0; hp < 2; ++hp) {
       const int p = 2 * c + hp;
       const float2 k1 = hp == 0 ? make_float2(q1.x, q1.y) : make_float2(q1.z, q1.w);
-      float2 sv = __fmul2_rn(bcast(c_b[1]), k1);
-      float2 se = __fmul2_rn(bcast(c_ebar[1]), k1);
-      float2 sev = __fmul2_rn(bcast(c_e[1]), k1);
+      float2 sv = pmul<NF>(p, bcast(c_b[1]), k1);
+      float2 se = pmul<NF>(p, bcast(c_ebar[1]), k1);
+      float2 sev = pmul<NF>(p, bcast(c_e[1]), k1);
 #pragma unroll
       for (int l = 1; l < 6; ++l) {
         const float2 kl = hp == 0 ? make_float2(q[l - 1].x, q[l - 1].y) : make_float2(q[l - 1].z, q[l - 1].w);
-        if (l != 1) sv = __ffma2_rn(bcast(c_b[l + 1]), kl, sv);
-        se = __ffma2_rn(bcast(c_ebar[l + 1]), kl, se);
-        if (l != 1) sev = __ffma2_rn(bcast(c_e[l + 1]), kl, sev);
+        if (l != 1) sv = pfma<NF>(p, bcast(c_b[l + 1]), kl, sv);
+        se = pfma<NF>(p, bcast(c_ebar[l + 1]), kl, se);
+        if (l != 1) sev = pfma<NF>(p, bcast(c_e[l + 1]), kl, sev);
       }
-      const float2 incv = __fmul2_rn(bcast(hh), sv);
+      const float2 incv = pmul<NF>(p, bcast(hh), sv);
       if (S::kKahan) {  // compensated update; the new compensation goes to the other cv slot
         const float4 qc = ks[(s.cvs * NC + c) * B];
         const float2 y = __ffma2_rn(bcast(-1.0f), hp == 0 ? make_float2(qc.x, qc.y) : make_float2(qc.z, qc.w), incv);
@@ -980,11 +1004,11 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE, T>& s, const R
         const float2 cn = __ffma2_rn(bcast(-1.0f), y, __ffma2_rn(bcast(-1.0f), s.v[p], vn[p]));
         reinterpret_cast<float2*>(ks + ((19 - s.cvs) * NC + c) * B)[hp] = cn;
       } else {
-        vn[p] = __fadd2_rn(s.v[p], incv);
+        vn[p] = padd<NF>(p, s.v[p], incv);
       }
-      const float2 ex = __fmul2_rn(bcast(hh2), se);
+      const float2 ex = pmul<NF>(p, bcast(hh2), se);
       const float2 k7 = hp == 0 ? make_float2(q[5].x, q[5].y) : make_float2(q[5].z, q[5].w);
-      const float2 ev = __fmul2_rn(bcast(hh), __ffma2_rn(bcast(c_e[7]), k7, sev));
+      const float2 ev = pmul<NF>(p, bcast(hh), pfma<NF>(p, bcast(c_e[7]), k7, sev));
       // Scaled errors e / (atol + rtol max(|y0|, |y1|)), both halves of the pair
       // at once; a zero-padded half is left out (its scale could be 0).
       if (2 * p + 1 < NF) {
