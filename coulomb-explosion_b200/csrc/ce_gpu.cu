@@ -431,10 +431,19 @@ int run_streamed(ce_engine* e, uint64_t S, const float* pos, const ce_run_config
       st = cudaMemcpyAsync(ready + j, e->h_io + ce::kIoOne, sizeof(unsigned), cudaMemcpyHostToDevice, e->s_in);
     if (st != cudaSuccess) return abort_run(ce::cuda_fail(e, st, "cudaMemcpyAsync(streamed H2D)"));
   }
+  if ((rc = ce::record(e, e->ev_loaded[1], e->s_in)) != CE_OK) return abort_run(rc);
   // Results down, chunk by chunk as the kernel completes them. The host waits
   // at most kIoHostWaitSeconds for one chunk, and stops waiting once the kernel
-  // has ended without completing it.
+  // has ended without completing it. If the input copies have not all landed
+  // within a few seconds of the launch (far longer than they take beside the
+  // kernel), the copies are being held back until the kernel ends (a tool that
+  // serialises GPU work, not caught by gpu_work_serialised): the host raises the
+  // abort word, the kernel's waits end at their next check, and ce_run falls
+  // back to the chunked pipeline instead of waiting for the waits to run out.
   constexpr double kIoHostWaitSeconds = 120.0;
+  const double input_deadline = 2.0 + static_cast<double>(S * n3 * sizeof(float)) * 1e-9;  // >= 1 GB/s
+  const auto t_launch = std::chrono::steady_clock::now();
+  bool inputs_landed = false;
   for (uint64_t j = 0; j < J; ++j) {
     const auto t0 = std::chrono::steady_clock::now();
     for (uint64_t spin = 1; hio[j] == 0u; ++spin) {
@@ -444,7 +453,17 @@ int run_streamed(ce_engine* e, uint64_t S, const float* pos, const ce_run_config
           if (q != cudaSuccess) return abort_run(ce::cuda_fail(e, q, "streamed kernel"));
           return abort_run(ce::fail(e, CE_ERR_CUDA, "ce_run: the streamed kernel ended before finishing a chunk"));
         }
-        if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > kIoHostWaitSeconds)
+        const auto now = std::chrono::steady_clock::now();
+        if (!inputs_landed && std::chrono::duration<double>(now - t_launch).count() > input_deadline) {
+          const cudaError_t qi = cudaEventQuery(e->ev_loaded[1]);
+          if (qi == cudaErrorNotReady) {
+            abort_run(CE_OK);
+            return kIoWaitRanOut;
+          }
+          if (qi != cudaSuccess) return abort_run(ce::cuda_fail(e, qi, "streamed input copies"));
+          inputs_landed = true;
+        }
+        if (std::chrono::duration<double>(now - t0).count() > kIoHostWaitSeconds)
           return abort_run(ce::fail(e, CE_ERR_CUDA, "ce_run: timed out waiting for a streamed chunk"));
         std::this_thread::yield();
       }

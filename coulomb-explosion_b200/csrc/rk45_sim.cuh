@@ -953,11 +953,11 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE, T>& s, const R
         sum = pfma<NF>(p, bcast(c_abar[7][l + 1]), (p & 1) ? make_float2(q.z, q.w) : make_float2(q.x, q.y), sum);
       }
       if (S::kKahan) {  // compensated update; the new compensation goes to the other cx slot
-        const float2 inc = __ffma2_rn(bcast(hh2), sum, __fmul2_rn(bcast(hh), s.v[p]));
+        const float2 inc = pfma<NF>(p, bcast(hh2), sum, pmul<NF>(p, bcast(hh), s.v[p]));
         const float4 qc = ks[(s.cxs * NC + (p >> 1)) * B];
-        const float2 y = __ffma2_rn(bcast(-1.0f), (p & 1) ? make_float2(qc.z, qc.w) : make_float2(qc.x, qc.y), inc);
-        xs[p] = __fadd2_rn(s.x[p], y);
-        const float2 cn = __ffma2_rn(bcast(-1.0f), y, __ffma2_rn(bcast(-1.0f), s.x[p], xs[p]));
+        const float2 y = pfma<NF>(p, bcast(-1.0f), (p & 1) ? make_float2(qc.z, qc.w) : make_float2(qc.x, qc.y), inc);
+        xs[p] = padd<NF>(p, s.x[p], y);
+        const float2 cn = pfma<NF>(p, bcast(-1.0f), y, pfma<NF>(p, bcast(-1.0f), s.x[p], xs[p]));
         reinterpret_cast<float2*>(ks + ((15 - s.cxs) * NC + (p >> 1)) * B)[p & 1] = cn;
       } else {
         xs[p] = pfma<NF>(p, bcast(hh2), sum, pfma<NF>(p, bcast(hh), s.v[p], s.x[p]));  // c_7 = 1
@@ -999,9 +999,9 @@ __device__ __forceinline__ bool thread_attempt(ThreadSim<N, MODE, T>& s, const R
       const float2 incv = pmul<NF>(p, bcast(hh), sv);
       if (S::kKahan) {  // compensated update; the new compensation goes to the other cv slot
         const float4 qc = ks[(s.cvs * NC + c) * B];
-        const float2 y = __ffma2_rn(bcast(-1.0f), hp == 0 ? make_float2(qc.x, qc.y) : make_float2(qc.z, qc.w), incv);
-        vn[p] = __fadd2_rn(s.v[p], y);
-        const float2 cn = __ffma2_rn(bcast(-1.0f), y, __ffma2_rn(bcast(-1.0f), s.v[p], vn[p]));
+        const float2 y = pfma<NF>(p, bcast(-1.0f), hp == 0 ? make_float2(qc.x, qc.y) : make_float2(qc.z, qc.w), incv);
+        vn[p] = padd<NF>(p, s.v[p], y);
+        const float2 cn = pfma<NF>(p, bcast(-1.0f), y, pfma<NF>(p, bcast(-1.0f), s.v[p], vn[p]));
         reinterpret_cast<float2*>(ks + ((19 - s.cvs) * NC + c) * B)[hp] = cn;
       } else {
         vn[p] = padd<NF>(p, s.v[p], incv);
