@@ -846,7 +846,8 @@ def run_stream(args):
         d["host"] = {k: torch.empty(d[k].shape, dtype=d[k].dtype, pin_memory=True)
                      for k in ("momenta", "ker", "steps", "status")}
         slots.append(d)
-    _, sched = eng.autotune_mixed(C_, slots[0]["cb"], cfg)
+    mrep, sched = eng.autotune_mixed(C_, slots[0]["cb"], cfg)
+    mixed_pick = max(mrep, key=lambda r: r["sims_per_s"]) if mrep else {"lanes_per_sim": 0}
     eng.reserve_mixed(C_)
     # the plain leg: this molecule through the fixed-molecule entry point (rows of
     # 10 atoms are the same [S][10][3] layout in both), its layout autotuned
@@ -1013,8 +1014,9 @@ def run_stream(args):
                                "2-slot pinned host ring consumed by the host",
                    "plain_path": "ce_run_device (fixed molecule), autotuned lanes_per_sim "
                                  f"{fixed_tuning['lanes_per_sim']}, refill {fixed_tuning['refill_threshold']}",
-                   "closure_path": "ce_closure_serve: loose run and continuation through the mixed-batch kernels "
-                                   "(lane per atom)",
+                   "closure_path": "ce_closure_serve: loose run and continuation through the mixed-batch kernels, "
+                                   "autotuned " + ("two threads per sim" if mixed_pick["lanes_per_sim"] == 2
+                                                   else "one lane per atom"),
                    "d2h_bytes_per_chunk": d2h_bytes},
         "plain": res["plain"], "closure": res["closure"],
         "speedup_vs_plain": res["closure"]["explosions_per_s"] / res["plain"]["explosions_per_s"],
